@@ -1,0 +1,416 @@
+"""``CudaAcousticFDTD``: the reference solver surface over the sm_100a kernels.
+
+Same constructor, methods and properties as ac-fdtd's ``AcousticFDTD`` (``src/ac_fdtd/
+scheme.py:82-389``) and ``CAcousticFDTD`` (``src/ac_fdtd/c_backend.py:160-382``): a caller swaps
+the class and nothing else. The state lives on the GPU; ``p``, ``velocity`` and
+``relaxation_states`` are host snapshots in pinned memory, refreshed from the device on every
+access, and whatever is written into them is uploaded before the next ``run``. Arrays obtained
+before a ``run`` are not updated by it: read the property again afterwards.
+
+There is no CPU path. If the CUDA library cannot be loaded or no GPU is present, the
+constructor raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import numpy as np
+
+from . import _native
+from .coefficients import room_coefficients
+from .grid import cell_index
+from .medium import AIR
+
+__all__ = ["CudaAcousticFDTD", "DEFAULT_STEPS_PER_GRAPH", "pinned_array"]
+
+#: Steps captured per CUDA graph for long runs; shorter runs launch step by step.
+DEFAULT_STEPS_PER_GRAPH = 64
+
+
+def _as_double_pointer(array: np.ndarray):
+    return array.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _free_native(handle):
+    if handle:
+        _native.library().acf_destroy(handle)
+
+
+class _PinnedBlock:
+    """Pinned host memory owned by the numpy arrays that view it; freed with the last view."""
+
+    def __init__(self, lib, shape, dtype: np.dtype):
+        self._lib = lib
+        self.pointer = ctypes.c_void_p()
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        _native.check(lib.acf_host_alloc(nbytes, ctypes.byref(self.pointer)), "acf_host_alloc")
+        self.__array_interface__ = {
+            "shape": tuple(shape), "typestr": dtype.str, "version": 3,
+            "data": (self.pointer.value or 0, False),
+        }
+
+    def __del__(self):
+        if self.pointer.value:
+            self._lib.acf_host_free(self.pointer)
+            self.pointer = ctypes.c_void_p()
+
+
+def pinned_array(shape, dtype=np.float32) -> np.ndarray:
+    """A zeroed numpy array in page-locked host memory (full-speed host<->device copies)."""
+    array = np.asarray(_PinnedBlock(_native.library(), tuple(shape), np.dtype(dtype)))
+    array[...] = 0
+    return array
+
+
+class CudaAcousticFDTD:
+    """The staggered pressure-velocity leapfrog on one B200, two fused sweeps per step.
+
+    Args mirror ``AcousticFDTD.__init__`` (``scheme.py:107-116``); ``stream`` is an optional
+    ``cudaStream_t`` handle (an int) to run on, and ``steps_per_graph`` the CUDA-graph chunk.
+    """
+
+    def __init__(self, grid, medium=AIR, courant: float = 1.0, dtype=np.float64, walls=None,
+                 absorbing_layer=None, air_absorption=None, *, stream: int = 0,
+                 steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH) -> None:
+        block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
+                                  air_absorption)
+        self.grid = grid
+        self.medium = medium
+        self.courant = courant
+        self.dtype = block.dtype
+        self.walls = walls
+        self.absorbing_layer = absorbing_layer
+        self.air_absorption = air_absorption
+        self.dt = block.dt
+        self.step_index = 0
+        self.coefficients = block
+        self._shape = block.shape
+        self._stream = ctypes.c_void_p(int(stream))
+
+        self._lib = _native.library()
+        count = ctypes.c_int(0)
+        _native.check(self._lib.acf_device_count(ctypes.byref(count)), "acf_device_count")
+        if count.value < 1:
+            raise RuntimeError("no CUDA device is visible; the cuda backend has no CPU path")
+
+        config = _native.AcfConfig()
+        config.nx, config.ny, config.nz = block.shape
+        config.precision = self.dtype.itemsize
+        config.n_relax = block.n_relax
+        config.vel_coef = block.vel_coef
+        config.pres_coef = block.pres_coef
+        config.src_coef = block.src_coef
+        config.relax_scale = block.relax_scale
+        for r in range(block.n_relax):
+            config.relax_decay[r] = block.relax_decay[r]
+            config.relax_mean[r] = block.relax_mean[r]
+            config.relax_gain[r] = block.relax_gain[r]
+        keep = []  # arrays that must outlive acf_create
+        if block.wall_shell is not None:
+            for f, shell in enumerate(block.wall_shell):
+                keep.append(shell)
+                config.wall_shell[f] = _as_double_pointer(shell)
+        if block.layer_cell is not None:
+            for a in range(3):
+                keep += [block.layer_cell[a], block.layer_face[a]]
+                config.cell[a] = _as_double_pointer(block.layer_cell[a])
+                config.face[a] = _as_double_pointer(block.layer_face[a])
+        handle = ctypes.c_void_p()
+        _native.check(self._lib.acf_create(ctypes.byref(config), ctypes.byref(handle)), "acf_create")
+        self._handle = handle
+        self._finalizer = weakref.finalize(self, _free_native, handle.value)
+        _native.check(self._lib.acf_set_graph(handle, int(steps_per_graph)), "acf_set_graph")
+
+        # Host snapshots: name -> ndarray, plus which are current and which were handed out.
+        self._mirror: dict[int, np.ndarray] = {}
+        self._mirror_current: set[int] = set()
+        self._mirror_exposed: set[int] = set()
+
+        self._sources: list[tuple[int, np.ndarray]] = []
+        self._receivers: list[tuple[int, int]] = []  # (flat cell, start step)
+        self._sources_dirty = False
+        self._receivers_dirty = False
+
+    # ------------------------------------------------------------------ geometry / time
+    @property
+    def time(self) -> float:
+        return self.step_index * self.dt
+
+    @property
+    def sample_rate(self) -> float:
+        return 1.0 / self.dt
+
+    @property
+    def n_relax(self) -> int:
+        return self.coefficients.n_relax
+
+    def _flat(self, point) -> int:
+        index = cell_index(float(self.grid.dx), self._shape, point)
+        return int(np.ravel_multi_index(index, self._shape))
+
+    # ------------------------------------------------------------------ state mirrors
+    def _field_shape(self, field: int) -> tuple[int, int, int]:
+        shape = list(self._shape)
+        if 1 <= field <= 3:
+            shape[field - 1] += 1
+        return tuple(shape)
+
+    def _mirror_array(self, field: int) -> np.ndarray:
+        if field not in self._mirror:
+            block = _PinnedBlock(self._lib, self._field_shape(field), self.dtype)
+            self._mirror[field] = np.asarray(block)
+        return self._mirror[field]
+
+    def _pull(self, fields) -> None:
+        pending = [f for f in fields if f not in self._mirror_current]
+        for f in pending:
+            array = self._mirror_array(f)
+            _native.check(self._lib.acf_download(self._handle, f, array.ctypes.data, self._stream),
+                          "acf_download")
+        if pending:
+            self.synchronize()
+            self._mirror_current.update(pending)
+
+    def _flush(self) -> None:
+        """Upload every snapshot the caller may have written since it was handed out."""
+        if not self._mirror_exposed:
+            return
+        for f in sorted(self._mirror_exposed):
+            array = self._mirror[f]
+            _native.check(self._lib.acf_upload(self._handle, f, array.ctypes.data, self._stream),
+                          "acf_upload")
+        # The copies read pinned memory asynchronously; finish them before the caller can
+        # write into the snapshots again.
+        self.synchronize()
+        self._mirror_exposed.clear()
+
+    def _expose(self, fields) -> list[np.ndarray]:
+        self._pull(fields)
+        self._mirror_exposed.update(fields)
+        return [self._mirror[f] for f in fields]
+
+    @property
+    def p(self) -> np.ndarray:
+        """Pressure p^n, shape (nx, ny, nz); a writable host snapshot."""
+        return self._expose([_native.FIELD_P])[0]
+
+    @p.setter
+    def p(self, value) -> None:
+        self.p[...] = value
+
+    @property
+    def velocity(self) -> list[np.ndarray]:
+        """[vx, vy, vz] at n - 1/2, shapes from ``Grid.velocity_shape``; writable snapshots."""
+        return self._expose([_native.FIELD_VX, _native.FIELD_VY, _native.FIELD_VZ])
+
+    @property
+    def vx(self) -> np.ndarray:
+        return self._expose([_native.FIELD_VX])[0]
+
+    @property
+    def vy(self) -> np.ndarray:
+        return self._expose([_native.FIELD_VY])[0]
+
+    @property
+    def vz(self) -> np.ndarray:
+        return self._expose([_native.FIELD_VZ])[0]
+
+    def set_state(self, p=None, velocity=None, relaxation=None) -> int:
+        """Upload state straight from caller arrays (reference layout, solver dtype).
+
+        Arrays in pinned memory (see :func:`pinned_array`) move at full link speed. Returns the
+        number of bytes copied host to device.
+        """
+        self._flush()
+        items = []
+        if p is not None:
+            items.append((_native.FIELD_P, p))
+        if velocity is not None:
+            items += [(_native.FIELD_VX + a, v) for a, v in enumerate(velocity)]
+        if relaxation is not None:
+            if len(relaxation) != self.n_relax:
+                raise ValueError(f"expected {self.n_relax} relaxation states, got {len(relaxation)}")
+            items += [(_native.FIELD_PSI0 + r, s) for r, s in enumerate(relaxation)]
+        total = 0
+        keep = []
+        for field, array in items:
+            array = np.ascontiguousarray(array, dtype=self.dtype)
+            if array.shape != self._field_shape(field):
+                raise ValueError(f"field {field}: shape {array.shape}, expected {self._field_shape(field)}")
+            keep.append(array)
+            _native.check(self._lib.acf_upload(self._handle, field, array.ctypes.data, self._stream),
+                          "acf_upload")
+            self._mirror_current.discard(field)
+            total += array.nbytes
+        self.synchronize()
+        return total
+
+    def get_state(self, p=None, velocity=None) -> int:
+        """Download p and/or the velocities into caller arrays; returns bytes copied."""
+        self._flush()
+        items = []
+        if p is not None:
+            items.append((_native.FIELD_P, p))
+        if velocity is not None:
+            items += [(_native.FIELD_VX + a, v) for a, v in enumerate(velocity)]
+        total = 0
+        for field, array in items:
+            if (array.shape != self._field_shape(field) or array.dtype != self.dtype
+                    or not array.flags.c_contiguous):
+                raise ValueError(f"field {field}: need a C-contiguous {self.dtype} array of shape "
+                                 f"{self._field_shape(field)}")
+            _native.check(self._lib.acf_download(self._handle, field, array.ctypes.data, self._stream),
+                          "acf_download")
+            total += array.nbytes
+        self.synchronize()
+        return total
+
+    @property
+    def relaxation_states(self) -> list[np.ndarray]:
+        """The ISO relaxation states psi_r, one (nx, ny, nz) snapshot per process."""
+        return self._expose([_native.FIELD_PSI0 + r for r in range(self.n_relax)])
+
+    # ------------------------------------------------------------------ sources / receivers
+    def add_volume_source(self, point, signal) -> None:
+        """Soft volume source at the cell containing ``point`` (``scheme.py:231-244``)."""
+        values = np.asarray(signal, dtype=self.dtype).reshape(-1)
+        self._sources.append((self._flat(point), values))
+        self._sources_dirty = True
+
+    def add_pressure_receiver(self, point) -> int:
+        """Record p at ``point`` after every step from now on (``scheme.py:246-255``)."""
+        self._receivers.append((self._flat(point), self.step_index))
+        self._receivers_dirty = True
+        return len(self._receivers) - 1
+
+    def _push_points(self) -> None:
+        if self._sources_dirty:
+            n = len(self._sources)
+            stride = max((s.size for _, s in self._sources), default=0)
+            cells = np.array([c for c, _ in self._sources], dtype=np.int64)
+            lengths = np.array([s.size for _, s in self._sources], dtype=np.int64)
+            signals = np.zeros((n, max(stride, 1)), dtype=np.float64)
+            for q, (_, s) in enumerate(self._sources):
+                signals[q, : s.size] = s
+            _native.check(self._lib.acf_set_sources(
+                self._handle, n, cells.ctypes.data_as(_native._I64P),
+                lengths.ctypes.data_as(_native._I64P), _as_double_pointer(signals), stride),
+                "acf_set_sources")
+            self._sources_dirty = False
+        if self._receivers_dirty:
+            cells = np.array([c for c, _ in self._receivers], dtype=np.int64)
+            starts = np.array([s for _, s in self._receivers], dtype=np.int64)
+            _native.check(self._lib.acf_set_receivers(
+                self._handle, len(self._receivers), cells.ctypes.data_as(_native._I64P),
+                starts.ctypes.data_as(_native._I64P)), "acf_set_receivers")
+            self._receivers_dirty = False
+
+    @property
+    def recorded_pressure(self) -> np.ndarray:
+        """Every receiver's samples as ``(channel, sample)`` (``scheme.py:257-262``).
+
+        Like the reference, receivers added part-way through have fewer samples, and asking
+        for a ragged set raises instead of padding.
+        """
+        if not self._receivers:
+            return np.zeros((0, 0))
+        self._push_points()
+        rows = []
+        for r, (_, start) in enumerate(self._receivers):
+            n = self.step_index - start
+            row = np.empty(n, dtype=self.dtype)
+            if n > 0:
+                _native.check(self._lib.acf_read_recording(
+                    self._handle, r, start, n, row.ctypes.data, self._stream), "acf_read_recording")
+            rows.append(row)
+        if len({row.size for row in rows}) > 1:
+            raise ValueError(
+                "receivers were added at different steps, so their recordings have different "
+                f"lengths {[row.size for row in rows]}; read them one by one with recording(r)"
+            )
+        return np.stack(rows)
+
+    def recording(self, receiver: int) -> np.ndarray:
+        """Samples of one receiver since it was added."""
+        self._push_points()
+        _, start = self._receivers[receiver]
+        n = self.step_index - start
+        row = np.empty(n, dtype=self.dtype)
+        if n > 0:
+            _native.check(self._lib.acf_read_recording(
+                self._handle, receiver, start, n, row.ctypes.data, self._stream),
+                "acf_read_recording")
+        return row
+
+    def probe_pressure(self, point) -> float:
+        return float(self.p[cell_index(float(self.grid.dx), self._shape, point)])
+
+    def probe_velocity(self, point, axis: int) -> float:
+        return float(self.velocity[axis][cell_index(float(self.grid.dx), self._shape, point)])
+
+    # ------------------------------------------------------------------ stepping
+    def run(self, n_steps: int) -> None:
+        """Advance ``n_steps`` on the GPU; asynchronous with respect to the host."""
+        n_steps = int(n_steps)
+        if n_steps <= 0:
+            return
+        self._flush()
+        self._push_points()
+        _native.check(self._lib.acf_run(self._handle, n_steps, self.step_index, self._stream),
+                      "acf_run")
+        self.step_index += n_steps
+        self._mirror_current.clear()
+
+    def step(self) -> None:
+        self.run(1)
+
+    def synchronize(self) -> None:
+        _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")
+
+    # ------------------------------------------------------------------ diagnostics
+    def energy_terms(self) -> np.ndarray:
+        """The seven FP64 device sums behind :meth:`energy` (see ``acf_energy_terms``)."""
+        self._flush()
+        terms = np.zeros(7)
+        _native.check(self._lib.acf_energy_terms(self._handle, float(self.grid.dx),
+                                                 _as_double_pointer(terms), self._stream),
+                      "acf_energy_terms")
+        return terms
+
+    def energy(self) -> float:
+        """Acoustic energy of the stored (p^n, v^{n-1/2}) pair in joules (``scheme.py:365-389``).
+
+        The sums are accumulated in FP64 on the device in either precision.
+        """
+        terms = self.energy_terms()
+        rho = float(self.medium.density)
+        c = float(self.medium.sound_speed)
+        potential = terms[0] / (2.0 * rho * c**2)
+        kinetic = 0.0
+        coupling = 0.0
+        for axis in range(3):
+            kinetic += 0.5 * rho * terms[1 + axis]
+            coupling += terms[4 + axis]
+        return float(self.grid.dx) ** 3 * (potential + kinetic - 0.5 * self.dt * coupling)
+
+    def launch_count(self) -> int:
+        return int(self._lib.acf_launch_count(self._handle))
+
+    def profile(self, enable: bool) -> None:
+        """Time each sweep with CUDA events during subsequent runs (step-by-step launches)."""
+        _native.check(self._lib.acf_profile_enable(self._handle, int(bool(enable))),
+                      "acf_profile_enable")
+
+    def profile_read(self) -> tuple[float, float, int]:
+        """(velocity-sweep ms, pressure-sweep ms, steps timed) since profiling was enabled."""
+        a, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _native.check(self._lib.acf_profile_read(self._handle, ctypes.byref(a), ctypes.byref(b),
+                                                 ctypes.byref(n)), "acf_profile_read")
+        return a.value, b.value, n.value
+
+    def close(self) -> None:
+        """Release the device state now instead of at garbage collection."""
+        self._finalizer()
+        self._mirror.clear()

@@ -1,0 +1,368 @@
+"""Throughput of the CUDA leapfrog on the large plain-method room, in Gcell-updates/s.
+
+Workload (one bench step = one full impulse-response run): 384^3 cells at dx = c/(10*4 kHz),
+float32, per-wall absorption drawn U(0.05, 0.5) (seeded), a 16-cell sponge on the two x faces,
+ISO 9613-1 air at 20 C / 50 % RH (three relaxation states: O2, N2, classical), a Gaussian pulse
+to 4 kHz at a seeded interior cell and four seeded receivers, 4000 leapfrog steps. The fields
+(2.5 GB) are far larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``value`` is device-timed (CUDA events on the launching stream, inputs resident in HBM); ``e2e``
+goes through the public API with host buffers: upload the full state from pinned host memory,
+run, read back the recordings and the final pressure. The reference arm times the reference's
+own compiled C backend (``oracle/_ref``) on the host cores over a bounded sample of the same
+workload. Multi-GPU runs are independent replicas of the room (one per rank, weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-updates/s"
+N_RECEIVERS = 4
+
+
+def workload(size: int, seed: int = 2):
+    from ac_fdtd_b200 import (
+        AbsorbingLayer,
+        AirAbsorption,
+        Grid,
+        WallAdmittances,
+        admittance_from_absorption,
+    )
+
+    rng = np.random.default_rng(seed)
+    dx = 343.2 / (10 * 4000.0)
+    grid = Grid(dx=dx, nx=size, ny=size, nz=size)
+    alphas = rng.uniform(0.05, 0.5, 6)
+    objects = dict(
+        walls=WallAdmittances(*[admittance_from_absorption(a) for a in alphas]),
+        absorbing_layer=AbsorbingLayer(thickness=16, faces=((0, 0), (0, 1))),
+        air_absorption=AirAbsorption(temperature=20.0, relative_humidity=50.0),
+    )
+    margin = max(1, min(24, size // 4))
+    cells = [tuple(int(v) for v in rng.integers(margin, size - margin, 3))
+             for _ in range(1 + N_RECEIVERS)]
+    points = [tuple((i + 0.5) * dx for i in c) for c in cells]
+    return grid, objects, points
+
+
+def config_dict(args, grid) -> dict:
+    return {
+        "workload": f"plain-method room {grid.nx}^3 fp32, 6 walls alpha~U(0.05,0.5), "
+                    f"16-cell sponge on 2 x faces, ISO air 20C/50%RH (3 relaxation states), "
+                    f"gaussian pulse 4 kHz, {N_RECEIVERS} receivers, {args.time_steps} steps "
+                    f"per bench step",
+        "cells": grid.n_cells,
+        "time_steps_per_bench_step": args.time_steps,
+        "relaxation_states": 3,
+        "dtype": "float32",
+        "l2": "inputs larger than L2 (fields 2.5 GB at 384^3); no flush",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm_max = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        loaded = [s for s in sm if s > 0] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(sm_max) if sm_max else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_cell() -> float | None:
+    """DRAM bytes per cell of one pressure-sweep launch, from the committed ncu summary."""
+    path = ROOT / "profiles" / "pressure_sweep_traffic.json"
+    if not path.exists():
+        return None
+    try:
+        return float(json.loads(path.read_text())["dram_bytes_per_cell"])
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(size: int, budget_s: float = 12.0) -> dict:
+    """The reference C backend on this host's cores, on a bounded sample of the workload."""
+    from oracle import ref_c
+
+    grid, objects, points = workload(size)
+    if ref_c.available() or ref_c.build():
+        from ac_fdtd_b200 import AIR
+
+        solver = ref_c.RefCSolver(grid, AIR, dtype=np.float32, threads=0, **objects)
+        kind = "reference"
+        cores = solver.threads
+    else:
+        from ac_fdtd_b200 import AIR
+        from oracle.leapfrog import OracleFDTD
+
+        solver = OracleFDTD(grid, AIR, dtype=np.float32, **objects)
+        kind = "port"
+        cores = 1
+    from ac_fdtd_b200 import gaussian_pulse
+
+    solver.add_volume_source(points[0], gaussian_pulse(4000, solver.dt, 4000.0))
+    for point in points[1:]:
+        solver.add_pressure_receiver(point)
+    solver.run(2)  # warm-up: first touch of the 1.6 GB of host fields
+    start = time.perf_counter()
+    solver.run(2)
+    per_step = (time.perf_counter() - start) / 2
+    steps = int(max(2, min(400, budget_s / max(per_step, 1e-6))))
+    start = time.perf_counter()
+    solver.run(steps)
+    elapsed = time.perf_counter() - start
+    value = grid.n_cells * steps / elapsed / 1e9
+    return {"value": value, "unit": METRIC, "cores": int(cores), "kind": kind,
+            "host_cpus": os.cpu_count(),
+            "sample": f"{size}^3 fp32 same room, {steps} leapfrog steps after 4 warm-up steps, "
+                      f"{elapsed:.1f} s"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    values = []
+    last = None
+    for _ in range(args.warmup):
+        cpu_baseline(args.size, budget_s=2.0)
+    for _ in range(args.steps):
+        last = cpu_baseline(args.size, budget_s=args.cpu_budget)
+        values.append(last["value"])
+    from ac_fdtd_b200 import Grid
+
+    grid = Grid(dx=343.2 / 40000.0, nx=args.size, ny=args.size, nz=args.size)
+    value = float(statistics.median(values))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": grid.n_cells / (value * 1e9) * 1e3 * args.time_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(args, grid),
+        "cpu_baseline": {**last, "value": value},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args) -> None:
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse, pinned_array
+
+    grid, objects, points = workload(args.size)
+    solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
+    solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
+    for point in points[1:]:
+        solver.add_pressure_receiver(point)
+    T = args.time_steps
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def one_run():
+        solver.step_index = 0
+        solver.run(T)
+
+    # ---- device-resident timing, with per-sweep CUDA events (the roofline numbers)
+    for _ in range(args.warmup):
+        one_run()
+    solver.profile(True)
+    launches0 = solver.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        start.record()
+        for _ in range(args.steps):
+            one_run()
+        end.record()
+        barrier()
+    elapsed_ms = max_over_ranks(start.elapsed_time(end))
+    launches = solver.launch_count() - launches0
+    vel_ms, pres_ms, timed_steps = solver.profile_read()
+    solver.profile(False)
+    cell_updates = grid.n_cells * T * args.steps * world
+    value = cell_updates / (elapsed_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel (pressure sweep)
+    R = 3
+    itemsize = 4
+    pressure_bytes = grid.n_cells * (5 + 2 * R) * itemsize
+    velocity_bytes = grid.n_cells * 7 * itemsize
+    pres_avg = pres_ms / max(timed_steps, 1)
+    vel_avg = vel_ms / max(timed_steps, 1)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = pressure_bytes / (pres_avg * 1e-3) / 1e9
+    traffic_per_cell = ncu_traffic_per_cell()
+    roofline = {
+        "bound": "hbm", "kernel": "pressure_sweep<float,layer,walls,3>",
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+        else "fallback 6650 GB/s",
+        "algorithmic_bytes_per_launch": pressure_bytes,
+        "bytes_per_cell": (5 + 2 * R) * itemsize,
+        "avg_launch_ms": pres_avg,
+        "traffic": None if traffic_per_cell is None else traffic_per_cell * grid.n_cells,
+        "velocity_sweep": {"avg_launch_ms": vel_avg, "bytes_per_cell": 7 * itemsize,
+                           "achieved": velocity_bytes / (vel_avg * 1e-3) / 1e9},
+        "step": {"bytes_per_cell": (12 + 2 * R) * itemsize,
+                 "achieved": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9,
+                 "frac": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9 / peak},
+    }
+
+    # ---- end to end through the public API with pinned host buffers
+    p0 = pinned_array(grid.shape, np.float32)
+    v0 = [pinned_array(grid.velocity_shape(a), np.float32) for a in range(3)]
+    psi0 = [pinned_array(grid.shape, np.float32) for _ in range(R)]
+    p_out = pinned_array(grid.shape, np.float32)
+    p0[...] = np.random.default_rng(rank).standard_normal(grid.shape).astype(np.float32) * 1e-3
+
+    def e2e_step():
+        solver.step_index = 0
+        h2d = solver.set_state(p=p0, velocity=v0, relaxation=psi0)
+        solver.run(T)
+        recorded = solver.recorded_pressure
+        d2h = solver.get_state(p=p_out) + recorded.nbytes
+        return h2d, d2h
+
+    for _ in range(min(args.warmup, 1)):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h2d, d2h = e2e_step()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = cell_updates / e2e_s / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(args, grid),
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "CudaAcousticFDTD.set_state (pinned) -> run(4000) -> recorded_pressure, get_state"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
+    elif rank == 0:
+        line["cpu_baseline"] = None
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=3)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--size", type=int, default=384)
+    parser.add_argument("--time-steps", type=int, default=4000)
+    parser.add_argument("--cpu-budget", type=float, default=12.0)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

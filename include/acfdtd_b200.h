@@ -1,0 +1,163 @@
+/* acfdtd_b200.h -- C ABI of the sm_100a staggered pressure-velocity leapfrog.
+ *
+ * One solver handle owns the device state of one rectangular room: the pressure p at cell
+ * centres, the three face velocities vx, vy, vz, and up to four ISO 9613-1 relaxation states.
+ * Every call returns an int status (ACF_OK on success); acf_last_error() gives a message for
+ * the last failure on the calling thread.
+ *
+ * Interfaces replaced (paths are inside the ac-fdtd project):
+ *   acf_create / acf_run      <- struct `acfdtd` + acfdtd_run(acfdtd*, int64_t step_offset)
+ *                                (src/ac_fdtd/c/acfdtd.c:56-97, 355-376). The reference borrows
+ *                                caller arrays for the duration of one call; here the handle owns
+ *                                device buffers and the caller moves state with acf_upload and
+ *                                acf_download.
+ *   acf_struct_size           <- acfdtd_struct_size (src/ac_fdtd/c/acfdtd.c:99), the ctypes
+ *                                mirror check of src/ac_fdtd/c_backend.py:194-200.
+ *   acf_is_double             <- acfdtd_is_double (src/ac_fdtd/c/acfdtd.c:101); the precision
+ *                                is a per-handle choice here, not a build option.
+ *   acf_energy_terms          <- AcousticFDTD.energy (src/ac_fdtd/scheme.py:365-389).
+ *
+ * Coefficients cross the boundary in FP64 and are rounded once to the solver precision, as
+ * the reference casts its FP64 host setup with `dtype.type(...)`/`astype(dtype)`
+ * (src/ac_fdtd/scheme.py:135-212).
+ *
+ * Streams are passed as `void*` (a cudaStream_t, 0 for the legacy default stream) so that FFI
+ * callers need no CUDA headers.
+ */
+#ifndef ACFDTD_B200_H
+#define ACFDTD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ACF_ABI_VERSION 1
+#define ACF_MAX_RELAXATION 4
+
+/* Status codes. */
+enum {
+    ACF_OK = 0,
+    ACF_ERR_ARGUMENT = 1,    /* a null pointer, a size out of range, an unknown field */
+    ACF_ERR_CUDA = 2,        /* a CUDA runtime call failed; see acf_last_error() */
+    ACF_ERR_MEMORY = 3,      /* device or pinned host allocation failed */
+    ACF_ERR_STATE = 4,       /* call not valid in the handle's current state */
+    ACF_ERR_NUMERIC = 5      /* non-finite value detected in the state */
+};
+
+/* Fields addressable by acf_upload / acf_download / acf_field_pointer. The relaxation state r
+ * is ACF_FIELD_PSI0 + r. Reference shapes (C order, z fastest): p (nx,ny,nz); vx (nx+1,ny,nz);
+ * vy (nx,ny+1,nz); vz (nx,ny,nz+1); psi_r (nx,ny,nz) -- src/ac_fdtd/grid.py:125-129. */
+enum {
+    ACF_FIELD_P = 0,
+    ACF_FIELD_VX = 1,
+    ACF_FIELD_VY = 2,
+    ACF_FIELD_VZ = 3,
+    ACF_FIELD_PSI0 = 4
+};
+
+typedef struct acf_solver acf_solver;
+typedef void *acf_stream;
+
+/* Everything the two sweeps need, computed on the host in FP64.
+ *
+ * Wall coefficients use a shell layout: for each of the six faces in the reference's FACES
+ * order ((0,0),(0,1),(1,0),(1,1),(2,0),(2,1); src/ac_fdtd/boundaries.py:73), a row-major
+ * (n_b, n_c) array over the two remaining axes in increasing order, holding for every cell on
+ * that face the pair (1/(1+a), a/(1+a)) where a is the sum over ALL faces touching the cell
+ * (src/ac_fdtd/boundaries.py:167-207). Pair (1, 0) marks a cell with no absorbing face. Pass
+ * NULL for all six when every wall is rigid.
+ *
+ * Layer profiles (src/ac_fdtd/boundaries.py:244-283): cell[a] has n_a entries (cell centres),
+ * face[a] has n_a + 1 (faces). Pass NULL for all six when there is no absorbing layer. */
+typedef struct acf_config {
+    int32_t nx, ny, nz;
+    int32_t precision;   /* bytes per element: 4 (float) or 8 (double) */
+    int32_t n_relax;     /* 0 .. ACF_MAX_RELAXATION */
+    int32_t reserved;
+    double vel_coef;     /* dt / (rho dx)                         scheme.py:135 */
+    double pres_coef;    /* rho c^2 dt / dx                       scheme.py:136-138 */
+    double src_coef;     /* rho c^2 dt                            scheme.py:141 */
+    double relax_scale;  /* dt * sum of gains                     scheme.py:189-191 */
+    double relax_decay[ACF_MAX_RELAXATION];  /* exp(-dt/tau)         scheme.py:172 */
+    double relax_mean[ACF_MAX_RELAXATION];   /* dt * mean weight     scheme.py:176,182 */
+    double relax_gain[ACF_MAX_RELAXATION];   /* rho c_r^2 Delta / dx scheme.py:177 */
+    const double *wall_shell[6];             /* 2 * n_b * n_c doubles each, or NULL */
+    const double *cell[3];                   /* n_a doubles each, or NULL */
+    const double *face[3];                   /* n_a + 1 doubles each, or NULL */
+} acf_config;
+
+/* Library identity. */
+int acf_abi_version(void);
+size_t acf_struct_size(void);          /* sizeof(acf_config), for FFI mirror checks */
+const char *acf_last_error(void);      /* message of the last failure on this thread */
+int acf_device_count(int *count);
+
+/* Handle lifetime. acf_create allocates zeroed device state on the current device. */
+int acf_create(const acf_config *config, acf_solver **out);
+int acf_destroy(acf_solver *solver);
+int acf_is_double(const acf_solver *solver);
+
+/* Sources (src/ac_fdtd/scheme.py:231-244, 360-363). `cell` holds reference flat indices
+ * (i*ny + j)*nz + k; `signal` is n rows of `stride` doubles, row s valid for `length[s]`
+ * samples. Sample n is added after the damping of step n, in the order given. Replaces the
+ * previous set. */
+int acf_set_sources(acf_solver *solver, int64_t n, const int64_t *cell, const int64_t *length,
+                    const double *signal, int64_t stride);
+
+/* Receivers (src/ac_fdtd/scheme.py:246-262, 294-296): receiver r records p[cell[r]] after
+ * every step whose absolute index is >= start_step[r]. Replaces the previous set; recordings of
+ * receivers that keep their position in the list are kept. */
+int acf_set_receivers(acf_solver *solver, int64_t n, const int64_t *cell,
+                      const int64_t *start_step);
+
+/* Copy `n` samples of receiver r, starting at absolute step `first_step`, to host memory
+ * `dst` (solver precision). Synchronous. */
+int acf_read_recording(acf_solver *solver, int64_t receiver, int64_t first_step, int64_t n,
+                       void *dst, acf_stream stream);
+
+/* Move one field between the reference layout (dense C order, solver precision) and the
+ * device. `src`/`dst` may be host (pageable or pinned) or device memory. Asynchronous on
+ * `stream` for pinned and device memory. */
+int acf_upload(acf_solver *solver, int field, const void *src, acf_stream stream);
+int acf_download(acf_solver *solver, int field, void *dst, acf_stream stream);
+
+/* Advance n_steps. step_offset is the absolute index of the first step, which selects the
+ * source samples (src/ac_fdtd/c/acfdtd.c:358-371). Asynchronous on `stream`. */
+int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream stream);
+
+/* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
+int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);
+
+/* The seven FP64 sums the reference energy is built from, for the stored (p^n, v^{n-1/2})
+ * pair (src/ac_fdtd/scheme.py:365-389): terms[0] = sum p^2; terms[1+a] = sum v_a^2 over all
+ * faces; terms[4+a] = sum over interior faces of v_a * (p_hi - p_lo) / dx. Synchronous. */
+int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream stream);
+
+/* Device address and element strides (z, y, x order reversed: strides[0] is the x stride)
+ * of one field in the internal padded layout. */
+int acf_field_pointer(acf_solver *solver, int field, void **ptr, int64_t strides[3]);
+
+/* Instrumentation: when enabled, acf_run launches step by step with CUDA events around each
+ * sweep and accumulates their device time. */
+int acf_profile_enable(acf_solver *solver, int32_t enable);
+int acf_profile_read(acf_solver *solver, double *velocity_ms, double *pressure_ms,
+                     int64_t *launches);
+
+/* Kernels launched by this handle since creation (sweeps, graph replays counted per kernel). */
+int64_t acf_launch_count(const acf_solver *solver);
+
+/* Block until all work queued on `stream` is done. */
+int acf_synchronize(acf_stream stream);
+
+/* Pinned host memory for fast state transfers. */
+int acf_host_alloc(size_t bytes, void **out);
+int acf_host_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACFDTD_B200_H */

@@ -1,0 +1,198 @@
+"""The CUDA backend against the oracle and the reference's golden outputs, on a GPU.
+
+The claim tested is the strong one: in float64 and in float32 the sweeps perform the same
+roundings as the NumPy reference, so fields, recordings and energies agree bit for bit
+(the reference's own backend parity tests ask for rtol 1e-11, ``tests/test_c_backend.py:51-65``).
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from ac_fdtd_b200 import AIR, CudaAcousticFDTD, WallAdmittances, gaussian_pulse
+from oracle.leapfrog import OracleFDTD
+from tests.cases import CONFIGURATIONS, GRID, RECEIVER, SOURCE, full_room, plain_room, prepare
+
+pytestmark = pytest.mark.gpu
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def paired(dtype=np.float64, steps_per_graph=64, **configuration):
+    oracle = prepare(OracleFDTD(GRID, AIR, dtype=dtype, **configuration))
+    cuda = prepare(CudaAcousticFDTD(GRID, dtype=dtype, steps_per_graph=steps_per_graph,
+                                    **configuration))
+    return oracle, cuda
+
+
+def assert_same_state(cuda, oracle):
+    np.testing.assert_array_equal(cuda.p, oracle.p)
+    for axis in range(3):
+        np.testing.assert_array_equal(cuda.velocity[axis], oracle.velocity[axis])
+    np.testing.assert_array_equal(cuda.recorded_pressure, oracle.recorded_pressure)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("name", list(CONFIGURATIONS))
+def test_matches_the_oracle_bitwise(name, dtype, golden_meta, golden_trajectories):
+    oracle, cuda = paired(dtype=dtype, **CONFIGURATIONS[name])
+    oracle.run(150)
+    cuda.run(150)
+    assert_same_state(cuda, oracle)
+    # ... and therefore the reference's own run, pinned in the golden fixtures.
+    key = f"{np.dtype(dtype).name}/{name}/"
+    assert digest(cuda.p) == golden_meta["trajectories"][key]["p"]
+    np.testing.assert_array_equal(cuda.recorded_pressure, golden_trajectories[key + "recording"])
+    if dtype == np.float64:
+        assert cuda.energy() == pytest.approx(oracle.energy(), rel=1e-12)
+    else:
+        assert cuda.energy() == pytest.approx(oracle.energy(), rel=1e-5)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_relaxation_states_match(dtype):
+    configuration = CONFIGURATIONS["everything at once"]
+    oracle, cuda = paired(dtype=dtype, **configuration)
+    oracle.run(77)
+    cuda.run(77)
+    states = cuda.relaxation_states
+    assert len(states) == len(oracle.relax) == 3
+    for got, (want, *_rest) in zip(states, oracle.relax, strict=True):
+        np.testing.assert_array_equal(got, want)
+
+
+def test_graphs_and_step_by_step_launches_agree_bitwise():
+    configuration = CONFIGURATIONS["everything at once"]
+    _, graphed = paired(steps_per_graph=16, **configuration)
+    _, direct = paired(steps_per_graph=0, **configuration)
+    graphed.run(150)
+    direct.run(150)
+    np.testing.assert_array_equal(graphed.p, direct.p)
+    np.testing.assert_array_equal(graphed.recorded_pressure, direct.recorded_pressure)
+
+
+def test_running_in_pieces_is_the_same_as_running_at_once():
+    _, whole = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16)
+    _, pieces = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16)
+    whole.run(120)
+    for n in (30, 1, 16, 40, 33):
+        pieces.run(n)
+    np.testing.assert_array_equal(pieces.p, whole.p)
+    np.testing.assert_array_equal(pieces.recorded_pressure, whole.recorded_pressure)
+
+
+def test_state_written_between_runs_is_used():
+    oracle, cuda = paired(walls=WallAdmittances.uniform(0.3))
+    oracle.run(20)
+    cuda.run(20)
+    rng = np.random.default_rng(9)
+    new_p = rng.standard_normal(GRID.shape)
+    new_vy = rng.standard_normal(GRID.velocity_shape(1)) * 1e-3
+    for solver in (oracle, cuda):
+        solver.p[:] = new_p
+        solver.velocity[1][:] = new_vy
+    oracle.run(25)
+    cuda.run(25)
+    assert_same_state(cuda, oracle)
+
+
+def test_sources_receivers_edge_cases():
+    """Two sources in one cell, a source longer than the run, a receiver added mid-run."""
+    oracle, cuda = paired(walls=WallAdmittances.uniform(0.1))
+    for solver in (oracle, cuda):
+        solver.add_volume_source(SOURCE, np.linspace(0.0, 1.0, 7))
+        solver.add_volume_source((0.05, 0.45, 0.4), np.ones(500))
+    oracle.run(30)
+    cuda.run(30)
+    late = [s.add_pressure_receiver((0.59, 0.01, 0.44)) for s in (oracle, cuda)]
+    assert late[0] == late[1] == 1
+    oracle.run(40)
+    cuda.run(40)
+    np.testing.assert_array_equal(cuda.p, oracle.p)
+    np.testing.assert_array_equal(cuda.recording(0), np.array(oracle.receivers[0][1]))
+    np.testing.assert_array_equal(cuda.recording(1), np.array(oracle.receivers[1][1]))
+    assert cuda.recording(1).size == 40
+    with pytest.raises(ValueError):
+        cuda.recorded_pressure  # noqa: B018 -- ragged recordings are refused, as NumPy does
+
+
+def test_receivers_record_the_same_samples_as_probing_by_hand():
+    solver = CudaAcousticFDTD(GRID, dtype=np.float64)
+    solver.add_volume_source(SOURCE, np.ones(50))
+    solver.add_pressure_receiver(RECEIVER)
+    solver.run(20)
+    solver.run(20)
+    recorded = solver.recorded_pressure
+    assert recorded.shape == (1, 40)
+    assert recorded[0, -1] == solver.p[GRID.cell_index(RECEIVER)]
+
+
+def test_rigid_walls_are_never_written_to():
+    solver = CudaAcousticFDTD(GRID)
+    solver.p[:] = np.random.default_rng(0).standard_normal(GRID.shape)
+    solver.run(20)
+    for axis in range(3):
+        wall = solver.velocity[axis]
+        lower = tuple(0 if a == axis else slice(None) for a in range(3))
+        upper = tuple(-1 if a == axis else slice(None) for a in range(3))
+        assert np.all(wall[lower] == 0.0)
+        assert np.all(wall[upper] == 0.0)
+
+
+def test_plain_room_matches_the_reference(golden_meta, golden_rooms):
+    meta = golden_meta["rooms"]["plain"]
+    grid, objects = plain_room(meta)
+    solver = CudaAcousticFDTD(grid, **objects)
+    solver.add_volume_source(meta["source"], golden_rooms["plain/signal"])
+    solver.add_pressure_receiver(meta["receiver"])
+    solver.run(meta["steps"])
+    np.testing.assert_array_equal(solver.recorded_pressure, golden_rooms["plain/numpy/recording"])
+    assert digest(solver.p) == golden_meta["rooms"]["plain/numpy/p"]
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_walls_sponge_air_room_matches_the_reference(dtype, golden_meta, golden_rooms):
+    meta = golden_meta["rooms"]["full"]
+    grid, objects = full_room(meta)
+    solver = CudaAcousticFDTD(grid, dtype=dtype, **objects)
+    solver.add_volume_source(meta["points"][0], gaussian_pulse(meta["steps"], solver.dt, 4000.0))
+    for point in meta["points"][1:]:
+        solver.add_pressure_receiver(point)
+    solver.run(meta["steps"])
+    name = np.dtype(dtype).name
+    np.testing.assert_array_equal(solver.recorded_pressure,
+                                  golden_rooms[f"full/{name}/numpy/recording"])
+    assert digest(solver.p) == golden_meta["rooms"][f"full/{name}/numpy/p"]
+    # The reference C backend differs from NumPy by rounding order only.
+    c = golden_rooms[f"full/{name}/c/recording"]
+    scale = np.max(np.abs(c))
+    tol = 1e-13 if dtype == np.float64 else 1e-5
+    assert np.max(np.abs(solver.recorded_pressure - c)) <= tol * scale
+
+
+def test_odd_and_degenerate_grids():
+    """Sizes that are not multiples of the 4-element vector, and 1-cell-wide ducts."""
+    from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid
+
+    for shape in ((1, 1, 9), (5, 1, 1), (3, 2, 7), (2, 3, 1), (7, 5, 13)):
+        grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
+        configuration = dict(walls=WallAdmittances(0.4, 0.1, 0.0, 0.7, 0.2, 0.0),
+                             absorbing_layer=AbsorbingLayer(thickness=2),
+                             air_absorption=AirAbsorption())
+        oracle = OracleFDTD(grid, AIR, **configuration)
+        cuda = CudaAcousticFDTD(grid, **configuration)
+        rng = np.random.default_rng(sum(shape))
+        initial = rng.standard_normal(shape)
+        point = tuple((n - 0.5) * 0.02 for n in shape)
+        for solver in (oracle, cuda):
+            solver.p[:] = initial
+            solver.add_volume_source((0.0, 0.0, 0.0), np.hanning(12))
+            solver.add_pressure_receiver(point)
+        oracle.run(40)
+        cuda.run(40)
+        assert_same_state(cuda, oracle)
