@@ -331,7 +331,8 @@ def run_ours(args) -> None:
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "path": "CudaAcousticFDTD.set_state (pinned) -> run(4000) -> recorded_pressure, get_state"},
+                "path": f"CudaAcousticFDTD.set_state (pinned host) -> run({T}) -> "
+                        "recorded_pressure, get_state (pinned host)"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
