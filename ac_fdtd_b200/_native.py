@@ -26,6 +26,7 @@ EXPORTED_SYMBOLS = (
     "acf_read_recording", "acf_upload", "acf_download", "acf_run", "acf_set_graph",
     "acf_energy_terms", "acf_field_pointer", "acf_profile_enable", "acf_profile_read",
     "acf_launch_count", "acf_synchronize", "acf_host_alloc", "acf_host_free",
+    "acf_energy_terms_noalloc",
 )
 
 
@@ -84,6 +85,9 @@ _SIGNATURES = {
     "acf_synchronize": (ctypes.c_int, [_P]),
     "acf_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "acf_host_free": (ctypes.c_int, [_P]),
+    "acf_energy_terms_noalloc": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                _P, _P]),
 }
 
 

@@ -772,6 +772,91 @@ void free_solver(acf_solver *h) {
 
 }  // namespace
 
+// ------------------------------------------------------------------------------------------
+// Energy sums without allocation (acf_energy_terms_noalloc). The fields are the caller's, in
+// the reference's dense C-order layout; the per-plane partial sums live in a static device
+// array instead of a cudaMalloc'd buffer. One block per x plane (planes 0..nx, vx has nx+1)
+// writes exactly one slot of 7 partials, so every slot the final pass reads was written by the
+// same call and nothing needs clearing between calls.
+
+static __device__ __align__(256) double g_noalloc_scratch[ACF_NOALLOC_MAX_PLANES * kEnergyTerms];
+
+template <typename T>
+static __global__ void __launch_bounds__(256) energy_dense_planes(const T *__restrict__ p,
+                                                           const T *__restrict__ vx,
+                                                           const T *__restrict__ vy,
+                                                           const T *__restrict__ vz, int nx,
+                                                           int ny, int nz, double inv_dx,
+                                                           double *partials) {
+    const int i = blockIdx.x;  // plane 0..nx
+    double acc[kEnergyTerms];
+#pragma unroll
+    for (int t = 0; t < kEnergyTerms; t++) acc[t] = 0.0;
+    const int64_t per_plane = (int64_t)(ny + 1) * (nz + 1);
+    for (int64_t n = threadIdx.x; n < per_plane; n += blockDim.x) {
+        const int k = (int)(n % (nz + 1));
+        const int j = (int)(n / (nz + 1));
+        const bool in_x = i < nx, in_y = j < ny, in_z = k < nz;
+        const int64_t c = ((int64_t)i * ny + j) * nz + k;  // p, vx, and the p neighbours
+        if (in_x && in_y && in_z) {
+            const double v = (double)p[c];
+            acc[0] += v * v;
+        }
+        if (in_y && in_z) {  // vx (nx+1, ny, nz): same index as p
+            const double v = (double)vx[c];
+            acc[1] += v * v;
+            if (i > 0 && i < nx)
+                acc[4] += v * (((double)p[c] - (double)p[c - (int64_t)ny * nz]) * inv_dx);
+        }
+        if (in_x && in_z) {  // vy (nx, ny+1, nz)
+            const double v = (double)vy[((int64_t)i * (ny + 1) + j) * nz + k];
+            acc[2] += v * v;
+            if (j > 0 && j < ny) acc[5] += v * (((double)p[c] - (double)p[c - nz]) * inv_dx);
+        }
+        if (in_x && in_y) {  // vz (nx, ny, nz+1)
+            const double v = (double)vz[((int64_t)i * ny + j) * (nz + 1) + k];
+            acc[3] += v * v;
+            if (k > 0 && k < nz) acc[6] += v * (((double)p[c] - (double)p[c - 1]) * inv_dx);
+        }
+    }
+    __shared__ double red[kEnergyTerms][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int t = 0; t < kEnergyTerms; t++) {
+        double v = acc[t];
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+        if (lane == 0) red[t][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kEnergyTerms) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x][w];
+        partials[(int64_t)i * kEnergyTerms + threadIdx.x] = v;
+    }
+}
+
+static constexpr int kNoallocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static double *g_noalloc_address[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device. In
+// host code the symbol itself is only a host-side stand-in and must never reach a kernel.
+static int noalloc_scratch(double **out) {
+    int device = 0;
+    ACF_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return fail(ACF_ERR_ARGUMENT, "device %d beyond the %d devices supported", device, kNoallocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[device]) {
+        void *address = nullptr;
+        ACF_CUDA(cudaGetSymbolAddress(&address, g_noalloc_scratch));
+        if (!address) return fail(ACF_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+        g_noalloc_address[device] = (double *)address;
+    }
+    *out = g_noalloc_address[device];
+    return ACF_OK;
+}
+
 // ==========================================================================================
 // C ABI
 
@@ -1110,6 +1195,38 @@ int acf_profile_read(acf_solver *h, double *velocity_ms, double *pressure_ms, in
 }
 
 int64_t acf_launch_count(const acf_solver *h) { return h ? h->launches : -1; }
+
+int acf_energy_terms_noalloc(const void *p, const void *vx, const void *vy, const void *vz,
+                             int32_t nx, int32_t ny, int32_t nz, int32_t precision, double dx,
+                             double *terms_device, acf_stream stream) {
+    if (!p || !vx || !vy || !vz || !terms_device) return fail(ACF_ERR_ARGUMENT, "null field or output pointer");
+    if (nx < 1 || ny < 1 || nz < 1)
+        return fail(ACF_ERR_ARGUMENT, "cell counts must be >= 1, got (%d, %d, %d)", nx, ny, nz);
+    if (precision != 4 && precision != 8)
+        return fail(ACF_ERR_ARGUMENT, "precision must be 4 or 8 bytes, got %d", precision);
+    if (!(dx > 0)) return fail(ACF_ERR_ARGUMENT, "dx must be positive");
+    if ((int64_t)nx + 1 > ACF_NOALLOC_MAX_PLANES)
+        return fail(ACF_ERR_ARGUMENT,
+                    "nx + 1 = %lld x planes exceeds the static scratch of %d planes; "
+                    "use acf_energy_terms for larger grids",
+                    (long long)nx + 1, ACF_NOALLOC_MAX_PLANES);
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const double inv_dx = 1.0 / dx;
+    if (precision == 8)
+        energy_dense_planes<double><<<nx + 1, 256, 0, st>>>((const double *)p, (const double *)vx,
+                                                            (const double *)vy, (const double *)vz,
+                                                            nx, ny, nz, inv_dx, scratch);
+    else
+        energy_dense_planes<float><<<nx + 1, 256, 0, st>>>((const float *)p, (const float *)vx,
+                                                           (const float *)vy, (const float *)vz,
+                                                           nx, ny, nz, inv_dx, scratch);
+    energy_finish<<<1, 32, 0, st>>>(scratch, nx + 1, terms_device);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
 
 int acf_synchronize(acf_stream stream) {
     ACF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));

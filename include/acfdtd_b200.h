@@ -136,6 +136,30 @@ int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);
  * faces; terms[4+a] = sum over interior faces of v_a * (p_hi - p_lo) / dx. Synchronous. */
 int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream stream);
 
+/* Energy sums without any allocation. No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory themselves or have the library allocate
+ * it: an application that hands this code a fixed device-memory budget from its own pool (an
+ * audio plug-in host, a game or simulation engine), or a real-time thread on which
+ * cudaMalloc/cudaFree may block or synchronize the device. It computes the same seven sums as
+ * acf_energy_terms, but from fields the caller already holds in device memory in the
+ * reference's dense C-order layout -- p (nx,ny,nz), vx (nx+1,ny,nz), vy (nx,ny+1,nz),
+ * vz (nx,ny,nz+1), `precision` 4 or 8 bytes -- and writes them to `terms_device`, 7 doubles
+ * in device memory. It needs no handle and calls no allocator.
+ *
+ * Its working memory is one static device array of ACF_NOALLOC_MAX_PLANES * 7 doubles
+ * (224 KiB), which every GPU that loads this library holds until the process exits. Grids
+ * with nx + 1 > ACF_NOALLOC_MAX_PLANES are refused with ACF_ERR_ARGUMENT. The first call on
+ * each device looks up that array's device address (with the device current); make that
+ * first call before any stream capture. All calls share the one array: calls that overlap on
+ * the GPU (two streams, or two host threads) race and must be serialized by the caller. Each
+ * call writes every scratch entry it later reads, so nothing is left to clear between calls.
+ * Asynchronous on `stream`. */
+#define ACF_NOALLOC_MAX_PLANES 4096
+int acf_energy_terms_noalloc(const void *p, const void *vx, const void *vy, const void *vz,
+                             int32_t nx, int32_t ny, int32_t nz, int32_t precision, double dx,
+                             double *terms_device, acf_stream stream);
+
 /* Device address and element strides (z, y, x order reversed: strides[0] is the x stride)
  * of one field in the internal padded layout. */
 int acf_field_pointer(acf_solver *solver, int field, void **ptr, int64_t strides[3]);
