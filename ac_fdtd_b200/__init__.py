@@ -8,6 +8,7 @@ accepted too.
 """
 
 from .air import AirAbsorption, RelaxationProcess
+from .batch import RoomBatch
 from .boundaries import (
     FACES,
     AbsorbingLayer,
@@ -32,6 +33,7 @@ __all__ = [
     "Grid",
     "Medium",
     "RelaxationProcess",
+    "RoomBatch",
     "WallAdmittances",
     "admittance_from_absorption",
     "band_limited_impulse",

@@ -26,7 +26,12 @@ EXPORTED_SYMBOLS = (
     "acf_read_recording", "acf_upload", "acf_download", "acf_run", "acf_set_graph",
     "acf_energy_terms", "acf_field_pointer", "acf_profile_enable", "acf_profile_read",
     "acf_launch_count", "acf_synchronize", "acf_host_alloc", "acf_host_free",
-    "acf_energy_terms_noalloc",
+    "acf_energy_terms_noalloc", "acf_set_launch",
+    "acf_batch_create", "acf_batch_destroy", "acf_batch_room_count", "acf_batch_set_sources",
+    "acf_batch_set_receivers", "acf_batch_read_recording", "acf_batch_upload",
+    "acf_batch_download", "acf_batch_run", "acf_batch_set_graph", "acf_batch_set_launch",
+    "acf_batch_energy_terms", "acf_batch_profile_enable", "acf_batch_profile_read",
+    "acf_batch_launch_count",
 )
 
 
@@ -77,6 +82,7 @@ _SIGNATURES = {
     "acf_download": (ctypes.c_int, [_P, ctypes.c_int, _P, _P]),
     "acf_run": (ctypes.c_int, [_P, _I64, _I64, _P]),
     "acf_set_graph": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_set_launch": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "acf_energy_terms": (ctypes.c_int, [_P, ctypes.c_double, _DP, _P]),
     "acf_field_pointer": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), _I64P]),
     "acf_profile_enable": (ctypes.c_int, [_P, ctypes.c_int32]),
@@ -88,6 +94,22 @@ _SIGNATURES = {
     "acf_energy_terms_noalloc": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                                 _P, _P]),
+    "acf_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(AcfConfig),
+                                        ctypes.POINTER(_P)]),
+    "acf_batch_destroy": (ctypes.c_int, [_P]),
+    "acf_batch_room_count": (ctypes.c_int, [_P]),
+    "acf_batch_set_sources": (ctypes.c_int, [_P, ctypes.c_int32, _I64, _I64P, _I64P, _DP, _I64]),
+    "acf_batch_set_receivers": (ctypes.c_int, [_P, ctypes.c_int32, _I64, _I64P, _I64P]),
+    "acf_batch_read_recording": (ctypes.c_int, [_P, ctypes.c_int32, _I64, _I64, _I64, _P, _P]),
+    "acf_batch_upload": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int, _P, _P]),
+    "acf_batch_download": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int, _P, _P]),
+    "acf_batch_run": (ctypes.c_int, [_P, _I64, _I64, _P]),
+    "acf_batch_set_graph": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_batch_set_launch": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "acf_batch_energy_terms": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, _DP, _P]),
+    "acf_batch_profile_enable": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_batch_profile_read": (ctypes.c_int, [_P, _DP, _DP, _I64P]),
+    "acf_batch_launch_count": (ctypes.c_int64, [_P]),
 }
 
 

@@ -1,0 +1,94 @@
+"""Pick the sweeps' launch geometry by timing the candidates on the device.
+
+The geometry -- threads per block and how many consecutive x planes a block marches through --
+changes only the speed, never the result (every cell is computed by one thread with the same
+arithmetic). Timing runs on a throwaway solver with the same shape, precision and physics so
+the caller's state is untouched. Results are cached per process, keyed by the shape class,
+dtype and which terms are active, and optionally in a JSON file named by ``ACF_TUNE_CACHE``.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["CANDIDATES", "tune", "apply_tuned"]
+
+#: (threads per block, planes per block) tried by default.
+CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
+
+_cache: dict[str, tuple[int, int]] = {}
+
+
+def _key(solver) -> str:
+    nx, ny, nz = solver._shape
+    block = solver.coefficients
+    return json.dumps([nx, ny, nz, solver.dtype.name, block.n_relax,
+                       block.layer_cell is not None, block.wall_shell is not None])
+
+
+def _load_file() -> dict:
+    path = os.environ.get("ACF_TUNE_CACHE")
+    if path and Path(path).exists():
+        try:
+            return json.loads(Path(path).read_text())
+        except (OSError, ValueError):
+            return {}
+    return {}
+
+
+def _store_file(key: str, value) -> None:
+    path = os.environ.get("ACF_TUNE_CACHE")
+    if not path:
+        return
+    data = _load_file()
+    data[key] = list(value)
+    Path(path).write_text(json.dumps(data, indent=1))
+
+
+def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2):
+    """Time each candidate on a scratch twin of ``solver``; return (best, {candidate: ms/step})."""
+    from .solver import CudaAcousticFDTD
+
+    twin = CudaAcousticFDTD(solver.grid, solver.medium, solver.courant, solver.dtype,
+                            solver.walls, solver.absorbing_layer, solver.air_absorption,
+                            steps_per_graph=0)
+    twin.p[:] = np.random.default_rng(0).standard_normal(twin.p.shape) * 1e-3
+    timings = {}
+    try:
+        for candidate in candidates:
+            try:
+                twin.set_launch(*candidate)
+            except RuntimeError:
+                continue
+            twin.run(2)
+            best = float("inf")
+            for _ in range(repeats):
+                twin.profile(True)
+                twin.run(steps)
+                velocity_ms, pressure_ms, n = twin.profile_read()
+                twin.profile(False)
+                best = min(best, (velocity_ms + pressure_ms) / max(n, 1))
+            timings[candidate] = best
+    finally:
+        twin.close()
+    winner = min(timings, key=timings.get)
+    return winner, timings
+
+
+def apply_tuned(solver, candidates=CANDIDATES):
+    """Set the fastest geometry for this configuration (tuning once per shape class)."""
+    key = _key(solver)
+    if key not in _cache:
+        stored = _load_file().get(key)
+        if stored:
+            _cache[key] = tuple(stored)
+        else:
+            winner, _ = tune(solver, candidates)
+            _cache[key] = winner
+            _store_file(key, winner)
+    solver.set_launch(*_cache[key])
+    return _cache[key]

@@ -3,21 +3,27 @@
 // One time step is two HBM-bound sweeps over the grid (ac-fdtd: src/ac_fdtd/scheme.py:285-296,
 // src/ac_fdtd/c/acfdtd.c:110-190,342-376):
 //
-//   (a) velocity_sweep: v_a -= c_v (p_hi - p_lo) on interior faces, then the absorbing-layer
-//       damping x, y, z in that order on every face (scheme.py:287-290,298-311).
-//   (b) pressure_sweep: div v, the relaxation states, p -= c_p div, the time-centred wall
-//       closed form, the layer damping, the volume sources and the receiver gather, all in the
+//   (a) velocity: v_a -= c_v (p_hi - p_lo) on interior faces, then the absorbing-layer damping
+//       x, y, z in that order on every face (scheme.py:287-290,298-311).
+//   (b) pressure: div v, the relaxation states, p -= c_p div, the time-centred wall closed
+//       form, the layer damping, the volume sources and the receiver gather, all in the
 //       registers of the thread that owns the cell (scheme.py:291-296,313-363).
 //
 // Arithmetic order follows the NumPy reference operation by operation and the library is
 // built with -fmad=false, so no multiply-add is contracted: both precisions reproduce the
-// reference's own float64/float32 arithmetic.
+// reference's own float64/float32 arithmetic bit for bit.
 //
-// Layout in HBM: every field uses the same padded geometry, (nx+1) planes of (ny+1) rows of
-// pz elements, pz = nz+1 rounded up to a multiple of 8. Element (i,j,k) of any field is at
-// (i*(ny+1) + j)*pz + k, so vx's extra plane, vy's extra row and vz's extra face all fit and a
-// neighbour on any axis is a constant stride away. Rows start on 32-byte boundaries, which
+// Layout in HBM: every field of a room uses the same padded geometry, (nx+1) planes of (ny+1)
+// rows of pz elements, pz = nz+1 rounded up to a multiple of 8. Element (i,j,k) of any field is
+// at (i*(ny+1) + j)*pz + k, so vx's extra plane, vy's extra row and vz's extra face all fit and
+// a neighbour on any axis is a constant stride away. Rows start on 32-byte boundaries, which
 // keeps every 4-element group of a thread a single aligned vector access.
+//
+// Two launch forms share the per-column code:
+//   * one room: a 2D grid of (z chunk, y row) threads, each block marching `planes` x planes;
+//   * a batch of rooms of different sizes packed in one arena: a persistent grid walks a flat
+//     tile table (room, first (row, chunk) pair, plane range); each CTA stages its room's
+//     description in shared memory. One launch per sweep covers every room.
 
 #include <cuda_runtime.h>
 
@@ -72,6 +78,11 @@ struct Vec4<float> {
     __device__ __forceinline__ static void store(float *__restrict__ a, const float v[4]) {
         *reinterpret_cast<float4 *>(a) = make_float4(v[0], v[1], v[2], v[3]);
     }
+    // Read-only path: only for arrays no thread writes during the kernel.
+    __device__ __forceinline__ static void ldg(const float *__restrict__ a, float v[4]) {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(a));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
 };
 
 template <>
@@ -85,13 +96,18 @@ struct Vec4<double> {
         *reinterpret_cast<double2 *>(a) = make_double2(v[0], v[1]);
         *reinterpret_cast<double2 *>(a + 2) = make_double2(v[2], v[3]);
     }
+    __device__ __forceinline__ static void ldg(const double *__restrict__ a, double v[4]) {
+        const double2 t0 = __ldg(reinterpret_cast<const double2 *>(a));
+        const double2 t1 = __ldg(reinterpret_cast<const double2 *>(a + 2));
+        v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+    }
 };
 
 // ------------------------------------------------------------------------------------------
-// Kernel parameters (passed by value).
+// What the sweeps read about one room. Plain data, identical on host and device.
 
 template <typename T>
-struct StepParams {
+struct Room {
     int32_t nx, ny, nz, nchunks;
     int64_t pz, plane, field;      // row pitch, plane pitch, elements per field
     T *p, *vx, *vy, *vz, *psi;     // psi: n_relax fields back to back
@@ -101,142 +117,131 @@ struct StepParams {
     const T *face[3];              // layer profiles at faces
     const T *shell[6];             // wall pairs (1/(1+a), a/(1+a)) per face cell
     int32_t n_src;
+    int32_t n_rec;
     const int64_t *src_off;        // padded offsets
     const int64_t *src_len;
     const T *src_sig;
     int64_t src_stride;
-    int32_t n_rec;
     const int64_t *rec_off;        // padded offsets
     const int64_t *rec_start;      // first absolute step recorded
     T *rec;
     int64_t rec_stride, rec_origin;
+};
+
+template <typename T>
+struct StepParams {
+    Room<T> room;
     const int64_t *step_base;      // absolute step of local step 0, in device memory
     int32_t local_step;
+    int32_t planes;                // consecutive x planes marched by one block
+};
+
+// One unit of work of a batched sweep: up to blockDim.x consecutive (row, chunk) pairs of one
+// room, over the x planes [i_begin, i_end).
+struct Tile {
+    int32_t room, first, count, i_begin, i_end, reserved;
+};
+
+template <typename T>
+struct BatchParams {
+    const Room<T> *rooms;
+    const Tile *tiles;
+    int32_t n_tiles;
+    int32_t local_step;
+    const int64_t *step_base;
 };
 
 // ------------------------------------------------------------------------------------------
-// (a) velocity sweep. Thread (chunk c, row j) marches over planes i. Each cell owns the lower
-// face of each axis; the far boundary faces (x = nx, y = ny, z = nz) are only ever damped.
+// (a) velocity, one (row j, chunk c) column over the x planes [i_begin, i_end). Each cell owns
+// the lower face of each axis; the far boundary faces (x = nx, y = ny, z = nz) are only ever
+// damped. Every global load of a plane is issued before its first store, so a thread has all
+// of its fields in flight at once (a store may alias a later load, which would otherwise
+// serialise them); p of the previous plane stays in registers.
 
 template <typename T, bool LAYER>
-__global__ void __launch_bounds__(256) velocity_sweep(const StepParams<T> s) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= s.nchunks || j >= s.ny) return;
+__device__ __forceinline__ void velocity_column(const Room<T> &s, int i_begin, int i_end, int j,
+                                                int c) {
     const int k0 = c * kVec;
     const T cv = s.cv;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    T Pm[kVec];  // p at plane i - 1
+    if (i_begin > 0) Vec4<T>::ldg(s.p + (int64_t)(i_begin - 1) * s.plane + column, Pm);
 
-    T fk_cell[kVec], fk_face[kVec];
-    T fj_cell = T(1), fj_face = T(1);
-    if (LAYER) {
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        // ---- loads
+        T P[kVec], Py[kVec], VX[kVec], VY[kVec], VZ[kVec];
+        Vec4<T>::ldg(s.p + base, P);
+        if (j > 0) Vec4<T>::ldg(s.p + base - s.pz, Py);
+        const T below = (k0 > 0) ? __ldg(s.p + base - 1) : T(0);
+        Vec4<T>::load(s.vx + base, VX);
+        Vec4<T>::load(s.vy + base, VY);
+        Vec4<T>::load(s.vz + base, VZ);
+
+        // ---- compute, in the reference's order: gradient update, then x, y, z damping
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
-            const int k = min(k0 + e, s.nz - 1);
-            fk_cell[e] = s.cell[2][k];
-            fk_face[e] = s.face[2][min(k0 + e, s.nz)];
+            const int k = k0 + e;
+            if (k < s.nz) {
+                T vx = VX[e], vy = VY[e], vz = VZ[e];
+                if (i > 0) vx = vx - cv * (P[e] - Pm[e]);
+                if (j > 0) vy = vy - cv * (P[e] - Py[e]);
+                if (k > 0) vz = vz - cv * (P[e] - (e == 0 ? below : P[e - 1]));
+                if (LAYER) {
+                    const T fi_cell = __ldg(s.cell[0] + i), fi_face = __ldg(s.face[0] + i);
+                    const T fj_cell = __ldg(s.cell[1] + j), fj_face = __ldg(s.face[1] + j);
+                    const T fk_cell = __ldg(s.cell[2] + k), fk_face = __ldg(s.face[2] + k);
+                    vx = vx * fi_face;
+                    vx = vx * fj_cell;
+                    vx = vx * fk_cell;
+                    vy = vy * fi_cell;
+                    vy = vy * fj_face;
+                    vy = vy * fk_cell;
+                    vz = vz * fi_cell;
+                    vz = vz * fj_cell;
+                    vz = vz * fk_face;
+                }
+                VX[e] = vx;
+                VY[e] = vy;
+                VZ[e] = vz;
+            }
         }
-        fj_cell = s.cell[1][j];
-        fj_face = s.face[1][j];
-    }
 
-    for (int i = blockIdx.z; i < s.nx; i += gridDim.z) {
-        const int64_t base = (int64_t)i * s.plane + (int64_t)j * s.pz + k0;
-        T fi_cell = T(1), fi_face = T(1);
-        if (LAYER) {
-            fi_cell = s.cell[0][i];
-            fi_face = s.face[0][i];
-        }
-        T P[kVec];
-        Vec4<T>::load(s.p + base, P);
+        // ---- stores
+        Vec4<T>::store(s.vx + base, VX);
+        Vec4<T>::store(s.vy + base, VY);
+        Vec4<T>::store(s.vz + base, VZ);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Pm[e] = P[e];
 
-        // vx, lower x face of cell (i, j, k): interior for i >= 1.
-        {
-            T V[kVec];
-            Vec4<T>::load(s.vx + base, V);
-            T Q[kVec];
-            if (i > 0) Vec4<T>::load(s.p + base - s.plane, Q);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                if (k0 + e < s.nz) {
-                    T v = V[e];
-                    if (i > 0) v = v - cv * (P[e] - Q[e]);
-                    if (LAYER) {
-                        v = v * fi_face;
-                        v = v * fj_cell;
-                        v = v * fk_cell[e];
-                    }
-                    V[e] = v;
-                }
-            }
-            Vec4<T>::store(s.vx + base, V);
-        }
-        // vy, lower y face: interior for j >= 1.
-        {
-            T V[kVec];
-            Vec4<T>::load(s.vy + base, V);
-            T Q[kVec];
-            if (j > 0) Vec4<T>::load(s.p + base - s.pz, Q);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                if (k0 + e < s.nz) {
-                    T v = V[e];
-                    if (j > 0) v = v - cv * (P[e] - Q[e]);
-                    if (LAYER) {
-                        v = v * fi_cell;
-                        v = v * fj_face;
-                        v = v * fk_cell[e];
-                    }
-                    V[e] = v;
-                }
-            }
-            Vec4<T>::store(s.vy + base, V);
-        }
-        // vz, lower z face: interior for k >= 1.
-        {
-            T V[kVec];
-            Vec4<T>::load(s.vz + base, V);
-            const T below = (k0 > 0) ? s.p[base - 1] : T(0);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                const int k = k0 + e;
-                if (k < s.nz) {
-                    T v = V[e];
-                    if (k > 0) v = v - cv * (P[e] - (e == 0 ? below : P[e - 1]));
-                    if (LAYER) {
-                        v = v * fi_cell;
-                        v = v * fj_cell;
-                        v = v * fk_face[e];
-                    }
-                    V[e] = v;
-                }
-            }
-            Vec4<T>::store(s.vz + base, V);
-        }
-        // Far boundary faces: never updated, but the reference damps them with its slabs.
+        // Far boundary faces (x = nx, y = ny, z = nz): never updated, but the reference damps
+        // them with its slabs. Only the threads on those faces do this, after their stores.
         if (LAYER) {
+            const T fi_cell = __ldg(s.cell[0] + i);
+            const T fj_cell = __ldg(s.cell[1] + j);
             if (i == s.nx - 1) {
                 T V[kVec];
                 Vec4<T>::load(s.vx + base + s.plane, V);
-                const T f = s.face[0][s.nx];
+                const T f = __ldg(s.face[0] + s.nx);
 #pragma unroll
                 for (int e = 0; e < kVec; e++)
                     if (k0 + e < s.nz) {
                         T v = V[e] * f;
                         v = v * fj_cell;
-                        V[e] = v * fk_cell[e];
+                        V[e] = v * __ldg(s.cell[2] + k0 + e);
                     }
                 Vec4<T>::store(s.vx + base + s.plane, V);
             }
             if (j == s.ny - 1) {
                 T V[kVec];
                 Vec4<T>::load(s.vy + base + s.pz, V);
-                const T f = s.face[1][s.ny];
+                const T f = __ldg(s.face[1] + s.ny);
 #pragma unroll
                 for (int e = 0; e < kVec; e++)
                     if (k0 + e < s.nz) {
                         T v = V[e] * fi_cell;
                         v = v * f;
-                        V[e] = v * fk_cell[e];
+                        V[e] = v * __ldg(s.cell[2] + k0 + e);
                     }
                 Vec4<T>::store(s.vy + base + s.pz, V);
             }
@@ -244,18 +249,18 @@ __global__ void __launch_bounds__(256) velocity_sweep(const StepParams<T> s) {
                 T *top = s.vz + (base - k0) + s.nz;
                 T v = *top * fi_cell;
                 v = v * fj_cell;
-                *top = v * s.face[2][s.nz];
+                *top = v * __ldg(s.face[2] + s.nz);
             }
         }
     }
 }
 
 // ------------------------------------------------------------------------------------------
-// (b) pressure sweep.
+// (b) pressure, one column. The velocities are read-only here; p and psi are read and written
+// by their owning thread only. vx of the upper face is carried into the next plane's lower face.
 
 template <typename T>
-__device__ __forceinline__ bool wall_pair(const StepParams<T> &s, int i, int j, int k, T &fu,
-                                          T &fp) {
+__device__ __forceinline__ bool wall_pair(const Room<T> &s, int i, int j, int k, T &fu, T &fp) {
     const T *entry;
     if (i == 0) entry = s.shell[0] + 2 * ((int64_t)j * s.nz + k);
     else if (i == s.nx - 1) entry = s.shell[1] + 2 * ((int64_t)j * s.nz + k);
@@ -264,89 +269,78 @@ __device__ __forceinline__ bool wall_pair(const StepParams<T> &s, int i, int j, 
     else if (k == 0) entry = s.shell[4] + 2 * ((int64_t)i * s.ny + j);
     else if (k == s.nz - 1) entry = s.shell[5] + 2 * ((int64_t)i * s.ny + j);
     else return false;
-    fu = entry[0];
-    fp = entry[1];
+    fu = __ldg(entry);
+    fp = __ldg(entry + 1);
     return fp != T(0) || fu != T(1);
 }
 
 template <typename T, bool LAYER, bool WALLS, int NR>
-__global__ void __launch_bounds__(256) pressure_sweep(const StepParams<T> s) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= s.nchunks || j >= s.ny) return;
+__device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, int i_end, int j,
+                                                int c, int64_t step) {
     const int k0 = c * kVec;
     const bool any_point = (s.n_src | s.n_rec) != 0;
-    const int64_t step = any_point ? (*s.step_base + s.local_step) : 0;
+    const bool has_above = k0 + kVec <= s.nz;
 
     T fk[kVec];
     T fj = T(1);
     if (LAYER) {
 #pragma unroll
-        for (int e = 0; e < kVec; e++) fk[e] = s.cell[2][min(k0 + e, s.nz - 1)];
-        fj = s.cell[1][j];
+        for (int e = 0; e < kVec; e++) fk[e] = __ldg(s.cell[2] + min(k0 + e, s.nz - 1));
+        fj = __ldg(s.cell[1] + j);
     }
     const T cp = s.cp;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    T XL[kVec];  // vx on the lower x face of the current plane
+    Vec4<T>::ldg(s.vx + (int64_t)i_begin * s.plane + column, XL);
 
-    for (int i = blockIdx.z; i < s.nx; i += gridDim.z) {
-        const int64_t base = (int64_t)i * s.plane + (int64_t)j * s.pz + k0;
-
-        // Divergence, summed x, then y, then z as the reference does (scheme.py:317-322).
-        T D[kVec];
-        {
-            T A[kVec], B[kVec];
-            Vec4<T>::load(s.vx + base, A);
-            Vec4<T>::load(s.vx + base + s.plane, B);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) D[e] = B[e] - A[e];
-            Vec4<T>::load(s.vy + base, A);
-            Vec4<T>::load(s.vy + base + s.pz, B);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) D[e] = D[e] + (B[e] - A[e]);
-            Vec4<T>::load(s.vz + base, A);
-            const T above = (k0 + kVec <= s.nz) ? s.vz[base + kVec] : T(0);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) D[e] = D[e] + ((e + 1 < kVec ? A[e + 1] : above) - A[e]);
-        }
-
-        T P[kVec], Pn[kVec];
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        // ---- loads
+        T XH[kVec], YL[kVec], YH[kVec], Z[kVec], P[kVec], S[NR > 0 ? NR : 1][kVec];
+        Vec4<T>::ldg(s.vx + base + s.plane, XH);
+        Vec4<T>::ldg(s.vy + base, YL);
+        Vec4<T>::ldg(s.vy + base + s.pz, YH);
+        Vec4<T>::ldg(s.vz + base, Z);
+        const T above = has_above ? __ldg(s.vz + base + kVec) : T(0);
         Vec4<T>::load(s.p + base, P);
 #pragma unroll
-        for (int e = 0; e < kVec; e++) Pn[e] = P[e];
+        for (int r = 0; r < NR; r++) Vec4<T>::load(s.psi + r * s.field + base, S[r]);
+        const T fi = LAYER ? __ldg(s.cell[0] + i) : T(1);
 
-        // Relaxation states (scheme.py:337-358), then p -= c_p div (scheme.py:325-326).
+        // ---- divergence x, then y, then z (scheme.py:317-322)
+        T D[kVec];
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            T S[kVec];
-            T *psi = s.psi + r * s.field + base;
-            Vec4<T>::load(psi, S);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                if (k0 + e < s.nz) {
-                    const T target = D[e] * s.gain[r];
-                    const T offset = S[e] - target;
-                    S[e] = offset * s.decay[r] + target;
-                    Pn[e] = Pn[e] + offset * s.mean[r];
-                }
-            }
-            Vec4<T>::store(psi, S);
+        for (int e = 0; e < kVec; e++) {
+            D[e] = XH[e] - XL[e];
+            D[e] = D[e] + (YH[e] - YL[e]);
+            D[e] = D[e] + ((e + 1 < kVec ? Z[e + 1] : above) - Z[e]);
         }
 
-        const T fi = LAYER ? s.cell[0][i] : T(1);
+        T Pn[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
             const int k = k0 + e;
-            if (k >= s.nz) continue;
-            T pe = Pn[e];
-            if (NR > 0) pe = pe + D[e] * s.relax_scale;
-            pe = pe - D[e] * cp;
-            if (WALLS) {
-                T fu, fp;
-                if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
-            }
-            if (LAYER) {
-                pe = pe * fi;
-                pe = pe * fj;
-                pe = pe * fk[e];
+            T pe = P[e];
+            if (k < s.nz) {
+                // relaxation states (scheme.py:337-358), then p -= c_p div (scheme.py:325-326)
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T target = D[e] * s.gain[r];
+                    const T offset = S[r][e] - target;
+                    S[r][e] = offset * s.decay[r] + target;
+                    pe = pe + offset * s.mean[r];
+                }
+                if (NR > 0) pe = pe + D[e] * s.relax_scale;
+                pe = pe - D[e] * cp;
+                if (WALLS) {
+                    T fu, fp;
+                    if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
+                }
+                if (LAYER) {
+                    pe = pe * fi;
+                    pe = pe * fj;
+                    pe = pe * fk[e];
+                }
             }
             Pn[e] = pe;
         }
@@ -362,7 +356,11 @@ __global__ void __launch_bounds__(256) pressure_sweep(const StepParams<T> s) {
                 }
             }
         }
+
+        // ---- stores
         Vec4<T>::store(s.p + base, Pn);
+#pragma unroll
+        for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, S[r]);
 
         // Receivers read the finished p (scheme.py:294-296).
         if (any_point) {
@@ -377,6 +375,90 @@ __global__ void __launch_bounds__(256) pressure_sweep(const StepParams<T> s) {
                 }
             }
         }
+#pragma unroll
+        for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// One room: 2D grid of (chunk, row) threads; blockIdx.z selects a group of `planes` x planes.
+
+template <typename T, bool LAYER>
+__global__ void __launch_bounds__(256) velocity_sweep(const StepParams<T> p) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= p.room.nchunks || j >= p.room.ny) return;
+    const int i_begin = blockIdx.z * p.planes;
+    velocity_column<T, LAYER>(p.room, i_begin, min(p.room.nx, i_begin + p.planes), j, c);
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 4)) pressure_sweep(const StepParams<T> p) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= p.room.nchunks || j >= p.room.ny) return;
+    const bool any_point = (p.room.n_src | p.room.n_rec) != 0;
+    const int64_t step = any_point ? (*p.step_base + p.local_step) : 0;
+    const int i_begin = blockIdx.z * p.planes;
+    pressure_column<T, LAYER, WALLS, NR>(p.room, i_begin, min(p.room.nx, i_begin + p.planes), j,
+                                         c, step);
+}
+
+// ------------------------------------------------------------------------------------------
+// Batches: a persistent grid walks the tile table with a static stride; no CTA waits on any
+// other. A CTA copies the description of its tile's room into shared memory when the room
+// changes (every thread takes part in the copy and both barriers, so they stay uniform).
+
+template <typename T>
+__device__ __forceinline__ void stage_room(const Room<T> *src, Room<T> *dst) {
+    static_assert(sizeof(Room<T>) % sizeof(int) == 0, "Room must be a whole number of words");
+    const int *from = reinterpret_cast<const int *>(src);
+    int *to = reinterpret_cast<int *>(dst);
+    for (int w = threadIdx.x; w < (int)(sizeof(Room<T>) / sizeof(int)); w += blockDim.x)
+        to[w] = __ldg(from + w);
+}
+
+template <typename T, bool LAYER>
+__global__ void __launch_bounds__(256) velocity_batch(const BatchParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(Room<T>)];
+    Room<T> *room = reinterpret_cast<Room<T> *>(raw);
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_room(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            velocity_column<T, LAYER>(*room, tile.i_begin, tile.i_end, pair / room->nchunks,
+                                      pair % room->nchunks);
+        }
+    }
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) pressure_batch(const BatchParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(Room<T>)];
+    Room<T> *room = reinterpret_cast<Room<T> *>(raw);
+    const int64_t step = *b.step_base + b.local_step;
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_room(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            pressure_column<T, LAYER, WALLS, NR>(*room, tile.i_begin, tile.i_end,
+                                                 pair / room->nchunks, pair % room->nchunks,
+                                                 step);
+        }
     }
 }
 
@@ -384,11 +466,11 @@ __global__ void set_step_base(int64_t *base, int64_t value) { *base = value; }
 __global__ void bump_step_base(int64_t *base, int64_t by) { *base += by; }
 
 // ------------------------------------------------------------------------------------------
-// Energy terms, FP64 accumulation (scheme.py:365-389). Two passes, fixed order: block partial
-// sums into a scratch array, then one block sums the partials.
+// Energy terms of one room, FP64 accumulation (scheme.py:365-389). Two passes, fixed order:
+// block partial sums into a scratch array, then one block sums the partials.
 
 template <typename T>
-__global__ void __launch_bounds__(256) energy_partials(const StepParams<T> s, double inv_dx,
+__global__ void __launch_bounds__(256) energy_partials(const Room<T> s, double inv_dx,
                                                        double *partials) {
     double acc[kEnergyTerms];
 #pragma unroll
@@ -449,325 +531,6 @@ __global__ void energy_finish(const double *partials, int n_blocks, double *out)
         for (int b = 0; b < n_blocks; b++) v += partials[b * kEnergyTerms + threadIdx.x];
         out[threadIdx.x] = v;
     }
-}
-
-// ------------------------------------------------------------------------------------------
-// Host side.
-
-struct DeviceGuard {
-    int previous = -1;
-    explicit DeviceGuard(int device) {
-        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
-        if (previous != device) cudaSetDevice(device);
-    }
-    ~DeviceGuard() {
-        int now = -1;
-        if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous)
-            cudaSetDevice(previous);
-    }
-};
-
-inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
-
-}  // namespace
-
-struct acf_solver {
-    int device = 0;
-    int precision = 8;
-    int32_t nx = 0, ny = 0, nz = 0, n_relax = 0;
-    int64_t pz = 0, plane = 0, field = 0;
-    bool has_layer = false, has_walls = false;
-    double coef[4] = {0, 0, 0, 0};   // cv, cp, cs, relax_scale
-    double decay[ACF_MAX_RELAXATION] = {}, mean[ACF_MAX_RELAXATION] = {},
-           gain[ACF_MAX_RELAXATION] = {};
-
-    void *state = nullptr;           // p, vx, vy, vz, psi[n_relax], contiguous fields
-    void *profiles = nullptr;        // cell[3] then face[3], solver precision
-    int64_t profile_off[6] = {};
-    void *shell = nullptr;           // 6 faces of wall pairs, solver precision
-    int64_t shell_off[6] = {};
-    int64_t *step_base = nullptr;    // one int64 in device memory
-    double *energy_scratch = nullptr;
-    int energy_blocks = 0;
-
-    // sources
-    int64_t n_src = 0, src_stride = 0;
-    int64_t *src_off = nullptr, *src_len = nullptr;
-    void *src_sig = nullptr;
-    // receivers
-    int64_t n_rec = 0, rec_capacity = 0, rec_origin = 0;
-    bool rec_origin_set = false;
-    int64_t *rec_off = nullptr, *rec_start = nullptr;
-    void *rec = nullptr;
-    std::vector<int64_t> host_rec_cell, host_rec_start;
-
-    // graphs
-    int32_t graph_steps = 0;
-    cudaGraphExec_t graph = nullptr;
-    cudaStream_t capture_stream = nullptr;
-    bool graph_dirty = true;
-
-    // profiling
-    bool profiling = false;
-    double prof_velocity_ms = 0, prof_pressure_ms = 0;
-    int64_t prof_launches = 0;
-    static constexpr int64_t kRing = 64;
-    cudaEvent_t ring[3 * kRing] = {};
-
-    int64_t launches = 0;
-
-    size_t elem() const { return (size_t)precision; }
-    char *field_ptr(int f) const { return (char *)state + (size_t)f * field * elem(); }
-};
-
-namespace {
-
-template <typename T>
-StepParams<T> make_params(const acf_solver *h) {
-    StepParams<T> s{};
-    s.nx = h->nx;
-    s.ny = h->ny;
-    s.nz = h->nz;
-    s.nchunks = (int32_t)((h->nz + kVec - 1) / kVec);
-    s.pz = h->pz;
-    s.plane = h->plane;
-    s.field = h->field;
-    s.p = (T *)h->field_ptr(ACF_FIELD_P);
-    s.vx = (T *)h->field_ptr(ACF_FIELD_VX);
-    s.vy = (T *)h->field_ptr(ACF_FIELD_VY);
-    s.vz = (T *)h->field_ptr(ACF_FIELD_VZ);
-    s.psi = (T *)h->field_ptr(ACF_FIELD_PSI0);
-    s.cv = (T)h->coef[0];
-    s.cp = (T)h->coef[1];
-    s.cs = (T)h->coef[2];
-    s.relax_scale = (T)h->coef[3];
-    for (int r = 0; r < ACF_MAX_RELAXATION; r++) {
-        s.decay[r] = (T)h->decay[r];
-        s.mean[r] = (T)h->mean[r];
-        s.gain[r] = (T)h->gain[r];
-    }
-    for (int a = 0; a < 3; a++) {
-        s.cell[a] = h->has_layer ? (const T *)h->profiles + h->profile_off[a] : nullptr;
-        s.face[a] = h->has_layer ? (const T *)h->profiles + h->profile_off[3 + a] : nullptr;
-    }
-    for (int f = 0; f < 6; f++)
-        s.shell[f] = h->has_walls ? (const T *)h->shell + h->shell_off[f] : nullptr;
-    s.n_src = (int32_t)h->n_src;
-    s.src_off = h->src_off;
-    s.src_len = h->src_len;
-    s.src_sig = (const T *)h->src_sig;
-    s.src_stride = h->src_stride;
-    s.n_rec = (int32_t)h->n_rec;
-    s.rec_off = h->rec_off;
-    s.rec_start = h->rec_start;
-    s.rec = (T *)h->rec;
-    s.rec_stride = h->rec_capacity;
-    s.rec_origin = h->rec_origin;
-    s.step_base = h->step_base;
-    s.local_step = 0;
-    return s;
-}
-
-struct LaunchShape {
-    dim3 grid, block;
-};
-
-LaunchShape sweep_shape(const acf_solver *h) {
-    const int nchunks = (int)((h->nz + kVec - 1) / kVec);
-    int bx = 1;
-    while (bx < nchunks && bx < 32) bx <<= 1;
-    int by = std::max(1, std::min<int>(h->ny, 128 / bx));
-    LaunchShape L;
-    L.block = dim3(bx, by, 1);
-    L.grid = dim3((nchunks + bx - 1) / bx, (h->ny + by - 1) / by, std::min<int>(h->nx, 65535));
-    return L;
-}
-
-template <typename T, bool LAYER>
-void launch_velocity(const StepParams<T> &s, const LaunchShape &L, cudaStream_t st) {
-    velocity_sweep<T, LAYER><<<L.grid, L.block, 0, st>>>(s);
-}
-
-template <typename T, bool LAYER, bool WALLS>
-void launch_pressure_nr(const StepParams<T> &s, int nr, const LaunchShape &L, cudaStream_t st) {
-    switch (nr) {
-        case 0: pressure_sweep<T, LAYER, WALLS, 0><<<L.grid, L.block, 0, st>>>(s); break;
-        case 1: pressure_sweep<T, LAYER, WALLS, 1><<<L.grid, L.block, 0, st>>>(s); break;
-        case 2: pressure_sweep<T, LAYER, WALLS, 2><<<L.grid, L.block, 0, st>>>(s); break;
-        case 3: pressure_sweep<T, LAYER, WALLS, 3><<<L.grid, L.block, 0, st>>>(s); break;
-        default: pressure_sweep<T, LAYER, WALLS, 4><<<L.grid, L.block, 0, st>>>(s); break;
-    }
-}
-
-template <typename T>
-void launch_step(const acf_solver *h, StepParams<T> s, int32_t local, const LaunchShape &L,
-                 cudaStream_t st, cudaEvent_t *events) {
-    s.local_step = local;
-    if (events) cudaEventRecord(events[0], st);
-    if (h->has_layer) launch_velocity<T, true>(s, L, st);
-    else launch_velocity<T, false>(s, L, st);
-    if (events) cudaEventRecord(events[1], st);
-    if (h->has_layer) {
-        if (h->has_walls) launch_pressure_nr<T, true, true>(s, h->n_relax, L, st);
-        else launch_pressure_nr<T, true, false>(s, h->n_relax, L, st);
-    } else {
-        if (h->has_walls) launch_pressure_nr<T, false, true>(s, h->n_relax, L, st);
-        else launch_pressure_nr<T, false, false>(s, h->n_relax, L, st);
-    }
-    if (events) cudaEventRecord(events[2], st);
-}
-
-template <typename T>
-int run_impl(acf_solver *h, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
-    const LaunchShape L = sweep_shape(h);
-    const StepParams<T> s = make_params<T>(h);
-    set_step_base<<<1, 1, 0, st>>>(h->step_base, step_offset);
-    h->launches += 1;
-
-    if (h->profiling) {
-        // Event ring: the host waits on a step's events only when the ring wraps, so the
-        // queue stays full while the sweeps are being timed.
-        const int64_t R = acf_solver::kRing;
-        auto drain = [&](int64_t slot) -> int {
-            cudaEvent_t *e = h->ring + 3 * slot;
-            ACF_CUDA(cudaEventSynchronize(e[2]));
-            float a = 0, b = 0;
-            ACF_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
-            ACF_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
-            h->prof_velocity_ms += a;
-            h->prof_pressure_ms += b;
-            h->prof_launches += 1;
-            return ACF_OK;
-        };
-        for (int64_t t = 0; t < n_steps; t++) {
-            const int64_t slot = t % R;
-            if (t >= R) {
-                int rc = drain(slot);
-                if (rc) return rc;
-            }
-            launch_step<T>(h, s, (int32_t)0, L, st, h->ring + 3 * slot);
-            bump_step_base<<<1, 1, 0, st>>>(h->step_base, 1);
-            h->launches += 3;
-        }
-        for (int64_t t = std::max<int64_t>(0, n_steps - R); t < n_steps; t++) {
-            int rc = drain(t % R);
-            if (rc) return rc;
-        }
-        ACF_CUDA(cudaGetLastError());
-        return ACF_OK;
-    }
-
-    int64_t done = 0;
-    const int64_t G = h->graph_steps;
-    if (G > 0 && n_steps >= G) {
-        if (h->graph_dirty || !h->graph) {
-            if (h->graph) {
-                cudaGraphExecDestroy(h->graph);
-                h->graph = nullptr;
-            }
-            if (!h->capture_stream)
-                ACF_CUDA(cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking));
-            ACF_CUDA(cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal));
-            for (int64_t t = 0; t < G; t++) launch_step<T>(h, s, (int32_t)t, L, h->capture_stream, nullptr);
-            bump_step_base<<<1, 1, 0, h->capture_stream>>>(h->step_base, G);
-            cudaGraph_t graph = nullptr;
-            ACF_CUDA(cudaStreamEndCapture(h->capture_stream, &graph));
-            cudaError_t err = cudaGraphInstantiate(&h->graph, graph, 0);
-            cudaGraphDestroy(graph);
-            if (err != cudaSuccess)
-                return fail(ACF_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(err));
-            h->graph_dirty = false;
-        }
-        for (; done + G <= n_steps; done += G) {
-            ACF_CUDA(cudaGraphLaunch(h->graph, st));
-            h->launches += 2 * G + 1;
-        }
-    }
-    for (int64_t t = 0; done + t < n_steps; t++) {
-        launch_step<T>(h, s, (int32_t)t, L, st, nullptr);
-        h->launches += 2;
-    }
-    ACF_CUDA(cudaGetLastError());
-    return ACF_OK;
-}
-
-template <typename T>
-int energy_impl(acf_solver *h, double dx, double *terms, cudaStream_t st) {
-    const StepParams<T> s = make_params<T>(h);
-    energy_partials<T><<<h->energy_blocks, 256, 0, st>>>(s, 1.0 / dx, h->energy_scratch);
-    energy_finish<<<1, 32, 0, st>>>(h->energy_scratch, h->energy_blocks,
-                                    h->energy_scratch + (size_t)h->energy_blocks * kEnergyTerms);
-    h->launches += 2;
-    ACF_CUDA(cudaGetLastError());
-    ACF_CUDA(cudaMemcpyAsync(terms, h->energy_scratch + (size_t)h->energy_blocks * kEnergyTerms,
-                             kEnergyTerms * sizeof(double), cudaMemcpyDeviceToHost, st));
-    ACF_CUDA(cudaStreamSynchronize(st));
-    return ACF_OK;
-}
-
-// Reference shape of a field: (nx + [f==VX], ny + [f==VY], nz + [f==VZ]).
-void field_shape(const acf_solver *h, int f, int64_t shape[3]) {
-    shape[0] = h->nx + (f == ACF_FIELD_VX);
-    shape[1] = h->ny + (f == ACF_FIELD_VY);
-    shape[2] = h->nz + (f == ACF_FIELD_VZ);
-}
-
-int check_field(const acf_solver *h, int f) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (f < 0 || f >= ACF_FIELD_PSI0 + h->n_relax)
-        return fail(ACF_ERR_ARGUMENT, "field %d out of range (0..%d)", f, ACF_FIELD_PSI0 + h->n_relax - 1);
-    return ACF_OK;
-}
-
-int copy_field(acf_solver *h, int f, void *host_or_dev, bool upload, cudaStream_t st) {
-    int64_t shape[3];
-    field_shape(h, f, shape);
-    const size_t es = h->elem();
-    cudaMemcpy3DParms p = {};
-    cudaPitchedPtr dense = make_cudaPitchedPtr(host_or_dev, (size_t)shape[2] * es, (size_t)shape[2],
-                                               (size_t)shape[1]);
-    cudaPitchedPtr padded = make_cudaPitchedPtr(h->field_ptr(f), (size_t)h->pz * es, (size_t)h->pz,
-                                                (size_t)(h->ny + 1));
-    p.srcPtr = upload ? dense : padded;
-    p.dstPtr = upload ? padded : dense;
-    p.extent = make_cudaExtent((size_t)shape[2] * es, (size_t)shape[1], (size_t)shape[0]);
-    p.kind = cudaMemcpyDefault;
-    ACF_CUDA(cudaMemcpy3DAsync(&p, st));
-    return ACF_OK;
-}
-
-int64_t padded_offset(const acf_solver *h, int64_t flat) {
-    const int64_t k = flat % h->nz;
-    const int64_t j = (flat / h->nz) % h->ny;
-    const int64_t i = flat / ((int64_t)h->nz * h->ny);
-    return i * h->plane + j * h->pz + k;
-}
-
-template <typename T>
-void cast_copy(void *dst, const double *src, size_t n) {
-    T *d = (T *)dst;
-    for (size_t q = 0; q < n; q++) d[q] = (T)src[q];
-}
-
-void free_solver(acf_solver *h) {
-    if (!h) return;
-    DeviceGuard guard(h->device);
-    if (h->graph) cudaGraphExecDestroy(h->graph);
-    if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
-    for (auto &e : h->ring)
-        if (e) cudaEventDestroy(e);
-    cudaFree(h->state);
-    cudaFree(h->profiles);
-    cudaFree(h->shell);
-    cudaFree(h->step_base);
-    cudaFree(h->energy_scratch);
-    cudaFree(h->src_off);
-    cudaFree(h->src_len);
-    cudaFree(h->src_sig);
-    cudaFree(h->rec_off);
-    cudaFree(h->rec_start);
-    cudaFree(h->rec);
-    delete h;
 }
 
 }  // namespace
@@ -857,6 +620,785 @@ static int noalloc_scratch(double **out) {
     return ACF_OK;
 }
 
+// ------------------------------------------------------------------------------------------
+// Host side.
+
+namespace {
+
+struct DeviceGuard {
+    int previous = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+        if (previous != device) cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous)
+            cudaSetDevice(previous);
+    }
+};
+
+inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Everything the host keeps about one room of a batch.
+struct RoomHost {
+    int32_t nx = 0, ny = 0, nz = 0, n_relax = 0;
+    int64_t pz = 0, plane = 0, field = 0;
+    bool has_layer = false, has_walls = false;
+    double coef[4] = {0, 0, 0, 0};   // cv, cp, cs, relax_scale
+    double decay[ACF_MAX_RELAXATION] = {}, mean[ACF_MAX_RELAXATION] = {},
+           gain[ACF_MAX_RELAXATION] = {};
+    size_t state_off = 0;            // byte offset of the room's fields in the state arena
+    void *profiles = nullptr;        // cell[3] then face[3], solver precision
+    int64_t profile_off[6] = {};
+    void *shell = nullptr;           // 6 faces of wall pairs, solver precision
+    int64_t shell_off[6] = {};
+    // sources
+    int64_t n_src = 0, src_stride = 0;
+    int64_t *src_off = nullptr, *src_len = nullptr;
+    void *src_sig = nullptr;
+    // receivers
+    int64_t n_rec = 0, rec_capacity = 0, rec_origin = 0;
+    bool rec_origin_set = false;
+    int64_t *rec_off = nullptr, *rec_start = nullptr;
+    void *rec = nullptr;
+    std::vector<int64_t> host_rec_start;
+
+    int64_t n_cells() const { return (int64_t)nx * ny * nz; }
+    int64_t padded_offset(int64_t flat) const {
+        const int64_t k = flat % nz;
+        const int64_t j = (flat / nz) % ny;
+        const int64_t i = flat / ((int64_t)nz * ny);
+        return i * plane + j * pz + k;
+    }
+};
+
+}  // namespace
+
+struct acf_batch {
+    int device = 0;
+    int precision = 8;
+    int n_relax = 0;                 // the same for every room of a batch
+    bool any_layer = false, any_walls = false;
+    std::vector<RoomHost> rooms;
+
+    void *state = nullptr;           // every room's fields, one arena
+    size_t state_bytes = 0;
+    void *room_table = nullptr;      // device array of Room<T>, one per room
+    bool room_table_dirty = true;
+    Tile *tiles = nullptr;
+    int32_t n_tiles = 0;
+    int32_t batch_ctas = 0;
+    int64_t *step_base = nullptr;    // one int64 in device memory
+    double *energy_scratch = nullptr;
+    int energy_blocks = 0;
+    int sms = 148;
+
+    // launch geometry (tunable; results never depend on it)
+    int block_threads = 256;
+    int planes = 4;
+    int ctas_per_sm = 4;
+
+    // graphs
+    int32_t graph_steps = 0;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    bool graph_dirty = true;
+
+    // profiling
+    bool profiling = false;
+    double prof_velocity_ms = 0, prof_pressure_ms = 0;
+    int64_t prof_launches = 0;
+    static constexpr int64_t kRing = 64;
+    cudaEvent_t ring[3 * kRing] = {};
+
+    int64_t launches = 0;
+
+    size_t elem() const { return (size_t)precision; }
+    int n_fields() const { return 4 + n_relax; }
+    char *field_ptr(int r, int f) const {
+        return (char *)state + rooms[r].state_off + (size_t)f * rooms[r].field * elem();
+    }
+};
+
+// A single room is a batch of one, launched with the 2D single-room kernels.
+struct acf_solver : acf_batch {};
+
+namespace {
+
+template <typename T>
+Room<T> make_room(const acf_batch *b, int r) {
+    const RoomHost &h = b->rooms[r];
+    Room<T> s{};
+    s.nx = h.nx;
+    s.ny = h.ny;
+    s.nz = h.nz;
+    s.nchunks = (int32_t)((h.nz + kVec - 1) / kVec);
+    s.pz = h.pz;
+    s.plane = h.plane;
+    s.field = h.field;
+    s.p = (T *)b->field_ptr(r, ACF_FIELD_P);
+    s.vx = (T *)b->field_ptr(r, ACF_FIELD_VX);
+    s.vy = (T *)b->field_ptr(r, ACF_FIELD_VY);
+    s.vz = (T *)b->field_ptr(r, ACF_FIELD_VZ);
+    s.psi = (T *)b->field_ptr(r, ACF_FIELD_PSI0);
+    s.cv = (T)h.coef[0];
+    s.cp = (T)h.coef[1];
+    s.cs = (T)h.coef[2];
+    s.relax_scale = (T)h.coef[3];
+    for (int q = 0; q < ACF_MAX_RELAXATION; q++) {
+        s.decay[q] = (T)h.decay[q];
+        s.mean[q] = (T)h.mean[q];
+        s.gain[q] = (T)h.gain[q];
+    }
+    for (int a = 0; a < 3; a++) {
+        s.cell[a] = h.profiles ? (const T *)h.profiles + h.profile_off[a] : nullptr;
+        s.face[a] = h.profiles ? (const T *)h.profiles + h.profile_off[3 + a] : nullptr;
+    }
+    for (int f = 0; f < 6; f++) s.shell[f] = h.shell ? (const T *)h.shell + h.shell_off[f] : nullptr;
+    s.n_src = (int32_t)h.n_src;
+    s.src_off = h.src_off;
+    s.src_len = h.src_len;
+    s.src_sig = (const T *)h.src_sig;
+    s.src_stride = h.src_stride;
+    s.n_rec = (int32_t)h.n_rec;
+    s.rec_off = h.rec_off;
+    s.rec_start = h.rec_start;
+    s.rec = (T *)h.rec;
+    s.rec_stride = h.rec_capacity;
+    s.rec_origin = h.rec_origin;
+    return s;
+}
+
+template <typename T>
+int upload_room_table(acf_batch *b) {
+    std::vector<Room<T>> table(b->rooms.size());
+    for (size_t r = 0; r < b->rooms.size(); r++) table[r] = make_room<T>(b, (int)r);
+    if (!b->room_table) ACF_CUDA(cudaMalloc(&b->room_table, table.size() * sizeof(Room<T>)));
+    ACF_CUDA(cudaMemcpy(b->room_table, table.data(), table.size() * sizeof(Room<T>), cudaMemcpyHostToDevice));
+    b->room_table_dirty = false;
+    return ACF_OK;
+}
+
+// Tiles in room order, then plane group, then (row, chunk) block: neighbouring tiles of one
+// room run close together, so the y- and x-neighbour rows they share are still in L2.
+int build_tiles(acf_batch *b) {
+    std::vector<Tile> tiles;
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        const RoomHost &h = b->rooms[r];
+        const int64_t nchunks = (h.nz + kVec - 1) / kVec;
+        const int64_t pairs = (int64_t)h.ny * nchunks;
+        for (int i0 = 0; i0 < h.nx; i0 += b->planes)
+            for (int64_t first = 0; first < pairs; first += b->block_threads) {
+                Tile t{};
+                t.room = (int32_t)r;
+                t.first = (int32_t)first;
+                t.count = (int32_t)std::min<int64_t>(b->block_threads, pairs - first);
+                t.i_begin = i0;
+                t.i_end = std::min(h.nx, i0 + b->planes);
+                tiles.push_back(t);
+            }
+    }
+    if (tiles.size() > (size_t)INT32_MAX) return fail(ACF_ERR_ARGUMENT, "too many tiles");
+    cudaFree(b->tiles);
+    b->tiles = nullptr;
+    ACF_CUDA(cudaMalloc(&b->tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    ACF_CUDA(cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    b->n_tiles = (int32_t)tiles.size();
+    b->batch_ctas = std::max(1, std::min(b->n_tiles, b->ctas_per_sm * b->sms));
+    return ACF_OK;
+}
+
+struct LaunchShape {
+    dim3 grid, block;
+};
+
+LaunchShape single_shape(const acf_batch *b) {
+    const RoomHost &h = b->rooms[0];
+    const int nchunks = (int)((h.nz + kVec - 1) / kVec);
+    int bx = 1;
+    while (bx < nchunks && bx < 32) bx <<= 1;
+    int by = std::max(1, std::min<int>(h.ny, b->block_threads / bx));
+    LaunchShape L;
+    L.block = dim3(bx, by, 1);
+    L.grid = dim3((nchunks + bx - 1) / bx, (h.ny + by - 1) / by, (h.nx + b->planes - 1) / b->planes);
+    return L;
+}
+
+// Template dispatch over the pressure kernels' compile-time features.
+template <typename T, template <typename, bool, bool, int> class K, typename P>
+void dispatch_pressure(bool layer, bool walls, int nr, const P &params, dim3 grid, dim3 block,
+                       cudaStream_t st) {
+#define ACF_NR(L, W)                                                                    \
+    switch (nr) {                                                                        \
+        case 0: K<T, L, W, 0>::launch(params, grid, block, st); break;                  \
+        case 1: K<T, L, W, 1>::launch(params, grid, block, st); break;                  \
+        case 2: K<T, L, W, 2>::launch(params, grid, block, st); break;                  \
+        case 3: K<T, L, W, 3>::launch(params, grid, block, st); break;                  \
+        default: K<T, L, W, 4>::launch(params, grid, block, st); break;                 \
+    }
+    if (layer) {
+        if (walls) { ACF_NR(true, true) } else { ACF_NR(true, false) }
+    } else {
+        if (walls) { ACF_NR(false, true) } else { ACF_NR(false, false) }
+    }
+#undef ACF_NR
+}
+
+template <typename T, bool L, bool W, int NR>
+struct SinglePressure {
+    static void launch(const StepParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        pressure_sweep<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct BatchPressure {
+    static void launch(const BatchParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        pressure_batch<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T>
+void launch_step(const acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
+    if (events) cudaEventRecord(events[0], st);
+    if (b->rooms.size() == 1) {
+        const RoomHost &h = b->rooms[0];
+        StepParams<T> p{};
+        p.room = make_room<T>(b, 0);
+        p.step_base = b->step_base;
+        p.local_step = local;
+        p.planes = b->planes;
+        const LaunchShape L = single_shape(b);
+        if (h.has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(p);
+        else velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(p);
+        if (events) cudaEventRecord(events[1], st);
+        dispatch_pressure<T, SinglePressure>(h.has_layer, h.has_walls, h.n_relax, p, L.grid,
+                                             L.block, st);
+    } else {
+        BatchParams<T> p{};
+        p.rooms = (const Room<T> *)b->room_table;
+        p.tiles = b->tiles;
+        p.n_tiles = b->n_tiles;
+        p.local_step = local;
+        p.step_base = b->step_base;
+        const dim3 grid(b->batch_ctas), block(b->block_threads);
+        if (b->any_layer) velocity_batch<T, true><<<grid, block, 0, st>>>(p);
+        else velocity_batch<T, false><<<grid, block, 0, st>>>(p);
+        if (events) cudaEventRecord(events[1], st);
+        dispatch_pressure<T, BatchPressure>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+    }
+    if (events) cudaEventRecord(events[2], st);
+}
+
+template <typename T>
+int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
+    if (b->rooms.size() > 1 && b->room_table_dirty) {
+        int rc = upload_room_table<T>(b);
+        if (rc) return rc;
+    }
+    set_step_base<<<1, 1, 0, st>>>(b->step_base, step_offset);
+    b->launches += 1;
+
+    if (b->profiling) {
+        // Event ring: the host waits on a step's events only when the ring wraps, so the
+        // queue stays full while the sweeps are being timed.
+        const int64_t R = acf_batch::kRing;
+        auto drain = [&](int64_t slot) -> int {
+            cudaEvent_t *e = b->ring + 3 * slot;
+            ACF_CUDA(cudaEventSynchronize(e[2]));
+            float x = 0, y = 0;
+            ACF_CUDA(cudaEventElapsedTime(&x, e[0], e[1]));
+            ACF_CUDA(cudaEventElapsedTime(&y, e[1], e[2]));
+            b->prof_velocity_ms += x;
+            b->prof_pressure_ms += y;
+            b->prof_launches += 1;
+            return ACF_OK;
+        };
+        for (int64_t t = 0; t < n_steps; t++) {
+            const int64_t slot = t % R;
+            if (t >= R) {
+                int rc = drain(slot);
+                if (rc) return rc;
+            }
+            launch_step<T>(b, 0, st, b->ring + 3 * slot);
+            bump_step_base<<<1, 1, 0, st>>>(b->step_base, 1);
+            b->launches += 3;
+        }
+        for (int64_t t = std::max<int64_t>(0, n_steps - R); t < n_steps; t++) {
+            int rc = drain(t % R);
+            if (rc) return rc;
+        }
+        ACF_CUDA(cudaGetLastError());
+        return ACF_OK;
+    }
+
+    int64_t done = 0;
+    const int64_t G = b->graph_steps;
+    if (G > 0 && n_steps >= G) {
+        if (b->graph_dirty || !b->graph) {
+            if (b->graph) {
+                cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+            if (!b->capture_stream)
+                ACF_CUDA(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
+            ACF_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+            for (int64_t t = 0; t < G; t++) launch_step<T>(b, (int32_t)t, b->capture_stream, nullptr);
+            bump_step_base<<<1, 1, 0, b->capture_stream>>>(b->step_base, G);
+            cudaGraph_t graph = nullptr;
+            ACF_CUDA(cudaStreamEndCapture(b->capture_stream, &graph));
+            cudaError_t err = cudaGraphInstantiate(&b->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            if (err != cudaSuccess)
+                return fail(ACF_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(err));
+            b->graph_dirty = false;
+        }
+        for (; done + G <= n_steps; done += G) {
+            ACF_CUDA(cudaGraphLaunch(b->graph, st));
+            b->launches += 2 * G + 1;
+        }
+    }
+    for (int64_t t = 0; done + t < n_steps; t++) {
+        launch_step<T>(b, (int32_t)t, st, nullptr);
+        b->launches += 2;
+    }
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+template <typename T>
+int energy_impl(acf_batch *b, int room, double dx, double *terms, cudaStream_t st) {
+    const Room<T> s = make_room<T>(b, room);
+    energy_partials<T><<<b->energy_blocks, 256, 0, st>>>(s, 1.0 / dx, b->energy_scratch);
+    energy_finish<<<1, 32, 0, st>>>(b->energy_scratch, b->energy_blocks,
+                                    b->energy_scratch + (size_t)b->energy_blocks * kEnergyTerms);
+    b->launches += 2;
+    ACF_CUDA(cudaGetLastError());
+    ACF_CUDA(cudaMemcpyAsync(terms, b->energy_scratch + (size_t)b->energy_blocks * kEnergyTerms,
+                             kEnergyTerms * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACF_CUDA(cudaStreamSynchronize(st));
+    return ACF_OK;
+}
+
+// Reference shape of a field: (nx + [f==VX], ny + [f==VY], nz + [f==VZ]).
+void field_shape(const RoomHost &h, int f, int64_t shape[3]) {
+    shape[0] = h.nx + (f == ACF_FIELD_VX);
+    shape[1] = h.ny + (f == ACF_FIELD_VY);
+    shape[2] = h.nz + (f == ACF_FIELD_VZ);
+}
+
+int check_room(const acf_batch *b, int room) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (room < 0 || room >= (int)b->rooms.size())
+        return fail(ACF_ERR_ARGUMENT, "room %d out of range (0..%d)", room, (int)b->rooms.size() - 1);
+    return ACF_OK;
+}
+
+int check_field(const acf_batch *b, int room, int f) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    if (f < 0 || f >= b->n_fields())
+        return fail(ACF_ERR_ARGUMENT, "field %d out of range (0..%d)", f, b->n_fields() - 1);
+    return ACF_OK;
+}
+
+int copy_field(acf_batch *b, int room, int f, void *host_or_dev, bool upload, cudaStream_t st) {
+    const RoomHost &h = b->rooms[room];
+    int64_t shape[3];
+    field_shape(h, f, shape);
+    const size_t es = b->elem();
+    cudaMemcpy3DParms p = {};
+    cudaPitchedPtr dense = make_cudaPitchedPtr(host_or_dev, (size_t)shape[2] * es, (size_t)shape[2],
+                                               (size_t)shape[1]);
+    cudaPitchedPtr padded = make_cudaPitchedPtr(b->field_ptr(room, f), (size_t)h.pz * es, (size_t)h.pz,
+                                                (size_t)(h.ny + 1));
+    p.srcPtr = upload ? dense : padded;
+    p.dstPtr = upload ? padded : dense;
+    p.extent = make_cudaExtent((size_t)shape[2] * es, (size_t)shape[1], (size_t)shape[0]);
+    p.kind = cudaMemcpyDefault;
+    ACF_CUDA(cudaMemcpy3DAsync(&p, st));
+    return ACF_OK;
+}
+
+template <typename T>
+void cast_copy(void *dst, const double *src, size_t n) {
+    T *d = (T *)dst;
+    for (size_t q = 0; q < n; q++) d[q] = (T)src[q];
+}
+
+int upload_cast(void **dst, const std::vector<double> &host, size_t es) {
+    std::vector<char> cast(std::max<size_t>(1, host.size()) * es, 0);
+    if (es == 4) cast_copy<float>(cast.data(), host.data(), host.size());
+    else cast_copy<double>(cast.data(), host.data(), host.size());
+    ACF_CUDA(cudaMalloc(dst, cast.size()));
+    ACF_CUDA(cudaMemcpy(*dst, cast.data(), cast.size(), cudaMemcpyHostToDevice));
+    return ACF_OK;
+}
+
+void free_room(RoomHost &h) {
+    cudaFree(h.profiles);
+    cudaFree(h.shell);
+    cudaFree(h.src_off);
+    cudaFree(h.src_len);
+    cudaFree(h.src_sig);
+    cudaFree(h.rec_off);
+    cudaFree(h.rec_start);
+    cudaFree(h.rec);
+    h = RoomHost();
+}
+
+void free_batch(acf_batch *b) {
+    if (!b) return;
+    DeviceGuard guard(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+    for (auto &e : b->ring)
+        if (e) cudaEventDestroy(e);
+    for (auto &r : b->rooms) free_room(r);
+    cudaFree(b->state);
+    cudaFree(b->room_table);
+    cudaFree(b->tiles);
+    cudaFree(b->step_base);
+    cudaFree(b->energy_scratch);
+    delete b;
+}
+
+int validate_config(const acf_config *cfg, int index) {
+    if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1)
+        return fail(ACF_ERR_ARGUMENT, "room %d: cell counts must be >= 1, got (%d, %d, %d)", index, cfg->nx,
+                    cfg->ny, cfg->nz);
+    if (cfg->precision != 4 && cfg->precision != 8)
+        return fail(ACF_ERR_ARGUMENT, "room %d: precision must be 4 or 8 bytes, got %d", index, cfg->precision);
+    if (cfg->n_relax < 0 || cfg->n_relax > ACF_MAX_RELAXATION)
+        return fail(ACF_ERR_ARGUMENT, "room %d: the kernel holds at most %d relaxation processes, got %d",
+                    index, ACF_MAX_RELAXATION, cfg->n_relax);
+    const bool layer = cfg->cell[0] != nullptr;
+    for (int a = 0; a < 3; a++)
+        if ((cfg->cell[a] != nullptr) != layer || (cfg->face[a] != nullptr) != layer)
+            return fail(ACF_ERR_ARGUMENT, "room %d: layer profiles must be all given or all NULL", index);
+    const bool walls = cfg->wall_shell[0] != nullptr;
+    for (int f = 0; f < 6; f++)
+        if ((cfg->wall_shell[f] != nullptr) != walls)
+            return fail(ACF_ERR_ARGUMENT, "room %d: wall shells must be all given or all NULL", index);
+    if ((int64_t)cfg->nx * cfg->ny > INT32_MAX / 2 || (int64_t)cfg->ny * ((cfg->nz + 3) / 4) > INT32_MAX / 2)
+        return fail(ACF_ERR_ARGUMENT, "room %d: grid too large", index);
+    return ACF_OK;
+}
+
+// Allocate and fill every room of a batch (single rooms are batches of one).
+int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
+    if (n_rooms < 1) return fail(ACF_ERR_ARGUMENT, "a batch needs at least one room");
+    for (int r = 0; r < n_rooms; r++) {
+        int rc = validate_config(configs + r, r);
+        if (rc) return rc;
+        if (configs[r].precision != configs[0].precision)
+            return fail(ACF_ERR_ARGUMENT, "room %d: every room of a batch must have the same precision", r);
+        if (configs[r].n_relax != configs[0].n_relax)
+            return fail(ACF_ERR_ARGUMENT, "room %d: every room of a batch must have the same number of "
+                        "relaxation processes", r);
+    }
+    ACF_CUDA(cudaGetDevice(&b->device));
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->precision = configs[0].precision;
+    b->n_relax = configs[0].n_relax;
+    b->rooms.resize((size_t)n_rooms);
+    const size_t es = b->elem();
+    size_t offset = 0;
+    for (int r = 0; r < n_rooms; r++) {
+        const acf_config &c = configs[r];
+        RoomHost &h = b->rooms[r];
+        h.nx = c.nx;
+        h.ny = c.ny;
+        h.nz = c.nz;
+        h.n_relax = c.n_relax;
+        h.pz = round_up((int64_t)c.nz + 1, kRowAlign);
+        h.plane = (int64_t)(c.ny + 1) * h.pz;
+        h.field = (int64_t)(c.nx + 1) * h.plane;
+        h.has_layer = c.cell[0] != nullptr;
+        h.has_walls = c.wall_shell[0] != nullptr;
+        b->any_layer |= h.has_layer;
+        b->any_walls |= h.has_walls;
+        h.coef[0] = c.vel_coef;
+        h.coef[1] = c.pres_coef;
+        h.coef[2] = c.src_coef;
+        h.coef[3] = c.relax_scale;
+        for (int q = 0; q < ACF_MAX_RELAXATION; q++) {
+            h.decay[q] = q < c.n_relax ? c.relax_decay[q] : 0.0;
+            h.mean[q] = q < c.n_relax ? c.relax_mean[q] : 0.0;
+            h.gain[q] = q < c.n_relax ? c.relax_gain[q] : 0.0;
+        }
+        h.state_off = offset;
+        // One guard row past the last field keeps every vector access of the last row in
+        // bounds; rooms start on 256-byte boundaries.
+        offset += (size_t)round_up(((int64_t)b->n_fields() * h.field + h.pz) * (int64_t)es, 256);
+    }
+    b->state_bytes = offset;
+    if (cudaMalloc(&b->state, b->state_bytes) != cudaSuccess)
+        return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of state failed", b->state_bytes);
+    ACF_CUDA(cudaMemset(b->state, 0, b->state_bytes));
+
+    const bool batched = n_rooms > 1;
+    for (int r = 0; r < n_rooms; r++) {
+        const acf_config &c = configs[r];
+        RoomHost &h = b->rooms[r];
+        const int64_t n_axis[3] = {c.nx, c.ny, c.nz};
+        // In a batch every room carries what any room needs; the neutral values (profiles of
+        // one, wall pairs (1, 0)) leave its arithmetic exactly as without the feature.
+        if (h.has_layer || (batched && b->any_layer)) {
+            std::vector<double> host;
+            for (int a = 0; a < 3; a++) {
+                h.profile_off[a] = (int64_t)host.size();
+                if (h.has_layer) host.insert(host.end(), c.cell[a], c.cell[a] + n_axis[a]);
+                else host.insert(host.end(), (size_t)n_axis[a], 1.0);
+            }
+            for (int a = 0; a < 3; a++) {
+                h.profile_off[3 + a] = (int64_t)host.size();
+                if (h.has_layer) host.insert(host.end(), c.face[a], c.face[a] + n_axis[a] + 1);
+                else host.insert(host.end(), (size_t)n_axis[a] + 1, 1.0);
+            }
+            int rc = upload_cast(&h.profiles, host, es);
+            if (rc) return rc;
+        }
+        if (h.has_walls || (batched && b->any_walls)) {
+            std::vector<double> host;
+            for (int f = 0; f < 6; f++) {
+                const int axis = f / 2;
+                const int64_t nb = axis == 0 ? n_axis[1] : n_axis[0];
+                const int64_t nc = axis == 2 ? n_axis[1] : n_axis[2];
+                h.shell_off[f] = (int64_t)host.size();
+                if (h.has_walls) {
+                    host.insert(host.end(), c.wall_shell[f], c.wall_shell[f] + 2 * nb * nc);
+                } else {
+                    for (int64_t q = 0; q < nb * nc; q++) {
+                        host.push_back(1.0);
+                        host.push_back(0.0);
+                    }
+                }
+            }
+            int rc = upload_cast(&h.shell, host, es);
+            if (rc) return rc;
+        }
+    }
+
+    if (cudaMalloc(&b->step_base, sizeof(int64_t)) != cudaSuccess)
+        return fail(ACF_ERR_MEMORY, "cudaMalloc of step counter failed");
+    ACF_CUDA(cudaMemset(b->step_base, 0, sizeof(int64_t)));
+    b->energy_blocks = 4 * b->sms;
+    const size_t scratch = ((size_t)b->energy_blocks + 1) * kEnergyTerms * sizeof(double);
+    if (cudaMalloc(&b->energy_scratch, scratch) != cudaSuccess)
+        return fail(ACF_ERR_MEMORY, "cudaMalloc of energy scratch failed");
+    for (auto &ev : b->ring) ACF_CUDA(cudaEventCreate(&ev));
+    if (batched) {
+        b->block_threads = 256;
+        b->planes = 4;
+    } else {
+        b->block_threads = 128;
+        b->planes = 4;
+        while ((b->rooms[0].nx + b->planes - 1) / b->planes > 65535) b->planes *= 2;
+    }
+    return batched ? build_tiles(b) : ACF_OK;
+}
+
+int set_sources(acf_batch *b, int room, int64_t n, const int64_t *cell, const int64_t *length,
+                const double *signal, int64_t stride) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    if (n < 0 || n > (1 << 20)) return fail(ACF_ERR_ARGUMENT, "source count %lld out of range", (long long)n);
+    if (n > 0 && (!cell || !length || (stride > 0 && !signal) || stride < 0))
+        return fail(ACF_ERR_ARGUMENT, "null source arrays");
+    RoomHost &h = b->rooms[room];
+    DeviceGuard guard(b->device);
+    std::vector<int64_t> off((size_t)n), len((size_t)n);
+    for (int64_t q = 0; q < n; q++) {
+        if (cell[q] < 0 || cell[q] >= h.n_cells())
+            return fail(ACF_ERR_ARGUMENT, "source %lld cell %lld outside the grid", (long long)q, (long long)cell[q]);
+        if (length[q] < 0 || length[q] > stride)
+            return fail(ACF_ERR_ARGUMENT, "source %lld length %lld exceeds stride %lld", (long long)q,
+                        (long long)length[q], (long long)stride);
+        off[q] = h.padded_offset(cell[q]);
+        len[q] = length[q];
+    }
+    ACF_CUDA(cudaDeviceSynchronize());
+    cudaFree(h.src_off);
+    cudaFree(h.src_len);
+    cudaFree(h.src_sig);
+    h.src_off = h.src_len = nullptr;
+    h.src_sig = nullptr;
+    h.n_src = 0;
+    b->graph_dirty = true;
+    b->room_table_dirty = true;
+    if (n == 0) return ACF_OK;
+    const size_t es = b->elem();
+    ACF_CUDA(cudaMalloc(&h.src_off, n * sizeof(int64_t)));
+    ACF_CUDA(cudaMalloc(&h.src_len, n * sizeof(int64_t)));
+    ACF_CUDA(cudaMemcpy(h.src_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    ACF_CUDA(cudaMemcpy(h.src_len, len.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    std::vector<double> host((size_t)n * (size_t)std::max<int64_t>(stride, 1), 0.0);
+    if (stride > 0) std::copy(signal, signal + (size_t)n * stride, host.begin());
+    rc = upload_cast(&h.src_sig, host, es);
+    if (rc) return rc;
+    h.n_src = n;
+    h.src_stride = stride;
+    return ACF_OK;
+}
+
+int set_receivers(acf_batch *b, int room, int64_t n, const int64_t *cell, const int64_t *start_step) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    if (n < 0 || n > (1 << 20)) return fail(ACF_ERR_ARGUMENT, "receiver count %lld out of range", (long long)n);
+    if (n > 0 && (!cell || !start_step)) return fail(ACF_ERR_ARGUMENT, "null receiver arrays");
+    RoomHost &h = b->rooms[room];
+    DeviceGuard guard(b->device);
+    std::vector<int64_t> off((size_t)n);
+    for (int64_t r = 0; r < n; r++) {
+        if (cell[r] < 0 || cell[r] >= h.n_cells())
+            return fail(ACF_ERR_ARGUMENT, "receiver %lld cell %lld outside the grid", (long long)r, (long long)cell[r]);
+        if (start_step[r] < 0) return fail(ACF_ERR_ARGUMENT, "negative start step");
+        off[r] = h.padded_offset(cell[r]);
+    }
+    int64_t origin = h.rec_origin;
+    if (n > 0 && !h.rec_origin_set) origin = *std::min_element(start_step, start_step + n);
+    for (int64_t r = 0; r < n; r++)
+        if (start_step[r] < origin)
+            return fail(ACF_ERR_ARGUMENT, "receiver %lld starts before the recording origin", (long long)r);
+    ACF_CUDA(cudaDeviceSynchronize());
+    if (n > 0 && !h.rec_origin_set) {
+        h.rec_origin = origin;
+        h.rec_origin_set = true;
+    }
+    // Keep existing recordings: grow the row count, preserving rows already written.
+    const size_t es = b->elem();
+    if (n > 0 && h.rec_capacity > 0 && n != h.n_rec) {
+        void *grown = nullptr;
+        ACF_CUDA(cudaMalloc(&grown, (size_t)n * h.rec_capacity * es));
+        ACF_CUDA(cudaMemset(grown, 0, (size_t)n * h.rec_capacity * es));
+        const int64_t keep = std::min<int64_t>(n, h.n_rec);
+        if (keep > 0 && h.rec)
+            ACF_CUDA(cudaMemcpy(grown, h.rec, (size_t)keep * h.rec_capacity * es, cudaMemcpyDeviceToDevice));
+        cudaFree(h.rec);
+        h.rec = grown;
+    }
+    cudaFree(h.rec_off);
+    cudaFree(h.rec_start);
+    h.rec_off = h.rec_start = nullptr;
+    h.n_rec = 0;
+    b->graph_dirty = true;
+    b->room_table_dirty = true;
+    h.host_rec_start.assign(start_step, start_step + n);
+    if (n == 0) return ACF_OK;
+    ACF_CUDA(cudaMalloc(&h.rec_off, n * sizeof(int64_t)));
+    ACF_CUDA(cudaMalloc(&h.rec_start, n * sizeof(int64_t)));
+    ACF_CUDA(cudaMemcpy(h.rec_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    ACF_CUDA(cudaMemcpy(h.rec_start, start_step, n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    h.n_rec = n;
+    return ACF_OK;
+}
+
+int read_recording(acf_batch *b, int room, int64_t r, int64_t first_step, int64_t n, void *dst,
+                   acf_stream stream) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    RoomHost &h = b->rooms[room];
+    if (r < 0 || r >= h.n_rec) return fail(ACF_ERR_ARGUMENT, "receiver %lld out of range", (long long)r);
+    if (n < 0 || (n > 0 && !dst)) return fail(ACF_ERR_ARGUMENT, "bad destination");
+    if (n == 0) return ACF_OK;
+    const int64_t col = first_step - h.rec_origin;
+    if (col < 0 || col + n > h.rec_capacity || first_step < h.host_rec_start[(size_t)r])
+        return fail(ACF_ERR_ARGUMENT, "steps [%lld, %lld) were not recorded by receiver %lld",
+                    (long long)first_step, (long long)(first_step + n), (long long)r);
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t es = b->elem();
+    ACF_CUDA(cudaMemcpyAsync(dst, (char *)h.rec + ((size_t)r * h.rec_capacity + col) * es, (size_t)n * es,
+                             cudaMemcpyDeviceToHost, st));
+    ACF_CUDA(cudaStreamSynchronize(st));
+    return ACF_OK;
+}
+
+int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
+    if (n_steps == 0) return ACF_OK;
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    // Recording capacity for every step this run can write.
+    for (RoomHost &h : b->rooms) {
+        if (h.n_rec == 0) continue;
+        const int64_t need = step_offset + n_steps - h.rec_origin;
+        if (need <= h.rec_capacity) continue;
+        int64_t cap = round_up(std::max<int64_t>(need, 2 * h.rec_capacity), 256);
+        const size_t es = b->elem();
+        void *grown = nullptr;
+        ACF_CUDA(cudaStreamSynchronize(st));
+        ACF_CUDA(cudaMalloc(&grown, (size_t)h.n_rec * cap * es));
+        ACF_CUDA(cudaMemset(grown, 0, (size_t)h.n_rec * cap * es));
+        if (h.rec && h.rec_capacity > 0)
+            ACF_CUDA(cudaMemcpy2D(grown, (size_t)cap * es, h.rec, (size_t)h.rec_capacity * es,
+                                  (size_t)h.rec_capacity * es, (size_t)h.n_rec, cudaMemcpyDeviceToDevice));
+        cudaFree(h.rec);
+        h.rec = grown;
+        h.rec_capacity = cap;
+        b->graph_dirty = true;
+        b->room_table_dirty = true;
+    }
+    return b->precision == 8 ? run_impl<double>(b, n_steps, step_offset, st)
+                             : run_impl<float>(b, n_steps, step_offset, st);
+}
+
+int set_launch(acf_batch *b, int32_t block_threads, int32_t planes, int32_t ctas_per_sm) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (block_threads < 32 || block_threads > 256 || (block_threads & (block_threads - 1)))
+        return fail(ACF_ERR_ARGUMENT, "block_threads must be a power of two in [32, 256], got %d", block_threads);
+    if (planes < 1 || planes > 1024) return fail(ACF_ERR_ARGUMENT, "planes must be in [1, 1024], got %d", planes);
+    if (ctas_per_sm < 1 || ctas_per_sm > 32)
+        return fail(ACF_ERR_ARGUMENT, "ctas_per_sm must be in [1, 32], got %d", ctas_per_sm);
+    if (b->rooms.size() == 1 && (b->rooms[0].nx + planes - 1) / planes > 65535)
+        return fail(ACF_ERR_ARGUMENT, "nx / planes exceeds the 65535 grid limit; use more planes per block");
+    DeviceGuard guard(b->device);
+    const bool changed = block_threads != b->block_threads || planes != b->planes || ctas_per_sm != b->ctas_per_sm;
+    b->block_threads = block_threads;
+    b->planes = planes;
+    b->ctas_per_sm = ctas_per_sm;
+    if (changed) {
+        b->graph_dirty = true;
+        if (b->rooms.size() > 1) {
+            ACF_CUDA(cudaDeviceSynchronize());
+            return build_tiles(b);
+        }
+    }
+    return ACF_OK;
+}
+
+int profile_read(acf_batch *b, double *velocity_ms, double *pressure_ms, int64_t *launches) {
+    if (!b || !velocity_ms || !pressure_ms || !launches) return fail(ACF_ERR_ARGUMENT, "null argument");
+    *velocity_ms = b->prof_velocity_ms;
+    *pressure_ms = b->prof_pressure_ms;
+    *launches = b->prof_launches;
+    return ACF_OK;
+}
+
+int profile_enable(acf_batch *b, int32_t enable) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    b->profiling = enable != 0;
+    b->prof_velocity_ms = b->prof_pressure_ms = 0;
+    b->prof_launches = 0;
+    return ACF_OK;
+}
+
+int energy_terms(acf_batch *b, int room, double dx, double terms[7], acf_stream stream) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    if (!terms) return fail(ACF_ERR_ARGUMENT, "null argument");
+    if (!(dx > 0)) return fail(ACF_ERR_ARGUMENT, "dx must be positive");
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    return b->precision == 8 ? energy_impl<double>(b, room, dx, terms, st)
+                             : energy_impl<float>(b, room, dx, terms, st);
+}
+
+}  // namespace
+
 // ==========================================================================================
 // C ABI
 
@@ -874,119 +1416,26 @@ int acf_device_count(int *count) {
     return ACF_OK;
 }
 
+// ---- one room ---------------------------------------------------------------------------
+
 int acf_create(const acf_config *cfg, acf_solver **out) {
     if (!cfg || !out) return fail(ACF_ERR_ARGUMENT, "null config or output pointer");
     *out = nullptr;
-    if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1)
-        return fail(ACF_ERR_ARGUMENT, "cell counts must be >= 1, got (%d, %d, %d)", cfg->nx, cfg->ny, cfg->nz);
-    if (cfg->precision != 4 && cfg->precision != 8)
-        return fail(ACF_ERR_ARGUMENT, "precision must be 4 or 8 bytes, got %d", cfg->precision);
-    if (cfg->n_relax < 0 || cfg->n_relax > ACF_MAX_RELAXATION)
-        return fail(ACF_ERR_ARGUMENT, "the kernel holds at most %d relaxation processes, got %d",
-                    ACF_MAX_RELAXATION, cfg->n_relax);
-    const bool layer = cfg->cell[0] != nullptr;
-    for (int a = 0; a < 3; a++)
-        if ((cfg->cell[a] != nullptr) != layer || (cfg->face[a] != nullptr) != layer)
-            return fail(ACF_ERR_ARGUMENT, "layer profiles must be all given or all NULL");
-    const bool walls = cfg->wall_shell[0] != nullptr;
-    for (int f = 0; f < 6; f++)
-        if ((cfg->wall_shell[f] != nullptr) != walls)
-            return fail(ACF_ERR_ARGUMENT, "wall shells must be all given or all NULL");
-
+    int rc = validate_config(cfg, 0);
+    if (rc) return rc;
     acf_solver *h = new (std::nothrow) acf_solver();
     if (!h) return fail(ACF_ERR_MEMORY, "host allocation failed");
-    cudaError_t e = cudaGetDevice(&h->device);
-    if (e != cudaSuccess) {
-        delete h;
-        return fail(ACF_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    rc = create_batch(1, cfg, h);
+    if (rc) {
+        free_batch(h);
+        return rc;
     }
-    h->precision = cfg->precision;
-    h->nx = cfg->nx;
-    h->ny = cfg->ny;
-    h->nz = cfg->nz;
-    h->n_relax = cfg->n_relax;
-    h->pz = round_up((int64_t)cfg->nz + 1, kRowAlign);
-    h->plane = (int64_t)(cfg->ny + 1) * h->pz;
-    h->field = (int64_t)(cfg->nx + 1) * h->plane;
-    h->has_layer = layer;
-    h->has_walls = walls;
-    h->coef[0] = cfg->vel_coef;
-    h->coef[1] = cfg->pres_coef;
-    h->coef[2] = cfg->src_coef;
-    h->coef[3] = cfg->relax_scale;
-    for (int r = 0; r < ACF_MAX_RELAXATION; r++) {
-        h->decay[r] = r < cfg->n_relax ? cfg->relax_decay[r] : 0.0;
-        h->mean[r] = r < cfg->n_relax ? cfg->relax_mean[r] : 0.0;
-        h->gain[r] = r < cfg->n_relax ? cfg->relax_gain[r] : 0.0;
-    }
-
-    auto cleanup = [&](int code) {
-        free_solver(h);
-        return code;
-    };
-    const size_t es = h->elem();
-    const size_t n_fields = 4 + (size_t)h->n_relax;
-    // One guard row past the last field keeps every vector access of the last row in bounds.
-    const size_t state_bytes = (n_fields * (size_t)h->field + (size_t)h->pz) * es;
-    if (cudaMalloc(&h->state, state_bytes) != cudaSuccess)
-        return cleanup(fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of state failed", state_bytes));
-    if (cudaMemset(h->state, 0, state_bytes) != cudaSuccess)
-        return cleanup(fail(ACF_ERR_CUDA, "cudaMemset of state failed"));
-    if (cudaMalloc(&h->step_base, sizeof(int64_t)) != cudaSuccess)
-        return cleanup(fail(ACF_ERR_MEMORY, "cudaMalloc of step counter failed"));
-    cudaMemset(h->step_base, 0, sizeof(int64_t));
-
-    const int64_t n_axis[3] = {cfg->nx, cfg->ny, cfg->nz};
-    if (layer) {
-        std::vector<double> host;
-        for (int a = 0; a < 3; a++) {
-            h->profile_off[a] = (int64_t)host.size();
-            host.insert(host.end(), cfg->cell[a], cfg->cell[a] + n_axis[a]);
-        }
-        for (int a = 0; a < 3; a++) {
-            h->profile_off[3 + a] = (int64_t)host.size();
-            host.insert(host.end(), cfg->face[a], cfg->face[a] + n_axis[a] + 1);
-        }
-        std::vector<char> cast(host.size() * es);
-        if (es == 4) cast_copy<float>(cast.data(), host.data(), host.size());
-        else cast_copy<double>(cast.data(), host.data(), host.size());
-        if (cudaMalloc(&h->profiles, cast.size()) != cudaSuccess)
-            return cleanup(fail(ACF_ERR_MEMORY, "cudaMalloc of layer profiles failed"));
-        if (cudaMemcpy(h->profiles, cast.data(), cast.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(ACF_ERR_CUDA, "copy of layer profiles failed"));
-    }
-    if (walls) {
-        std::vector<double> host;
-        for (int f = 0; f < 6; f++) {
-            const int axis = f / 2;
-            const int64_t nb = axis == 0 ? n_axis[1] : n_axis[0];
-            const int64_t nc = axis == 2 ? n_axis[1] : n_axis[2];
-            h->shell_off[f] = (int64_t)host.size();
-            host.insert(host.end(), cfg->wall_shell[f], cfg->wall_shell[f] + 2 * nb * nc);
-        }
-        std::vector<char> cast(host.size() * es);
-        if (es == 4) cast_copy<float>(cast.data(), host.data(), host.size());
-        else cast_copy<double>(cast.data(), host.data(), host.size());
-        if (cudaMalloc(&h->shell, cast.size()) != cudaSuccess)
-            return cleanup(fail(ACF_ERR_MEMORY, "cudaMalloc of wall shells failed"));
-        if (cudaMemcpy(h->shell, cast.data(), cast.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(ACF_ERR_CUDA, "copy of wall shells failed"));
-    }
-
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-    h->energy_blocks = 4 * sms;
-    const size_t scratch = ((size_t)h->energy_blocks + 1) * kEnergyTerms * sizeof(double);
-    if (cudaMalloc(&h->energy_scratch, scratch) != cudaSuccess)
-        return cleanup(fail(ACF_ERR_MEMORY, "cudaMalloc of energy scratch failed"));
-    for (auto &ev : h->ring)
-        if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(ACF_ERR_CUDA, "cudaEventCreate failed"));
     *out = h;
     return ACF_OK;
 }
 
 int acf_destroy(acf_solver *h) {
-    free_solver(h);
+    free_batch(h);
     return ACF_OK;
 }
 
@@ -994,207 +1443,152 @@ int acf_is_double(const acf_solver *h) { return h && h->precision == 8; }
 
 int acf_set_sources(acf_solver *h, int64_t n, const int64_t *cell, const int64_t *length,
                     const double *signal, int64_t stride) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (n < 0 || n > (1 << 20)) return fail(ACF_ERR_ARGUMENT, "source count %lld out of range", (long long)n);
-    if (n > 0 && (!cell || !length || (stride > 0 && !signal) || stride < 0))
-        return fail(ACF_ERR_ARGUMENT, "null source arrays");
-    DeviceGuard guard(h->device);
-    const int64_t n_cells = (int64_t)h->nx * h->ny * h->nz;
-    std::vector<int64_t> off((size_t)n), len((size_t)n);
-    for (int64_t q = 0; q < n; q++) {
-        if (cell[q] < 0 || cell[q] >= n_cells)
-            return fail(ACF_ERR_ARGUMENT, "source %lld cell %lld outside the grid", (long long)q, (long long)cell[q]);
-        if (length[q] < 0 || length[q] > stride)
-            return fail(ACF_ERR_ARGUMENT, "source %lld length %lld exceeds stride %lld", (long long)q,
-                        (long long)length[q], (long long)stride);
-        off[q] = padded_offset(h, cell[q]);
-        len[q] = length[q];
-    }
-    ACF_CUDA(cudaDeviceSynchronize());
-    cudaFree(h->src_off);
-    cudaFree(h->src_len);
-    cudaFree(h->src_sig);
-    h->src_off = h->src_len = nullptr;
-    h->src_sig = nullptr;
-    h->n_src = 0;
-    h->graph_dirty = true;
-    if (n == 0) return ACF_OK;
-    const size_t es = h->elem();
-    const size_t n_sig = (size_t)n * (size_t)std::max<int64_t>(stride, 1);
-    ACF_CUDA(cudaMalloc(&h->src_off, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMalloc(&h->src_len, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMalloc(&h->src_sig, n_sig * es));
-    ACF_CUDA(cudaMemcpy(h->src_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    ACF_CUDA(cudaMemcpy(h->src_len, len.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    std::vector<char> cast(n_sig * es, 0);
-    if (stride > 0) {
-        if (es == 4) cast_copy<float>(cast.data(), signal, (size_t)n * stride);
-        else cast_copy<double>(cast.data(), signal, (size_t)n * stride);
-    }
-    ACF_CUDA(cudaMemcpy(h->src_sig, cast.data(), cast.size(), cudaMemcpyHostToDevice));
-    h->n_src = n;
-    h->src_stride = stride;
-    return ACF_OK;
+    return set_sources(h, 0, n, cell, length, signal, stride);
 }
 
 int acf_set_receivers(acf_solver *h, int64_t n, const int64_t *cell, const int64_t *start_step) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (n < 0 || n > (1 << 20)) return fail(ACF_ERR_ARGUMENT, "receiver count %lld out of range", (long long)n);
-    if (n > 0 && (!cell || !start_step)) return fail(ACF_ERR_ARGUMENT, "null receiver arrays");
-    DeviceGuard guard(h->device);
-    const int64_t n_cells = (int64_t)h->nx * h->ny * h->nz;
-    std::vector<int64_t> off((size_t)n);
-    for (int64_t r = 0; r < n; r++) {
-        if (cell[r] < 0 || cell[r] >= n_cells)
-            return fail(ACF_ERR_ARGUMENT, "receiver %lld cell %lld outside the grid", (long long)r, (long long)cell[r]);
-        if (start_step[r] < 0) return fail(ACF_ERR_ARGUMENT, "negative start step");
-        off[r] = padded_offset(h, cell[r]);
-    }
-    ACF_CUDA(cudaDeviceSynchronize());
-    if (n > 0 && !h->rec_origin_set) {
-        h->rec_origin = *std::min_element(start_step, start_step + n);
-        h->rec_origin_set = true;
-    }
-    for (int64_t r = 0; r < n; r++)
-        if (start_step[r] < h->rec_origin)
-            return fail(ACF_ERR_ARGUMENT, "receiver %lld starts before the recording origin", (long long)r);
-    // Keep existing recordings: grow the row count, preserving rows already written.
-    const size_t es = h->elem();
-    if (n > 0 && h->rec_capacity > 0 && n != h->n_rec) {
-        void *grown = nullptr;
-        ACF_CUDA(cudaMalloc(&grown, (size_t)n * h->rec_capacity * es));
-        ACF_CUDA(cudaMemset(grown, 0, (size_t)n * h->rec_capacity * es));
-        const int64_t keep = std::min<int64_t>(n, h->n_rec);
-        if (keep > 0 && h->rec)
-            ACF_CUDA(cudaMemcpy(grown, h->rec, (size_t)keep * h->rec_capacity * es, cudaMemcpyDeviceToDevice));
-        cudaFree(h->rec);
-        h->rec = grown;
-    }
-    cudaFree(h->rec_off);
-    cudaFree(h->rec_start);
-    h->rec_off = h->rec_start = nullptr;
-    h->n_rec = 0;
-    h->graph_dirty = true;
-    h->host_rec_cell.assign(cell, cell + n);
-    h->host_rec_start.assign(start_step, start_step + n);
-    if (n == 0) return ACF_OK;
-    ACF_CUDA(cudaMalloc(&h->rec_off, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMalloc(&h->rec_start, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMemcpy(h->rec_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    ACF_CUDA(cudaMemcpy(h->rec_start, start_step, n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    h->n_rec = n;
-    return ACF_OK;
+    return set_receivers(h, 0, n, cell, start_step);
 }
 
 int acf_read_recording(acf_solver *h, int64_t r, int64_t first_step, int64_t n, void *dst,
                        acf_stream stream) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (r < 0 || r >= h->n_rec) return fail(ACF_ERR_ARGUMENT, "receiver %lld out of range", (long long)r);
-    if (n < 0 || (n > 0 && !dst)) return fail(ACF_ERR_ARGUMENT, "bad destination");
-    if (n == 0) return ACF_OK;
-    const int64_t col = first_step - h->rec_origin;
-    if (col < 0 || col + n > h->rec_capacity || first_step < h->host_rec_start[(size_t)r])
-        return fail(ACF_ERR_ARGUMENT, "steps [%lld, %lld) were not recorded by receiver %lld",
-                    (long long)first_step, (long long)(first_step + n), (long long)r);
-    DeviceGuard guard(h->device);
-    cudaStream_t st = (cudaStream_t)stream;
-    const size_t es = h->elem();
-    ACF_CUDA(cudaMemcpyAsync(dst, (char *)h->rec + ((size_t)r * h->rec_capacity + col) * es, (size_t)n * es,
-                             cudaMemcpyDeviceToHost, st));
-    ACF_CUDA(cudaStreamSynchronize(st));
-    return ACF_OK;
+    return read_recording(h, 0, r, first_step, n, dst, stream);
 }
 
 int acf_upload(acf_solver *h, int field, const void *src, acf_stream stream) {
-    int rc = check_field(h, field);
+    int rc = check_field(h, 0, field);
     if (rc) return rc;
     if (!src) return fail(ACF_ERR_ARGUMENT, "null source");
     DeviceGuard guard(h->device);
-    return copy_field(h, field, const_cast<void *>(src), true, (cudaStream_t)stream);
+    return copy_field(h, 0, field, const_cast<void *>(src), true, (cudaStream_t)stream);
 }
 
 int acf_download(acf_solver *h, int field, void *dst, acf_stream stream) {
-    int rc = check_field(h, field);
+    int rc = check_field(h, 0, field);
     if (rc) return rc;
     if (!dst) return fail(ACF_ERR_ARGUMENT, "null destination");
     DeviceGuard guard(h->device);
-    return copy_field(h, field, dst, false, (cudaStream_t)stream);
+    return copy_field(h, 0, field, dst, false, (cudaStream_t)stream);
 }
 
 int acf_run(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_stream stream) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
-    if (n_steps == 0) return ACF_OK;
-    DeviceGuard guard(h->device);
-    cudaStream_t st = (cudaStream_t)stream;
-    // Recording capacity for every step this run can write.
-    if (h->n_rec > 0) {
-        const int64_t need = step_offset + n_steps - h->rec_origin;
-        if (need > h->rec_capacity) {
-            int64_t cap = std::max<int64_t>(need, 2 * h->rec_capacity);
-            cap = round_up(cap, 256);
-            const size_t es = h->elem();
-            void *grown = nullptr;
-            ACF_CUDA(cudaStreamSynchronize(st));
-            ACF_CUDA(cudaMalloc(&grown, (size_t)h->n_rec * cap * es));
-            ACF_CUDA(cudaMemset(grown, 0, (size_t)h->n_rec * cap * es));
-            if (h->rec && h->rec_capacity > 0)
-                ACF_CUDA(cudaMemcpy2D(grown, (size_t)cap * es, h->rec, (size_t)h->rec_capacity * es,
-                                      (size_t)h->rec_capacity * es, (size_t)h->n_rec, cudaMemcpyDeviceToDevice));
-            cudaFree(h->rec);
-            h->rec = grown;
-            h->rec_capacity = cap;
-            h->graph_dirty = true;
-        }
-    }
-    return h->precision == 8 ? run_impl<double>(h, n_steps, step_offset, st)
-                             : run_impl<float>(h, n_steps, step_offset, st);
+    return run_batch(h, n_steps, step_offset, stream);
 }
 
-int acf_set_graph(acf_solver *h, int32_t steps) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (steps < 0 || steps > 4096) return fail(ACF_ERR_ARGUMENT, "steps_per_graph %d out of range", steps);
-    if (steps != h->graph_steps) h->graph_dirty = true;
-    h->graph_steps = steps;
-    return ACF_OK;
+int acf_set_graph(acf_solver *h, int32_t steps) { return acf_batch_set_graph(h, steps); }
+
+int acf_set_launch(acf_solver *h, int32_t block_threads, int32_t planes) {
+    return set_launch(h, block_threads, planes, h ? h->ctas_per_sm : 1);
 }
 
 int acf_energy_terms(acf_solver *h, double dx, double terms[7], acf_stream stream) {
-    if (!h || !terms) return fail(ACF_ERR_ARGUMENT, "null argument");
-    if (!(dx > 0)) return fail(ACF_ERR_ARGUMENT, "dx must be positive");
-    DeviceGuard guard(h->device);
-    cudaStream_t st = (cudaStream_t)stream;
-    return h->precision == 8 ? energy_impl<double>(h, dx, terms, st) : energy_impl<float>(h, dx, terms, st);
+    return energy_terms(h, 0, dx, terms, stream);
 }
 
 int acf_field_pointer(acf_solver *h, int field, void **ptr, int64_t strides[3]) {
-    int rc = check_field(h, field);
+    int rc = check_field(h, 0, field);
     if (rc) return rc;
     if (!ptr || !strides) return fail(ACF_ERR_ARGUMENT, "null output");
-    *ptr = h->field_ptr(field);
-    strides[0] = h->plane;
-    strides[1] = h->pz;
+    *ptr = h->field_ptr(0, field);
+    strides[0] = h->rooms[0].plane;
+    strides[1] = h->rooms[0].pz;
     strides[2] = 1;
     return ACF_OK;
 }
 
-int acf_profile_enable(acf_solver *h, int32_t enable) {
-    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
-    h->profiling = enable != 0;
-    h->prof_velocity_ms = h->prof_pressure_ms = 0;
-    h->prof_launches = 0;
-    return ACF_OK;
-}
+int acf_profile_enable(acf_solver *h, int32_t enable) { return profile_enable(h, enable); }
 
 int acf_profile_read(acf_solver *h, double *velocity_ms, double *pressure_ms, int64_t *launches) {
-    if (!h || !velocity_ms || !pressure_ms || !launches) return fail(ACF_ERR_ARGUMENT, "null argument");
-    *velocity_ms = h->prof_velocity_ms;
-    *pressure_ms = h->prof_pressure_ms;
-    *launches = h->prof_launches;
-    return ACF_OK;
+    return profile_read(h, velocity_ms, pressure_ms, launches);
 }
 
 int64_t acf_launch_count(const acf_solver *h) { return h ? h->launches : -1; }
+
+// ---- batches of rooms -------------------------------------------------------------------
+
+int acf_batch_create(int32_t n_rooms, const acf_config *configs, acf_batch **out) {
+    if (!configs || !out) return fail(ACF_ERR_ARGUMENT, "null configs or output pointer");
+    *out = nullptr;
+    if (n_rooms < 1 || n_rooms > (1 << 20))
+        return fail(ACF_ERR_ARGUMENT, "room count %d out of range", n_rooms);
+    acf_batch *b = new (std::nothrow) acf_batch();
+    if (!b) return fail(ACF_ERR_MEMORY, "host allocation failed");
+    int rc = create_batch(n_rooms, configs, b);
+    if (rc) {
+        free_batch(b);
+        return rc;
+    }
+    *out = b;
+    return ACF_OK;
+}
+
+int acf_batch_destroy(acf_batch *b) {
+    free_batch(b);
+    return ACF_OK;
+}
+
+int acf_batch_room_count(const acf_batch *b) { return b ? (int)b->rooms.size() : -1; }
+
+int acf_batch_set_sources(acf_batch *b, int32_t room, int64_t n, const int64_t *cell,
+                          const int64_t *length, const double *signal, int64_t stride) {
+    return set_sources(b, room, n, cell, length, signal, stride);
+}
+
+int acf_batch_set_receivers(acf_batch *b, int32_t room, int64_t n, const int64_t *cell,
+                            const int64_t *start_step) {
+    return set_receivers(b, room, n, cell, start_step);
+}
+
+int acf_batch_read_recording(acf_batch *b, int32_t room, int64_t receiver, int64_t first_step,
+                             int64_t n, void *dst, acf_stream stream) {
+    return read_recording(b, room, receiver, first_step, n, dst, stream);
+}
+
+int acf_batch_upload(acf_batch *b, int32_t room, int field, const void *src, acf_stream stream) {
+    int rc = check_field(b, room, field);
+    if (rc) return rc;
+    if (!src) return fail(ACF_ERR_ARGUMENT, "null source");
+    DeviceGuard guard(b->device);
+    return copy_field(b, room, field, const_cast<void *>(src), true, (cudaStream_t)stream);
+}
+
+int acf_batch_download(acf_batch *b, int32_t room, int field, void *dst, acf_stream stream) {
+    int rc = check_field(b, room, field);
+    if (rc) return rc;
+    if (!dst) return fail(ACF_ERR_ARGUMENT, "null destination");
+    DeviceGuard guard(b->device);
+    return copy_field(b, room, field, dst, false, (cudaStream_t)stream);
+}
+
+int acf_batch_run(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    return run_batch(b, n_steps, step_offset, stream);
+}
+
+int acf_batch_set_graph(acf_batch *b, int32_t steps) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (steps < 0 || steps > 4096) return fail(ACF_ERR_ARGUMENT, "steps_per_graph %d out of range", steps);
+    if (steps != b->graph_steps) b->graph_dirty = true;
+    b->graph_steps = steps;
+    return ACF_OK;
+}
+
+int acf_batch_set_launch(acf_batch *b, int32_t block_threads, int32_t planes, int32_t ctas_per_sm) {
+    return set_launch(b, block_threads, planes, ctas_per_sm);
+}
+
+int acf_batch_energy_terms(acf_batch *b, int32_t room, double dx, double terms[7], acf_stream stream) {
+    return energy_terms(b, room, dx, terms, stream);
+}
+
+int acf_batch_profile_enable(acf_batch *b, int32_t enable) { return profile_enable(b, enable); }
+
+int acf_batch_profile_read(acf_batch *b, double *velocity_ms, double *pressure_ms, int64_t *launches) {
+    return profile_read(b, velocity_ms, pressure_ms, launches);
+}
+
+int64_t acf_batch_launch_count(const acf_batch *b) { return b ? b->launches : -1; }
+
+// ---- utilities --------------------------------------------------------------------------
 
 int acf_energy_terms_noalloc(const void *p, const void *vx, const void *vy, const void *vz,
                              int32_t nx, int32_t ny, int32_t nz, int32_t precision, double dx,

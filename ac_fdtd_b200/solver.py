@@ -395,6 +395,11 @@ class CudaAcousticFDTD:
             coupling += terms[4 + axis]
         return float(self.grid.dx) ** 3 * (potential + kinetic - 0.5 * self.dt * coupling)
 
+    def set_launch(self, block_threads: int = 256, planes: int = 4) -> None:
+        """Launch geometry of the sweeps (threads per block, x planes per block)."""
+        _native.check(self._lib.acf_set_launch(self._handle, int(block_threads), int(planes)),
+                      "acf_set_launch")
+
     def launch_count(self) -> int:
         return int(self._lib.acf_launch_count(self._handle))
 

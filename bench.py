@@ -229,8 +229,11 @@ def run_ours(args) -> None:
 
     from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse, pinned_array
 
+    from ac_fdtd_b200.autotune import apply_tuned
+
     grid, objects, points = workload(args.size)
     solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
+    geometry = apply_tuned(solver)
     solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
     for point in points[1:]:
         solver.add_pressure_receiver(point)
@@ -327,7 +330,10 @@ def run_ours(args) -> None:
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(args, grid),
+        "data": "synthetic",
+        "config": {**config_dict(args, grid),
+                   "launch": {"block_threads": geometry[0], "planes_per_block": geometry[1],
+                              "chosen_by": "ac_fdtd_b200.autotune"}},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,

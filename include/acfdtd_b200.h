@@ -59,6 +59,7 @@ enum {
 };
 
 typedef struct acf_solver acf_solver;
+typedef struct acf_batch acf_batch;
 typedef void *acf_stream;
 
 /* Everything the two sweeps need, computed on the host in FP64.
@@ -131,6 +132,10 @@ int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream
 /* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
 int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);
 
+/* Launch geometry of both sweeps: threads per block (power of two, 32..256) and consecutive
+ * x planes each block marches through (1..1024). Results do not depend on it. */
+int acf_set_launch(acf_solver *solver, int32_t block_threads, int32_t planes);
+
 /* The seven FP64 sums the reference energy is built from, for the stored (p^n, v^{n-1/2})
  * pair (src/ac_fdtd/scheme.py:365-389): terms[0] = sum p^2; terms[1+a] = sum v_a^2 over all
  * faces; terms[4+a] = sum over interior faces of v_a * (p_hi - p_lo) / dx. Synchronous. */
@@ -172,6 +177,40 @@ int acf_profile_read(acf_solver *solver, double *velocity_ms, double *pressure_m
 
 /* Kernels launched by this handle since creation (sweeps, graph replays counted per kernel). */
 int64_t acf_launch_count(const acf_solver *solver);
+
+/* ---- Batches of rooms -------------------------------------------------------------------
+ *
+ * Many rooms of different sizes advanced together: each sweep is one persistent launch over a
+ * flat tile table covering every room, and runs replay CUDA graphs of both sweeps. No
+ * counterpart in the reference, whose solvers hold one room each (src/ac_fdtd/scheme.py:82);
+ * per room the arithmetic is exactly that of acf_create/acf_run, so each room's results equal
+ * a single-room run bit for bit. All rooms share the precision and the number of relaxation
+ * processes, and advance from the same step index. Room-level calls mirror the single-room
+ * ones with a room index. */
+int acf_batch_create(int32_t n_rooms, const acf_config *configs, acf_batch **out);
+int acf_batch_destroy(acf_batch *batch);
+int acf_batch_room_count(const acf_batch *batch);
+int acf_batch_set_sources(acf_batch *batch, int32_t room, int64_t n, const int64_t *cell,
+                          const int64_t *length, const double *signal, int64_t stride);
+int acf_batch_set_receivers(acf_batch *batch, int32_t room, int64_t n, const int64_t *cell,
+                            const int64_t *start_step);
+int acf_batch_read_recording(acf_batch *batch, int32_t room, int64_t receiver,
+                             int64_t first_step, int64_t n, void *dst, acf_stream stream);
+int acf_batch_upload(acf_batch *batch, int32_t room, int field, const void *src,
+                     acf_stream stream);
+int acf_batch_download(acf_batch *batch, int32_t room, int field, void *dst, acf_stream stream);
+int acf_batch_run(acf_batch *batch, int64_t n_steps, int64_t step_offset, acf_stream stream);
+int acf_batch_set_graph(acf_batch *batch, int32_t steps_per_graph);
+/* Threads per tile (power of two, 32..256), x planes per tile, resident CTAs per SM of the
+ * persistent grid. */
+int acf_batch_set_launch(acf_batch *batch, int32_t block_threads, int32_t planes,
+                         int32_t ctas_per_sm);
+int acf_batch_energy_terms(acf_batch *batch, int32_t room, double dx, double terms[7],
+                           acf_stream stream);
+int acf_batch_profile_enable(acf_batch *batch, int32_t enable);
+int acf_batch_profile_read(acf_batch *batch, double *velocity_ms, double *pressure_ms,
+                           int64_t *launches);
+int64_t acf_batch_launch_count(const acf_batch *batch);
 
 /* Block until all work queued on `stream` is done. */
 int acf_synchronize(acf_stream stream);
