@@ -31,8 +31,11 @@ EXPORTED_SYMBOLS = (
     "acf_batch_set_receivers", "acf_batch_read_recording", "acf_batch_upload",
     "acf_batch_download", "acf_batch_run", "acf_batch_set_graph", "acf_batch_set_launch",
     "acf_batch_energy_terms", "acf_batch_profile_enable", "acf_batch_profile_read",
-    "acf_batch_launch_count",
+    "acf_batch_launch_count", "acf_set_coefficients", "acf_adjoint_prepare",
+    "acf_adjoint_shell_size", "acf_forward_record", "acf_adjoint_run", "acf_adjoint_download",
 )
+
+GRAD_WALLS, GRAD_AIR = 1, 2
 
 
 class NativeError(RuntimeError):
@@ -110,6 +113,12 @@ _SIGNATURES = {
     "acf_batch_profile_enable": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_batch_profile_read": (ctypes.c_int, [_P, _DP, _DP, _I64P]),
     "acf_batch_launch_count": (ctypes.c_int64, [_P]),
+    "acf_set_coefficients": (ctypes.c_int, [_P, ctypes.POINTER(AcfConfig)]),
+    "acf_adjoint_prepare": (ctypes.c_int, [_P, ctypes.c_int32, _I64, ctypes.c_int32]),
+    "acf_adjoint_shell_size": (ctypes.c_int64, [_P]),
+    "acf_forward_record": (ctypes.c_int, [_P, _I64, _I64, _P]),
+    "acf_adjoint_run": (ctypes.c_int, [_P, _DP, _DP, _DP, _DP, _P]),
+    "acf_adjoint_download": (ctypes.c_int, [_P, ctypes.c_int, _P, _P]),
 }
 
 

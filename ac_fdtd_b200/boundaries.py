@@ -30,6 +30,8 @@ __all__ = [
     "layer_profiles",
     "wall_shell",
     "wall_cell_coefficients",
+    "WallPatches",
+    "patch_index",
 ]
 
 #: Face order used everywhere: (axis, side), side 0 = low, 1 = high (``boundaries.py:73``).
@@ -110,6 +112,51 @@ class AbsorbingLayer:
         return -(self.order + 1.0) * sound_speed * math.log(self.target_reflection) / (2.0 * depth)
 
 
+def patch_index(count: int, patches: int) -> np.ndarray:
+    """Patch of each of ``count`` cells along one wall axis: floor(i * patches / count)."""
+    return (np.arange(count) * patches) // count
+
+
+class WallPatches:
+    """Per-patch admittances: each wall split into ``patches x patches`` rectangles.
+
+    ``values`` has shape (6, patches, patches) in FACES order, each wall's patches indexed over
+    its two other axes in increasing order. A room whose patches on a wall are all equal is the
+    reference's ``WallAdmittances`` with that value. The reference has no per-patch walls
+    (its ``WallAdmittances`` holds six scalars, ``boundaries.py:120-146``).
+    """
+
+    def __init__(self, values) -> None:
+        values = np.asarray(values, dtype=np.float64)
+        if values.ndim != 3 or values.shape[0] != 6 or values.shape[1] != values.shape[2]:
+            raise ValueError(f"values must have shape (6, P, P), got {values.shape}")
+        if np.any(values < 0.0):
+            raise ValueError("negative admittance: that is a wall that generates sound")
+        self.patch_values = values
+
+    @property
+    def patches(self) -> int:
+        return self.patch_values.shape[1]
+
+    @property
+    def values(self) -> tuple[float, ...]:
+        """Mean admittance per wall (for code that wants six numbers)."""
+        return tuple(float(v.mean()) for v in self.patch_values)
+
+    def face_maps(self, shape) -> list[np.ndarray]:
+        maps = []
+        for f, (axis, _) in enumerate(FACES):
+            b, c = [a for a in range(3) if a != axis]
+            ib = patch_index(shape[b], self.patches)
+            ic = patch_index(shape[c], self.patches)
+            maps.append(self.patch_values[f][np.ix_(ib, ic)])
+        return maps
+
+    @classmethod
+    def uniform(cls, walls, patches: int) -> WallPatches:
+        return cls(np.repeat(np.asarray(walls.values, float)[:, None, None], patches, 1).repeat(patches, 2))
+
+
 def _face_maps(walls, shape) -> list[np.ndarray]:
     """Admittance of each face as a 2D map over its own (b, c) axes.
 
@@ -126,7 +173,8 @@ def _face_maps(walls, shape) -> list[np.ndarray]:
     return maps
 
 
-def wall_cell_coefficients(shape, sound_speed: float, dt: float, dx: float, walls):
+def wall_cell_coefficients(shape, sound_speed: float, dt: float, dx: float, walls,
+                           force: bool = False):
     """Per-face maps of the summed wall coefficient ``a`` for the cells on each face.
 
     ``a`` at a cell is the sum, in FACES order, of ``scale * xi_f`` over the faces f that touch
@@ -137,7 +185,7 @@ def wall_cell_coefficients(shape, sound_speed: float, dt: float, dx: float, wall
     coordinates. ``None`` when every wall is rigid.
     """
     maps = _face_maps(walls, shape)
-    if all(not np.any(m != 0.0) for m in maps):
+    if not force and all(not np.any(m != 0.0) for m in maps):
         return None
     scale = sound_speed * dt / (2.0 * dx)
     n = shape
@@ -158,13 +206,14 @@ def wall_cell_coefficients(shape, sound_speed: float, dt: float, dx: float, wall
     return out
 
 
-def wall_shell(shape, sound_speed: float, dt: float, dx: float, walls):
+def wall_shell(shape, sound_speed: float, dt: float, dx: float, walls, force: bool = False):
     """Six interleaved ``(1/(1+a), a/(1+a))`` arrays in FP64, or ``None`` when all rigid.
 
     The two factors are formed from ``a`` in FP64 exactly as ``scheme.py:156-157`` does before
-    casting to the working precision.
+    casting to the working precision. ``force`` returns the shells even for rigid walls (pairs
+    (1, 0), which leave the update unchanged), for solvers whose walls will be differentiated.
     """
-    sums = wall_cell_coefficients(shape, sound_speed, dt, dx, walls)
+    sums = wall_cell_coefficients(shape, sound_speed, dt, dx, walls, force)
     if sums is None:
         return None
     shells = []

@@ -55,7 +55,7 @@ def _rounded(dtype: np.dtype, value) -> float:
 
 
 def room_coefficients(grid, medium, courant: float, dtype, walls=None, absorbing_layer=None,
-                      air_absorption=None) -> RoomCoefficients:
+                      air_absorption=None, force_walls: bool = False) -> RoomCoefficients:
     """Host setup of ``AcousticFDTD.__init__`` (``scheme.py:107-212``) as one flat block."""
     if not 0.0 < courant <= 1.0:
         raise ValueError(f"courant must be in (0, 1], got {courant}")
@@ -95,7 +95,7 @@ def room_coefficients(grid, medium, courant: float, dtype, walls=None, absorbing
             gains.append(gain)
         block.relax_scale = _rounded(dtype, dt * sum(gains))
 
-    block.wall_shell = wall_shell(shape, c, dt, dx, walls)
+    block.wall_shell = wall_shell(shape, c, dt, dx, walls, force_walls)
     if absorbing_layer is not None:
         block.layer_cell, block.layer_face = layer_profiles(shape, dx, c, dt, absorbing_layer)
     return block

@@ -128,9 +128,26 @@ struct Room {
     int64_t rec_stride, rec_origin;
 };
 
+// Forward history kept for the adjoint (single rooms): per step, the pair (p^n, p-tilde^n) --
+// pressure before the step and before the wall closed form -- on every boundary cell, and, for a
+// segment of steps, the divergence D^n and the relaxation states psi^n before their update.
+// Boundary cells are indexed as in the wall shells: the first face of FACES order a cell lies
+// on, then row-major over that face's two other axes; face f starts at face_off[f].
+template <typename T>
+struct History {
+    T *shell;                      // steps x shell_total pairs, or null
+    int64_t shell_total, shell_step0, shell_steps;
+    int64_t face_off[6];
+    T *fields;                     // slots x (1 + n_relax) fields (padded geometry), or null
+    int64_t fields_step0;
+    int32_t fields_slots;
+    int32_t reserved;
+};
+
 template <typename T>
 struct StepParams {
     Room<T> room;
+    History<T> hist;
     const int64_t *step_base;      // absolute step of local step 0, in device memory
     int32_t local_step;
     int32_t planes;                // consecutive x planes marched by one block
@@ -259,24 +276,34 @@ __device__ __forceinline__ void velocity_column(const Room<T> &s, int i_begin, i
 // (b) pressure, one column. The velocities are read-only here; p and psi are read and written
 // by their owning thread only. vx of the upper face is carried into the next plane's lower face.
 
+// First face (FACES order) that cell (i, j, k) lies on, and its index within that face's
+// row-major (b, c) array; -1 for interior cells.
+template <typename T>
+__device__ __forceinline__ int shell_face(const Room<T> &s, int i, int j, int k, int64_t &idx) {
+    if (i == 0) { idx = (int64_t)j * s.nz + k; return 0; }
+    if (i == s.nx - 1) { idx = (int64_t)j * s.nz + k; return 1; }
+    if (j == 0) { idx = (int64_t)i * s.nz + k; return 2; }
+    if (j == s.ny - 1) { idx = (int64_t)i * s.nz + k; return 3; }
+    if (k == 0) { idx = (int64_t)i * s.ny + j; return 4; }
+    if (k == s.nz - 1) { idx = (int64_t)i * s.ny + j; return 5; }
+    return -1;
+}
+
 template <typename T>
 __device__ __forceinline__ bool wall_pair(const Room<T> &s, int i, int j, int k, T &fu, T &fp) {
-    const T *entry;
-    if (i == 0) entry = s.shell[0] + 2 * ((int64_t)j * s.nz + k);
-    else if (i == s.nx - 1) entry = s.shell[1] + 2 * ((int64_t)j * s.nz + k);
-    else if (j == 0) entry = s.shell[2] + 2 * ((int64_t)i * s.nz + k);
-    else if (j == s.ny - 1) entry = s.shell[3] + 2 * ((int64_t)i * s.nz + k);
-    else if (k == 0) entry = s.shell[4] + 2 * ((int64_t)i * s.ny + j);
-    else if (k == s.nz - 1) entry = s.shell[5] + 2 * ((int64_t)i * s.ny + j);
-    else return false;
+    int64_t idx;
+    const int f = shell_face(s, i, j, k, idx);
+    if (f < 0) return false;
+    const T *entry = s.shell[f] + 2 * idx;
     fu = __ldg(entry);
     fp = __ldg(entry + 1);
     return fp != T(0) || fu != T(1);
 }
 
-template <typename T, bool LAYER, bool WALLS, int NR>
+template <typename T, bool LAYER, bool WALLS, int NR, bool REC = false>
 __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, int i_end, int j,
-                                                int c, int64_t step) {
+                                                int c, int64_t step,
+                                                const History<T> *hist = nullptr) {
     const int k0 = c * kVec;
     const bool any_point = (s.n_src | s.n_rec) != 0;
     const bool has_above = k0 + kVec <= s.nz;
@@ -316,6 +343,16 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
             D[e] = D[e] + ((e + 1 < kVec ? Z[e + 1] : above) - Z[e]);
         }
 
+        if (REC && hist->fields) {
+            const int64_t slot = step - hist->fields_step0;
+            if (slot >= 0 && slot < hist->fields_slots) {
+                T *h = hist->fields + slot * (1 + NR) * s.field + base;
+                Vec4<T>::store(h, D);
+#pragma unroll
+                for (int r = 0; r < NR; r++) Vec4<T>::store(h + (1 + r) * s.field, S[r]);
+            }
+        }
+
         T Pn[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
@@ -332,6 +369,16 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
                 }
                 if (NR > 0) pe = pe + D[e] * s.relax_scale;
                 pe = pe - D[e] * cp;
+                if (REC && hist->shell) {
+                    int64_t idx;
+                    const int f = shell_face(s, i, j, k, idx);
+                    const int64_t slot = step - hist->shell_step0;
+                    if (f >= 0 && slot >= 0 && slot < hist->shell_steps) {
+                        T *h = hist->shell + 2 * (slot * hist->shell_total + hist->face_off[f] + idx);
+                        h[0] = P[e];
+                        h[1] = pe;
+                    }
+                }
                 if (WALLS) {
                     T fu, fp;
                     if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
@@ -404,6 +451,18 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 4)) pressure_sweep(
                                          c, step);
 }
 
+// The same pressure sweep, also writing the forward history the adjoint needs.
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) pressure_sweep_rec(const StepParams<T> p) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= p.room.nchunks || j >= p.room.ny) return;
+    const int64_t step = *p.step_base + p.local_step;
+    const int i_begin = blockIdx.z * p.planes;
+    pressure_column<T, LAYER, WALLS, NR, true>(p.room, i_begin, min(p.room.nx, i_begin + p.planes),
+                                               j, c, step, &p.hist);
+}
+
 // ------------------------------------------------------------------------------------------
 // Batches: a persistent grid walks the tile table with a static stride; no CTA waits on any
 // other. A CTA copies the description of its tile's room into shared memory when the room
@@ -458,6 +517,288 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) pressure_batch(
             pressure_column<T, LAYER, WALLS, NR>(*room, tile.i_begin, tile.i_end,
                                                  pair / room->nchunks, pair % room->nchunks,
                                                  step);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Adjoint: the transposed leapfrog, run backward in time (single rooms).
+//
+// The step is linear in the state x^n = (p^n, v^{n-1/2}, psi^n), so the adjoint recursion
+// lambda^n = A^T lambda^{n+1} needs no forward state; only parameter gradients read the forward
+// history. With mu the adjoint of the damped, gradient-updated face velocity and lambda_D the
+// adjoint of the divergence, the reverse of forward step n is two sweeps mirroring the forward:
+//
+//   cells: lp  = LP + c_v div_interior(mu^{n+1}) + dL/drec[n] (receiver cells)
+//          lp_hat = h lp ; lp_tilde = u lp_hat ; LP <- lp_tilde - q lp_hat        (walls: u, q)
+//          lambda_D = (S - c_p) lp_tilde + sum_r G_r ((1 - delta_r) lpsi_r - m_r lp_tilde)
+//          LPSI_r <- delta_r lpsi_r + m_r lp_tilde
+//          dL/dsignal_s[n] = c_s lp (source cells); dL/da (walls), dL/d(G, m, delta, S) (air)
+//   faces: mu_f = g_f (LV_f + lambda_D[lower cell] - lambda_D[upper cell]) -> LV
+//
+// where u = 1/(1+a), q = a/(1+a), h and g the layer products, S = dt sum G. The gradient of the
+// wall closed form p_hat = u p_tilde - q p with respect to a is -u^2 (p_tilde + p).
+
+template <typename T>
+struct AdjointParams {
+    Room<T> room;                  // coefficients, geometry, profiles, walls, points
+    T *lp, *lvx, *lvy, *lvz, *lpsi, *ld;  // adjoint fields (room geometry)
+    const double *grad_rec;        // n_rec rows of grad_stride, column = step - grad_step0
+    double *grad_src;              // n_src rows of grad_stride
+    int64_t grad_stride, grad_step0;
+    History<T> hist;
+    double *grad_shell;            // FP64 dL/da per boundary cell (shell index)
+    double *air_partials;          // per block: G_r (R), m_r (R), delta_r (R), S
+    int64_t step;                  // forward step being reversed
+    int32_t planes;
+    int32_t air;                   // accumulate air gradients (needs hist.fields)
+};
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParams<T> a) {
+    const Room<T> &s = a.room;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool active = c < s.nchunks && j < s.ny;
+    constexpr int NA = 3 * NR + 1;
+    double air_acc[NA];
+#pragma unroll
+    for (int t = 0; t < NA; t++) air_acc[t] = 0.0;
+
+    if (active) {
+        const int k0 = c * kVec;
+        const int i_begin = blockIdx.z * a.planes;
+        const int i_end = min(s.nx, i_begin + a.planes);
+        const int64_t column = (int64_t)j * s.pz + k0;
+        const bool has_above = k0 + kVec <= s.nz;
+        const int64_t step = a.step;
+        const T scp = s.relax_scale - s.cp;
+        T XL[kVec];
+        Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
+        for (int i = i_begin; i < i_end; i++) {
+            const int64_t base = (int64_t)i * s.plane + column;
+            T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
+            Vec4<T>::ldg(a.lvx + base + s.plane, XH);
+            Vec4<T>::ldg(a.lvy + base, YL);
+            Vec4<T>::ldg(a.lvy + base + s.pz, YH);
+            Vec4<T>::ldg(a.lvz + base, Z);
+            const T above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+            Vec4<T>::load(a.lp + base, L);
+#pragma unroll
+            for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
+            T HD[kVec], HS[NR > 0 ? NR : 1][kVec];
+            const bool air = NR > 0 && a.air;
+            if (air) {
+                const T *h = a.hist.fields + (step - a.hist.fields_step0) * (1 + NR) * s.field + base;
+                Vec4<T>::ldg(h, HD);
+#pragma unroll
+                for (int r = 0; r < NR; r++) Vec4<T>::ldg(h + (1 + r) * s.field, HS[r]);
+            }
+            T fi = T(1), fj = T(1);
+            if (LAYER) {
+                fi = __ldg(s.cell[0] + i);
+                fj = __ldg(s.cell[1] + j);
+            }
+            T LD[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                const int k = k0 + e;
+                LD[e] = T(0);
+                if (k >= s.nz) continue;
+                // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}
+                const T up = e + 1 < kVec ? Z[e + 1] : above;
+                T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
+                dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
+                dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
+                T lp = L[e] + s.cv * dmu;
+                const int64_t cell = base + e;
+                for (int r = 0; r < s.n_rec; r++)
+                    if (s.rec_off[r] == cell && step >= s.rec_start[r])
+                        lp = lp + (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
+                for (int q = 0; q < s.n_src; q++)
+                    if (s.src_off[q] == cell && step < s.src_len[q])
+                        a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * lp);
+                T lph = lp;
+                if (LAYER) {
+                    lph = lph * fi;
+                    lph = lph * fj;
+                    lph = lph * __ldg(s.cell[2] + k);
+                }
+                T lpt = lph, lpart = lph;
+                if (WALLS) {
+                    int64_t idx;
+                    const int f = shell_face(s, i, j, k, idx);
+                    if (f >= 0) {
+                        const T *entry = s.shell[f] + 2 * idx;
+                        const T u = __ldg(entry), q = __ldg(entry + 1);
+                        lpt = u * lph;
+                        lpart = lpt - q * lph;
+                        if (a.grad_shell) {
+                            const T *h = a.hist.shell + 2 * ((step - a.hist.shell_step0) * a.hist.shell_total +
+                                                             a.hist.face_off[f] + idx);
+                            const double uu = (double)u;
+                            a.grad_shell[a.hist.face_off[f] + idx] +=
+                                -(double)lph * uu * uu * ((double)h[1] + (double)h[0]);
+                        }
+                    }
+                }
+                T ld = scp * lpt;
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T lpsi = LS[r][e];
+                    ld = ld + s.gain[r] * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
+                    LS[r][e] = s.decay[r] * lpsi + s.mean[r] * lpt;
+                    if (air) {
+                        const double d = (double)HD[e];
+                        const double off = (double)HS[r][e] - (double)s.gain[r] * d;
+                        air_acc[r] += d * ((1.0 - (double)s.decay[r]) * (double)lpsi -
+                                           (double)s.mean[r] * (double)lpt);
+                        air_acc[NR + r] += (double)lpt * off;
+                        air_acc[2 * NR + r] += (double)lpsi * off;
+                    }
+                }
+                if (air) air_acc[3 * NR] += (double)HD[e] * (double)lpt;
+                L[e] = lpart;
+                LD[e] = ld;
+            }
+            Vec4<T>::store(a.lp + base, L);
+            Vec4<T>::store(a.ld + base, LD);
+#pragma unroll
+            for (int r = 0; r < NR; r++) Vec4<T>::store(a.lpsi + r * s.field + base, LS[r]);
+#pragma unroll
+            for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+        }
+    }
+
+    if (NR > 0 && a.air) {  // uniform per launch: every thread reaches the barrier
+        __shared__ double red[NA][8];
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+        const int lane = tid & 31, warp = tid >> 5;
+        const int n_warps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+        for (int t = 0; t < NA; t++) {
+            double v = air_acc[t];
+            for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+            if (lane == 0) red[t][warp] = v;
+        }
+        __syncthreads();
+        if (tid < NA) {
+            double v = 0.0;
+            for (int w = 0; w < n_warps; w++) v += red[tid][w];
+            const int64_t block = ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            a.air_partials[block * NA + tid] += v;
+        }
+    }
+}
+
+template <typename T, bool LAYER>
+__global__ void __launch_bounds__(256) adjoint_velocity_sweep(const AdjointParams<T> a) {
+    const Room<T> &s = a.room;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= s.nchunks || j >= s.ny) return;
+    const int k0 = c * kVec;
+    const int i_begin = blockIdx.z * a.planes;
+    const int i_end = min(s.nx, i_begin + a.planes);
+    const int64_t column = (int64_t)j * s.pz + k0;
+    T Dm[kVec];  // lambda_D at plane i - 1
+    if (i_begin > 0) Vec4<T>::ldg(a.ld + (int64_t)(i_begin - 1) * s.plane + column, Dm);
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        T Dc[kVec], Dy[kVec], VX[kVec], VY[kVec], VZ[kVec];
+        Vec4<T>::ldg(a.ld + base, Dc);
+        if (j > 0) Vec4<T>::ldg(a.ld + base - s.pz, Dy);
+        const T below = k0 > 0 ? __ldg(a.ld + base - 1) : T(0);
+        Vec4<T>::load(a.lvx + base, VX);
+        Vec4<T>::load(a.lvy + base, VY);
+        Vec4<T>::load(a.lvz + base, VZ);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            if (k >= s.nz) continue;
+            T mx = VX[e] + ((i > 0 ? Dm[e] : T(0)) - Dc[e]);
+            T my = VY[e] + ((j > 0 ? Dy[e] : T(0)) - Dc[e]);
+            T mz = VZ[e] + ((k > 0 ? (e == 0 ? below : Dc[e - 1]) : T(0)) - Dc[e]);
+            if (LAYER) {
+                const T fi_cell = __ldg(s.cell[0] + i), fi_face = __ldg(s.face[0] + i);
+                const T fj_cell = __ldg(s.cell[1] + j), fj_face = __ldg(s.face[1] + j);
+                const T fk_cell = __ldg(s.cell[2] + k), fk_face = __ldg(s.face[2] + k);
+                mx = ((mx * fi_face) * fj_cell) * fk_cell;
+                my = ((my * fi_cell) * fj_face) * fk_cell;
+                mz = ((mz * fi_cell) * fj_cell) * fk_face;
+            }
+            VX[e] = mx;
+            VY[e] = my;
+            VZ[e] = mz;
+        }
+        Vec4<T>::store(a.lvx + base, VX);
+        Vec4<T>::store(a.lvy + base, VY);
+        Vec4<T>::store(a.lvz + base, VZ);
+        // Far boundary faces: read by the divergence of the last cell, so they carry its lambda_D.
+        T fi_cell = T(1), fj_cell = T(1);
+        if (LAYER) {
+            fi_cell = __ldg(s.cell[0] + i);
+            fj_cell = __ldg(s.cell[1] + j);
+        }
+        if (i == s.nx - 1) {
+            T V[kVec];
+            Vec4<T>::load(a.lvx + base + s.plane, V);
+#pragma unroll
+            for (int e = 0; e < kVec; e++)
+                if (k0 + e < s.nz) {
+                    T m = V[e] + Dc[e];
+                    if (LAYER) m = ((m * __ldg(s.face[0] + s.nx)) * fj_cell) * __ldg(s.cell[2] + k0 + e);
+                    V[e] = m;
+                }
+            Vec4<T>::store(a.lvx + base + s.plane, V);
+        }
+        if (j == s.ny - 1) {
+            T V[kVec];
+            Vec4<T>::load(a.lvy + base + s.pz, V);
+#pragma unroll
+            for (int e = 0; e < kVec; e++)
+                if (k0 + e < s.nz) {
+                    T m = V[e] + Dc[e];
+                    if (LAYER) m = ((m * fi_cell) * __ldg(s.face[1] + s.ny)) * __ldg(s.cell[2] + k0 + e);
+                    V[e] = m;
+                }
+            Vec4<T>::store(a.lvy + base + s.pz, V);
+        }
+        if (s.nz - 1 >= k0 && s.nz - 1 < k0 + kVec) {
+            T last = Dc[0];
+#pragma unroll
+            for (int e = 1; e < kVec; e++)
+                if (k0 + e == s.nz - 1) last = Dc[e];
+            T *top = a.lvz + (base - k0) + s.nz;
+            T m = *top + last;
+            if (LAYER) m = ((m * fi_cell) * fj_cell) * __ldg(s.face[2] + s.nz);
+            *top = m;
+        }
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Dm[e] = Dc[e];
+    }
+}
+
+// lambda(p^0) = LP + c_v div_interior(mu^0): the gradient with respect to the initial pressure.
+template <typename T>
+__global__ void __launch_bounds__(256) adjoint_finish(const AdjointParams<T> a) {
+    const Room<T> &s = a.room;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= s.nchunks || j >= s.ny) return;
+    const int k0 = c * kVec;
+    const int i_begin = blockIdx.z * a.planes;
+    const int i_end = min(s.nx, i_begin + a.planes);
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + (int64_t)j * s.pz + k0;
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            if (k >= s.nz) continue;
+            const int64_t o = base + e;
+            T dmu = (i + 1 < s.nx ? a.lvx[o + s.plane] : T(0)) - (i > 0 ? a.lvx[o] : T(0));
+            dmu = dmu + ((j + 1 < s.ny ? a.lvy[o + s.pz] : T(0)) - (j > 0 ? a.lvy[o] : T(0)));
+            dmu = dmu + ((k + 1 < s.nz ? a.lvz[o + 1] : T(0)) - (k > 0 ? a.lvz[o] : T(0)));
+            a.lp[o] = a.lp[o] + s.cv * dmu;
         }
     }
 }
@@ -714,8 +1055,29 @@ struct acf_batch {
 
     int64_t launches = 0;
 
+    // adjoint (single rooms)
+    struct Adjoint {
+        int32_t flags = 0;
+        int64_t capacity = 0;        // steps a forward record may hold
+        int32_t every = 0;           // checkpoint interval
+        int64_t recorded = 0, step0 = 0;
+        int64_t shell_total = 0;
+        int64_t face_off[6] = {};
+        void *hist_shell = nullptr;  // capacity x shell_total pairs
+        void *checkpoints = nullptr; // ceil(capacity / every) room states
+        void *scratch = nullptr;     // recompute state
+        void *segment = nullptr;     // every x (1 + n_relax) fields
+        void *fields = nullptr;      // (5 + n_relax) adjoint fields
+        double *grad_shell = nullptr;
+        double *air_partials = nullptr;
+        int64_t air_blocks = 0;
+        double *grad_rec = nullptr, *grad_src = nullptr;
+        int64_t grad_rows_rec = 0, grad_rows_src = 0;
+    } adj;
+
     size_t elem() const { return (size_t)precision; }
     int n_fields() const { return 4 + n_relax; }
+    size_t room_block_bytes(int r) const { return (size_t)n_fields() * rooms[r].field * elem(); }
     char *field_ptr(int r, int f) const {
         return (char *)state + rooms[r].state_off + (size_t)f * rooms[r].field * elem();
     }
@@ -726,8 +1088,10 @@ struct acf_solver : acf_batch {};
 
 namespace {
 
+// `state` (optional) points at another copy of the room's fields in the same geometry, such as
+// the adjoint's recompute buffer.
 template <typename T>
-Room<T> make_room(const acf_batch *b, int r) {
+Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     const RoomHost &h = b->rooms[r];
     Room<T> s{};
     s.nx = h.nx;
@@ -737,11 +1101,12 @@ Room<T> make_room(const acf_batch *b, int r) {
     s.pz = h.pz;
     s.plane = h.plane;
     s.field = h.field;
-    s.p = (T *)b->field_ptr(r, ACF_FIELD_P);
-    s.vx = (T *)b->field_ptr(r, ACF_FIELD_VX);
-    s.vy = (T *)b->field_ptr(r, ACF_FIELD_VY);
-    s.vz = (T *)b->field_ptr(r, ACF_FIELD_VZ);
-    s.psi = (T *)b->field_ptr(r, ACF_FIELD_PSI0);
+    T *fields = state ? (T *)state : (T *)b->field_ptr(r, ACF_FIELD_P);
+    s.p = fields;
+    s.vx = fields + h.field;
+    s.vy = fields + 2 * h.field;
+    s.vz = fields + 3 * h.field;
+    s.psi = fields + 4 * h.field;
     s.cv = (T)h.coef[0];
     s.cp = (T)h.coef[1];
     s.cs = (T)h.coef[2];
@@ -1056,6 +1421,15 @@ void free_batch(acf_batch *b) {
     for (auto &e : b->ring)
         if (e) cudaEventDestroy(e);
     for (auto &r : b->rooms) free_room(r);
+    cudaFree(b->adj.hist_shell);
+    cudaFree(b->adj.checkpoints);
+    cudaFree(b->adj.scratch);
+    cudaFree(b->adj.segment);
+    cudaFree(b->adj.fields);
+    cudaFree(b->adj.grad_shell);
+    cudaFree(b->adj.air_partials);
+    cudaFree(b->adj.grad_rec);
+    cudaFree(b->adj.grad_src);
     cudaFree(b->state);
     cudaFree(b->room_table);
     cudaFree(b->tiles);
@@ -1399,6 +1773,301 @@ int energy_terms(acf_batch *b, int room, double dx, double terms[7], acf_stream 
 
 }  // namespace
 
+// ------------------------------------------------------------------------------------------
+// Adjoint orchestration (single rooms).
+
+namespace {
+
+template <typename T, bool L, bool W, int NR>
+struct RecPressure {
+    static void launch(const StepParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        pressure_sweep_rec<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct AdjPressure {
+    static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        adjoint_pressure_sweep<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T>
+History<T> make_history(const acf_batch *b) {
+    History<T> h{};
+    h.shell_total = b->adj.shell_total;
+    for (int f = 0; f < 6; f++) h.face_off[f] = b->adj.face_off[f];
+    return h;
+}
+
+// Forward steps [step_offset, step_offset + n) on `state` (the room's own fields, or the
+// recompute copy), writing the history described by `hist`. Receivers record only when
+// `receivers` is set, so a recompute leaves the caller's recordings alone.
+template <typename T>
+void record_steps(acf_batch *b, const void *state, const History<T> &hist, int64_t step_offset,
+                  int64_t n, bool receivers, cudaStream_t st, bool checkpoints) {
+    const RoomHost &h = b->rooms[0];
+    StepParams<T> p{};
+    p.room = make_room<T>(b, 0, state);
+    if (!receivers) p.room.n_rec = 0;
+    p.hist = hist;
+    p.step_base = b->step_base;
+    p.planes = b->planes;
+    const LaunchShape L = single_shape(b);
+    set_step_base<<<1, 1, 0, st>>>(b->step_base, step_offset);
+    b->launches += 1;
+    for (int64_t t = 0; t < n; t++) {
+        const int64_t absolute = step_offset + t;
+        if (checkpoints && (absolute - b->adj.step0) % b->adj.every == 0) {
+            const int64_t slot = (absolute - b->adj.step0) / b->adj.every;
+            cudaMemcpyAsync((char *)b->adj.checkpoints + slot * b->room_block_bytes(0), state,
+                            b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st);
+        }
+        p.local_step = (int32_t)t;
+        if (h.has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(p);
+        else velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(p);
+        dispatch_pressure<T, RecPressure>(h.has_layer, h.has_walls, h.n_relax, p, L.grid, L.block, st);
+        b->launches += 2;
+    }
+}
+
+template <typename T>
+int forward_record_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
+    b->adj.recorded = n_steps;
+    b->adj.step0 = step_offset;
+    History<T> hist = make_history<T>(b);
+    hist.shell = (T *)b->adj.hist_shell;
+    hist.shell_step0 = step_offset;
+    hist.shell_steps = b->adj.hist_shell ? n_steps : 0;
+    record_steps<T>(b, b->field_ptr(0, ACF_FIELD_P), hist, step_offset, n_steps, true, st,
+                    (b->adj.flags & ACF_GRAD_AIR) != 0);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+template <typename T>
+int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double *grad_shell,
+                 double *grad_air, cudaStream_t st) {
+    auto &A = b->adj;
+    const RoomHost &h = b->rooms[0];
+    const int64_t n = A.recorded;
+    const size_t es = b->elem();
+    const bool air = (A.flags & ACF_GRAD_AIR) && h.n_relax > 0;
+    const bool walls = (A.flags & ACF_GRAD_WALLS) && h.has_walls;
+    if (grad_shell && !walls)
+        return fail(ACF_ERR_STATE, "wall gradients need a room with wall coefficients and ACF_GRAD_WALLS");
+    if (grad_air && !air)
+        return fail(ACF_ERR_STATE, "air gradients need relaxation states and ACF_GRAD_AIR");
+
+    // Device inputs and zeroed accumulators.
+    if (h.n_rec > 0) {
+        cudaFree(A.grad_rec);
+        A.grad_rec = nullptr;
+        ACF_CUDA(cudaMalloc(&A.grad_rec, (size_t)h.n_rec * n * sizeof(double)));
+        ACF_CUDA(cudaMemcpyAsync(A.grad_rec, grad_rec, (size_t)h.n_rec * n * sizeof(double),
+                                 cudaMemcpyHostToDevice, st));
+    }
+    cudaFree(A.grad_src);
+    A.grad_src = nullptr;
+    if (h.n_src > 0) {
+        ACF_CUDA(cudaMalloc(&A.grad_src, (size_t)h.n_src * n * sizeof(double)));
+        ACF_CUDA(cudaMemsetAsync(A.grad_src, 0, (size_t)h.n_src * n * sizeof(double), st));
+    }
+    const size_t adj_bytes = ((size_t)(5 + h.n_relax) * h.field + h.pz) * es;
+    ACF_CUDA(cudaMemsetAsync(A.fields, 0, adj_bytes, st));
+    if (A.grad_shell) ACF_CUDA(cudaMemsetAsync(A.grad_shell, 0, A.shell_total * sizeof(double), st));
+    const LaunchShape L = single_shape(b);
+    const int64_t blocks = (int64_t)L.grid.x * L.grid.y * L.grid.z;
+    const int NA = 3 * h.n_relax + 1;
+    if (air) {
+        if (A.air_blocks < blocks) {
+            cudaFree(A.air_partials);
+            A.air_partials = nullptr;
+            ACF_CUDA(cudaMalloc(&A.air_partials, (size_t)blocks * NA * sizeof(double)));
+            A.air_blocks = blocks;
+        }
+        ACF_CUDA(cudaMemsetAsync(A.air_partials, 0, (size_t)blocks * NA * sizeof(double), st));
+    }
+
+    AdjointParams<T> a{};
+    a.room = make_room<T>(b, 0);
+    T *f = (T *)A.fields;
+    a.lp = f;
+    a.lvx = f + h.field;
+    a.lvy = f + 2 * h.field;
+    a.lvz = f + 3 * h.field;
+    a.lpsi = f + 4 * h.field;
+    a.ld = f + (4 + h.n_relax) * h.field;
+    a.grad_rec = A.grad_rec;
+    a.grad_src = A.grad_src;
+    a.grad_stride = n;
+    a.grad_step0 = A.step0;
+    a.hist = make_history<T>(b);
+    a.hist.shell = (T *)A.hist_shell;
+    a.hist.shell_step0 = A.step0;
+    a.hist.shell_steps = n;
+    a.hist.fields = (T *)A.segment;
+    a.grad_shell = walls ? A.grad_shell : nullptr;
+    a.air_partials = A.air_partials;
+    a.planes = b->planes;
+    a.air = air ? 1 : 0;
+
+    const int64_t K = air ? A.every : n;
+    const int64_t n_seg = (n + K - 1) / K;
+    for (int64_t seg = n_seg - 1; seg >= 0; seg--) {
+        const int64_t s0 = A.step0 + seg * K;
+        const int64_t s1 = std::min(s0 + K, A.step0 + n);
+        if (air) {
+            // Recompute the segment from its checkpoint, keeping D and psi of every step.
+            ACF_CUDA(cudaMemcpyAsync(A.scratch, (char *)A.checkpoints + seg * b->room_block_bytes(0),
+                                     b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st));
+            History<T> hist = make_history<T>(b);
+            hist.fields = (T *)A.segment;
+            hist.fields_step0 = s0;
+            hist.fields_slots = (int32_t)K;
+            record_steps<T>(b, A.scratch, hist, s0, s1 - s0, false, st, false);
+            a.hist.fields_step0 = s0;
+            a.hist.fields_slots = (int32_t)K;
+        }
+        for (int64_t step = s1 - 1; step >= s0; step--) {
+            a.step = step;
+            dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, a, L.grid, L.block, st);
+            if (h.has_layer) adjoint_velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(a);
+            else adjoint_velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(a);
+            b->launches += 2;
+        }
+    }
+    adjoint_finish<T><<<L.grid, L.block, 0, st>>>(a);
+    b->launches += 1;
+    ACF_CUDA(cudaGetLastError());
+
+    if (grad_src && h.n_src > 0)
+        ACF_CUDA(cudaMemcpyAsync(grad_src, A.grad_src, (size_t)h.n_src * n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    if (grad_shell)
+        ACF_CUDA(cudaMemcpyAsync(grad_shell, A.grad_shell, A.shell_total * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    std::vector<double> partials;
+    if (grad_air) {
+        partials.resize((size_t)blocks * NA);
+        ACF_CUDA(cudaMemcpyAsync(partials.data(), A.air_partials, partials.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    ACF_CUDA(cudaStreamSynchronize(st));
+    if (grad_air) {
+        for (int t = 0; t < NA; t++) grad_air[t] = 0.0;
+        for (int64_t blk = 0; blk < blocks; blk++)
+            for (int t = 0; t < NA; t++) grad_air[t] += partials[(size_t)blk * NA + t];
+    }
+    return ACF_OK;
+}
+
+int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t every) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (b->rooms.size() != 1) return fail(ACF_ERR_STATE, "the adjoint is for single rooms");
+    if (max_steps < 1) return fail(ACF_ERR_ARGUMENT, "max_steps must be >= 1");
+    if ((flags & ACF_GRAD_AIR) && (every < 1 || every > max_steps))
+        return fail(ACF_ERR_ARGUMENT, "checkpoint interval %d out of range", every);
+    DeviceGuard guard(b->device);
+    ACF_CUDA(cudaDeviceSynchronize());
+    auto &A = b->adj;
+    void **buffers[] = {&A.hist_shell, &A.checkpoints, &A.scratch, &A.segment, &A.fields};
+    for (void **p : buffers) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    cudaFree(A.grad_shell);
+    A.grad_shell = nullptr;
+    const RoomHost &h = b->rooms[0];
+    const size_t es = b->elem();
+    A.flags = flags;
+    A.capacity = max_steps;
+    A.every = (flags & ACF_GRAD_AIR) ? every : (int32_t)std::min<int64_t>(max_steps, INT32_MAX);
+    A.recorded = 0;
+    const int64_t sizes[6] = {(int64_t)h.ny * h.nz, (int64_t)h.ny * h.nz, (int64_t)h.nx * h.nz,
+                              (int64_t)h.nx * h.nz, (int64_t)h.nx * h.ny, (int64_t)h.nx * h.ny};
+    A.shell_total = 0;
+    for (int q = 0; q < 6; q++) {
+        A.face_off[q] = A.shell_total;
+        A.shell_total += sizes[q];
+    }
+    const size_t adj_bytes = ((size_t)(5 + h.n_relax) * h.field + h.pz) * es;
+    ACF_CUDA(cudaMalloc(&A.fields, adj_bytes));
+    if ((flags & ACF_GRAD_WALLS) && h.has_walls) {
+        const size_t bytes = (size_t)max_steps * A.shell_total * 2 * es;
+        if (cudaMalloc(&A.hist_shell, bytes) != cudaSuccess)
+            return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of wall history failed", bytes);
+        ACF_CUDA(cudaMalloc(&A.grad_shell, A.shell_total * sizeof(double)));
+    }
+    if ((flags & ACF_GRAD_AIR) && h.n_relax > 0) {
+        const int64_t n_ckpt = (max_steps + every - 1) / every;
+        const size_t block = b->room_block_bytes(0);
+        if (cudaMalloc(&A.checkpoints, (size_t)n_ckpt * block) != cudaSuccess)
+            return fail(ACF_ERR_MEMORY, "cudaMalloc of %lld checkpoints failed", (long long)n_ckpt);
+        ACF_CUDA(cudaMalloc(&A.scratch, block + (size_t)h.pz * es));
+        ACF_CUDA(cudaMemset(A.scratch, 0, block + (size_t)h.pz * es));
+        const size_t seg = ((size_t)every * (1 + h.n_relax) * h.field + h.pz) * es;
+        if (cudaMalloc(&A.segment, seg) != cudaSuccess)
+            return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of segment history failed", seg);
+        ACF_CUDA(cudaMemset(A.segment, 0, seg));
+    }
+    return ACF_OK;
+}
+
+int set_coefficients(acf_batch *b, int room, const acf_config *c) {
+    int rc = check_room(b, room);
+    if (rc) return rc;
+    if (!c) return fail(ACF_ERR_ARGUMENT, "null config");
+    RoomHost &h = b->rooms[room];
+    rc = validate_config(c, room);
+    if (rc) return rc;
+    if (c->nx != h.nx || c->ny != h.ny || c->nz != h.nz || c->precision != b->precision ||
+        c->n_relax != h.n_relax)
+        return fail(ACF_ERR_ARGUMENT, "new coefficients must keep the grid, precision and relaxation count");
+    if ((c->cell[0] != nullptr) != h.has_layer || (c->wall_shell[0] != nullptr) != h.has_walls)
+        return fail(ACF_ERR_ARGUMENT, "new coefficients must keep which of layer and walls are present");
+    DeviceGuard guard(b->device);
+    ACF_CUDA(cudaDeviceSynchronize());
+    h.coef[0] = c->vel_coef;
+    h.coef[1] = c->pres_coef;
+    h.coef[2] = c->src_coef;
+    h.coef[3] = c->relax_scale;
+    for (int q = 0; q < ACF_MAX_RELAXATION; q++) {
+        h.decay[q] = q < c->n_relax ? c->relax_decay[q] : 0.0;
+        h.mean[q] = q < c->n_relax ? c->relax_mean[q] : 0.0;
+        h.gain[q] = q < c->n_relax ? c->relax_gain[q] : 0.0;
+    }
+    const size_t es = b->elem();
+    const int64_t n_axis[3] = {c->nx, c->ny, c->nz};
+    if (h.has_layer) {
+        std::vector<double> host;
+        for (int a = 0; a < 3; a++) host.insert(host.end(), c->cell[a], c->cell[a] + n_axis[a]);
+        for (int a = 0; a < 3; a++) host.insert(host.end(), c->face[a], c->face[a] + n_axis[a] + 1);
+        std::vector<char> cast(host.size() * es);
+        if (es == 4) cast_copy<float>(cast.data(), host.data(), host.size());
+        else cast_copy<double>(cast.data(), host.data(), host.size());
+        ACF_CUDA(cudaMemcpy(h.profiles, cast.data(), cast.size(), cudaMemcpyHostToDevice));
+    }
+    if (h.has_walls) {
+        std::vector<double> host;
+        for (int f = 0; f < 6; f++) {
+            const int axis = f / 2;
+            const int64_t nb = axis == 0 ? n_axis[1] : n_axis[0];
+            const int64_t nc = axis == 2 ? n_axis[1] : n_axis[2];
+            host.insert(host.end(), c->wall_shell[f], c->wall_shell[f] + 2 * nb * nc);
+        }
+        std::vector<char> cast(host.size() * es);
+        if (es == 4) cast_copy<float>(cast.data(), host.data(), host.size());
+        else cast_copy<double>(cast.data(), host.data(), host.size());
+        ACF_CUDA(cudaMemcpy(h.shell, cast.data(), cast.size(), cudaMemcpyHostToDevice));
+    }
+    b->graph_dirty = true;
+    b->room_table_dirty = true;
+    return ACF_OK;
+}
+
+}  // namespace
+
 // ==========================================================================================
 // C ABI
 
@@ -1503,6 +2172,82 @@ int acf_profile_read(acf_solver *h, double *velocity_ms, double *pressure_ms, in
 }
 
 int64_t acf_launch_count(const acf_solver *h) { return h ? h->launches : -1; }
+
+int acf_set_coefficients(acf_solver *h, const acf_config *config) {
+    return set_coefficients(h, 0, config);
+}
+
+int acf_adjoint_prepare(acf_solver *h, int32_t flags, int64_t max_steps, int32_t checkpoint_every) {
+    return adjoint_prepare(h, flags, max_steps, checkpoint_every);
+}
+
+int64_t acf_adjoint_shell_size(const acf_solver *h) { return h ? h->adj.shell_total : -1; }
+
+int acf_forward_record(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (!h->adj.fields) return fail(ACF_ERR_STATE, "call acf_adjoint_prepare first");
+    if (n_steps < 1 || n_steps > h->adj.capacity)
+        return fail(ACF_ERR_ARGUMENT, "n_steps %lld outside 1..%lld prepared", (long long)n_steps,
+                    (long long)h->adj.capacity);
+    if (step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step offset");
+    DeviceGuard guard(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    // Recording capacity as acf_run ensures it.
+    int rc = ACF_OK;
+    for (RoomHost &r : h->rooms) {
+        if (r.n_rec == 0) continue;
+        const int64_t need = step_offset + n_steps - r.rec_origin;
+        if (need <= r.rec_capacity) continue;
+        // Reuse acf_run's growth path with a zero-step run is not possible; grow here.
+        int64_t cap = round_up(std::max<int64_t>(need, 2 * r.rec_capacity), 256);
+        const size_t es = h->elem();
+        void *grown = nullptr;
+        ACF_CUDA(cudaStreamSynchronize(st));
+        ACF_CUDA(cudaMalloc(&grown, (size_t)r.n_rec * cap * es));
+        ACF_CUDA(cudaMemset(grown, 0, (size_t)r.n_rec * cap * es));
+        if (r.rec && r.rec_capacity > 0)
+            ACF_CUDA(cudaMemcpy2D(grown, (size_t)cap * es, r.rec, (size_t)r.rec_capacity * es,
+                                  (size_t)r.rec_capacity * es, (size_t)r.n_rec, cudaMemcpyDeviceToDevice));
+        cudaFree(r.rec);
+        r.rec = grown;
+        r.rec_capacity = cap;
+        h->graph_dirty = true;
+    }
+    rc = h->precision == 8 ? forward_record_impl<double>(h, n_steps, step_offset, st)
+                           : forward_record_impl<float>(h, n_steps, step_offset, st);
+    return rc;
+}
+
+int acf_adjoint_run(acf_solver *h, const double *grad_rec, double *grad_src, double *grad_shell,
+                    double *grad_air, acf_stream stream) {
+    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (!h->adj.fields || h->adj.recorded < 1) return fail(ACF_ERR_STATE, "no recorded forward run");
+    if (h->rooms[0].n_rec > 0 && !grad_rec) return fail(ACF_ERR_ARGUMENT, "null receiver gradient");
+    DeviceGuard guard(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    return h->precision == 8 ? adjoint_impl<double>(h, grad_rec, grad_src, grad_shell, grad_air, st)
+                             : adjoint_impl<float>(h, grad_rec, grad_src, grad_shell, grad_air, st);
+}
+
+int acf_adjoint_download(acf_solver *h, int field, void *dst, acf_stream stream) {
+    if (!h || !dst) return fail(ACF_ERR_ARGUMENT, "null argument");
+    if (!h->adj.fields) return fail(ACF_ERR_STATE, "call acf_adjoint_prepare first");
+    if (field < 0 || field >= h->n_fields()) return fail(ACF_ERR_ARGUMENT, "field %d out of range", field);
+    DeviceGuard guard(h->device);
+    const RoomHost &r = h->rooms[0];
+    int64_t shape[3];
+    field_shape(r, field, shape);
+    const size_t es = h->elem();
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr((char *)h->adj.fields + (size_t)field * r.field * es, (size_t)r.pz * es,
+                                   (size_t)r.pz, (size_t)(r.ny + 1));
+    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)shape[2] * es, (size_t)shape[2], (size_t)shape[1]);
+    p.extent = make_cudaExtent((size_t)shape[2] * es, (size_t)shape[1], (size_t)shape[0]);
+    p.kind = cudaMemcpyDefault;
+    ACF_CUDA(cudaMemcpy3DAsync(&p, (cudaStream_t)stream));
+    ACF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return ACF_OK;
+}
 
 // ---- batches of rooms -------------------------------------------------------------------
 

@@ -33,6 +33,33 @@ def _as_double_pointer(array: np.ndarray):
     return array.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def config_from_block(block):
+    """Fill an ``acf_config`` from a coefficient block; returns it with the arrays it points to."""
+    config = _native.AcfConfig()
+    config.nx, config.ny, config.nz = block.shape
+    config.precision = block.dtype.itemsize
+    config.n_relax = block.n_relax
+    config.vel_coef = block.vel_coef
+    config.pres_coef = block.pres_coef
+    config.src_coef = block.src_coef
+    config.relax_scale = block.relax_scale
+    for r in range(block.n_relax):
+        config.relax_decay[r] = block.relax_decay[r]
+        config.relax_mean[r] = block.relax_mean[r]
+        config.relax_gain[r] = block.relax_gain[r]
+    keep = []
+    if block.wall_shell is not None:
+        for f, shell in enumerate(block.wall_shell):
+            keep.append(shell)
+            config.wall_shell[f] = _as_double_pointer(shell)
+    if block.layer_cell is not None:
+        for a in range(3):
+            keep += [block.layer_cell[a], block.layer_face[a]]
+            config.cell[a] = _as_double_pointer(block.layer_cell[a])
+            config.face[a] = _as_double_pointer(block.layer_face[a])
+    return config, keep
+
+
 def _free_native(handle):
     if handle:
         _native.library().acf_destroy(handle)
@@ -73,9 +100,11 @@ class CudaAcousticFDTD:
 
     def __init__(self, grid, medium=AIR, courant: float = 1.0, dtype=np.float64, walls=None,
                  absorbing_layer=None, air_absorption=None, *, stream: int = 0,
-                 steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH) -> None:
+                 steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
+                 differentiable_walls: bool = False) -> None:
         block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
-                                  air_absorption)
+                                  air_absorption, force_walls=differentiable_walls)
+        self._force_walls = differentiable_walls
         self.grid = grid
         self.medium = medium
         self.courant = courant
@@ -95,28 +124,7 @@ class CudaAcousticFDTD:
         if count.value < 1:
             raise RuntimeError("no CUDA device is visible; the cuda backend has no CPU path")
 
-        config = _native.AcfConfig()
-        config.nx, config.ny, config.nz = block.shape
-        config.precision = self.dtype.itemsize
-        config.n_relax = block.n_relax
-        config.vel_coef = block.vel_coef
-        config.pres_coef = block.pres_coef
-        config.src_coef = block.src_coef
-        config.relax_scale = block.relax_scale
-        for r in range(block.n_relax):
-            config.relax_decay[r] = block.relax_decay[r]
-            config.relax_mean[r] = block.relax_mean[r]
-            config.relax_gain[r] = block.relax_gain[r]
-        keep = []  # arrays that must outlive acf_create
-        if block.wall_shell is not None:
-            for f, shell in enumerate(block.wall_shell):
-                keep.append(shell)
-                config.wall_shell[f] = _as_double_pointer(shell)
-        if block.layer_cell is not None:
-            for a in range(3):
-                keep += [block.layer_cell[a], block.layer_face[a]]
-                config.cell[a] = _as_double_pointer(block.layer_cell[a])
-                config.face[a] = _as_double_pointer(block.layer_face[a])
+        config, keep = config_from_block(block)
         handle = ctypes.c_void_p()
         _native.check(self._lib.acf_create(ctypes.byref(config), ctypes.byref(handle)), "acf_create")
         self._handle = handle
@@ -279,6 +287,11 @@ class CudaAcousticFDTD:
         self._sources.append((self._flat(point), values))
         self._sources_dirty = True
 
+    def clear_sources(self) -> None:
+        """Remove every volume source (receivers and state are kept)."""
+        self._sources = []
+        self._sources_dirty = True
+
     def add_pressure_receiver(self, point) -> int:
         """Record p at ``point`` after every step from now on (``scheme.py:246-255``)."""
         self._receivers.append((self._flat(point), self.step_index))
@@ -394,6 +407,21 @@ class CudaAcousticFDTD:
             kinetic += 0.5 * rho * terms[1 + axis]
             coupling += terms[4 + axis]
         return float(self.grid.dx) ** 3 * (potential + kinetic - 0.5 * self.dt * coupling)
+
+    def set_coefficients(self, walls=None, absorbing_layer=None, air_absorption=None) -> None:
+        """Replace the wall, layer and air coefficients, keeping the grid and the state.
+
+        The new set must have the same relaxation count and the same presence of walls and
+        layer as the one the solver was built with.
+        """
+        block = room_coefficients(self.grid, self.medium, self.courant, self.dtype, walls,
+                                  absorbing_layer, air_absorption, force_walls=self._force_walls)
+        config, keep = config_from_block(block)
+        _native.check(self._lib.acf_set_coefficients(self._handle, ctypes.byref(config)),
+                      "acf_set_coefficients")
+        del keep
+        self.walls, self.absorbing_layer, self.air_absorption = walls, absorbing_layer, air_absorption
+        self.coefficients = block
 
     def set_launch(self, block_threads: int = 256, planes: int = 4) -> None:
         """Launch geometry of the sweeps (threads per block, x planes per block)."""

@@ -141,6 +141,37 @@ int acf_set_launch(acf_solver *solver, int32_t block_threads, int32_t planes);
  * faces; terms[4+a] = sum over interior faces of v_a * (p_hi - p_lo) / dx. Synchronous. */
 int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream stream);
 
+/* ---- Adjoint (single rooms) ----------------------------------------------------------
+ *
+ * Gradients of a loss of the receiver signals, by the transposed leapfrog run backward in
+ * time. No counterpart in the reference (its solvers are not differentiable). The step is
+ * linear in the state, so the backward recursion needs no forward state; parameter gradients
+ * read a forward history: the pressure before the step and before the wall closed form on
+ * every boundary cell (walls), and D and psi of every cell (air), recomputed segment by segment
+ * from full-state checkpoints taken every `checkpoint_every` steps.
+ *
+ * acf_adjoint_prepare  allocates the history for runs of up to max_steps steps.
+ * acf_forward_record   is acf_run that also writes that history (and the checkpoints).
+ * acf_adjoint_run      takes dL/drec (n_receivers rows of n_steps doubles, host) and returns
+ *                      (each optional, host, FP64): dL/dsignal (n_sources rows of n_steps),
+ *                      dL/da per boundary cell (acf_adjoint_shell_size entries, shell order of
+ *                      the wall coefficients with each cell on the first face it touches), and
+ *                      the air sums (dL/dgain_r, dL/dmean_r, dL/ddecay_r for r < n_relax, then
+ *                      dL/drelax_scale).
+ * acf_adjoint_download returns dL/d of the initial state, field by field.
+ * acf_set_coefficients swaps in new coefficients (same grid, precision, relaxation count and
+ *                      the same presence of layer and walls) without touching the state. */
+enum { ACF_GRAD_WALLS = 1, ACF_GRAD_AIR = 2 };
+int acf_set_coefficients(acf_solver *solver, const acf_config *config);
+int acf_adjoint_prepare(acf_solver *solver, int32_t flags, int64_t max_steps,
+                        int32_t checkpoint_every);
+int64_t acf_adjoint_shell_size(const acf_solver *solver);
+int acf_forward_record(acf_solver *solver, int64_t n_steps, int64_t step_offset,
+                       acf_stream stream);
+int acf_adjoint_run(acf_solver *solver, const double *grad_rec, double *grad_src,
+                    double *grad_shell, double *grad_air, acf_stream stream);
+int acf_adjoint_download(acf_solver *solver, int field, void *dst, acf_stream stream);
+
 /* Energy sums without any allocation. No counterpart in the reference.
  *
  * For callers that must not allocate device memory themselves or have the library allocate
