@@ -7,6 +7,8 @@ full-size tests use, from ``numpy.random.default_rng(seed)``:
   1 kHz at cell (16,16,20), receiver at cell (44,40,24), 2000 steps.
 * ``plain_room_large`` -- 384^3, per-wall absorption U(0.05, 0.5), 16-cell sponge on the two x
   faces, ISO air 20 C / 50 % RH (3 relaxation states), Gaussian pulse to 4 kHz, 4 receivers.
+* ``differentiable_room`` -- 128^3, six "true" admittances from absorption U(0.05, 0.5), a
+  start perturbed by up to +-30 % per wall, Gaussian pulse to 2 kHz, four receivers, 3000 steps.
 * ``uneven_rooms`` -- 64 rooms, 3-10 m per axis at dx = 5 cm (60-200 cells per axis; the
   reference's 10 points per wavelength at 2 kHz would give 175-583), per-wall absorption
   U(0.05, 0.5), air at U(15, 25) C and U(30, 70) % RH, one source and two receivers at least
@@ -21,7 +23,8 @@ from .air import AirAbsorption
 from .boundaries import AbsorbingLayer, WallAdmittances, admittance_from_absorption
 from .grid import Grid
 
-__all__ = ["plain_room_small", "plain_room_large", "uneven_rooms", "UNEVEN_DX"]
+__all__ = ["plain_room_small", "plain_room_large", "uneven_rooms", "differentiable_room",
+           "UNEVEN_DX"]
 
 UNEVEN_DX = 0.05
 
@@ -70,3 +73,17 @@ def uneven_rooms(n_rooms: int = 64, seed: int = 3, dx: float = UNEVEN_DX,
         points = [tuple(float(rng.uniform(lo, hi)) for lo, hi in inner) for _ in range(3)]
         out.append((spec, points[0], points[1:]))
     return out
+
+
+def differentiable_room(size: int = 128, seed: int = 4, n_receivers: int = 4):
+    """(grid, true admittances, start admittances, source point, receiver points)."""
+    rng = np.random.default_rng(seed)
+    dx = 343.2 / (10 * 2000.0)
+    grid = Grid(dx=dx, nx=size, ny=size, nz=size)
+    true_xi = np.array([admittance_from_absorption(a) for a in rng.uniform(0.05, 0.5, 6)])
+    start_xi = true_xi * (1.0 + rng.uniform(-0.3, 0.3, 6))
+    margin = max(1, size // 8)
+    cells = [tuple(int(v) for v in rng.integers(margin, size - margin, 3))
+             for _ in range(1 + n_receivers)]
+    points = [tuple((i + 0.5) * dx for i in c) for c in cells]
+    return grid, true_xi, start_xi, points[0], points[1:]

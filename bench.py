@@ -37,28 +37,10 @@ N_RECEIVERS = 4
 
 
 def workload(size: int, seed: int = 2):
-    from ac_fdtd_b200 import (
-        AbsorbingLayer,
-        AirAbsorption,
-        Grid,
-        WallAdmittances,
-        admittance_from_absorption,
-    )
+    from ac_fdtd_b200.workloads import plain_room_large
 
-    rng = np.random.default_rng(seed)
-    dx = 343.2 / (10 * 4000.0)
-    grid = Grid(dx=dx, nx=size, ny=size, nz=size)
-    alphas = rng.uniform(0.05, 0.5, 6)
-    objects = dict(
-        walls=WallAdmittances(*[admittance_from_absorption(a) for a in alphas]),
-        absorbing_layer=AbsorbingLayer(thickness=16, faces=((0, 0), (0, 1))),
-        air_absorption=AirAbsorption(temperature=20.0, relative_humidity=50.0),
-    )
-    margin = max(1, min(24, size // 4))
-    cells = [tuple(int(v) for v in rng.integers(margin, size - margin, 3))
-             for _ in range(1 + N_RECEIVERS)]
-    points = [tuple((i + 0.5) * dx for i in c) for c in cells]
-    return grid, objects, points
+    grid, objects, source, receivers = plain_room_large(size, seed, N_RECEIVERS)
+    return grid, objects, [source, *receivers]
 
 
 def config_dict(args, grid) -> dict:
@@ -233,7 +215,11 @@ def run_ours(args) -> None:
 
     grid, objects, points = workload(args.size)
     solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
-    geometry = apply_tuned(solver)
+    if args.launch:
+        geometry = tuple(int(v) for v in args.launch.split(","))
+        solver.set_launch(*geometry)
+    else:
+        geometry = apply_tuned(solver)
     solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
     for point in points[1:]:
         solver.add_pressure_receiver(point)
@@ -326,6 +312,9 @@ def run_ours(args) -> None:
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = cell_updates / e2e_s / 1e9
 
+    batched = None if args.skip_extras else batched_vs_per_room(args)
+    adjoint = None if args.skip_extras else adjoint_cost(args)
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
@@ -333,7 +322,7 @@ def run_ours(args) -> None:
         "data": "synthetic",
         "config": {**config_dict(args, grid),
                    "launch": {"block_threads": geometry[0], "planes_per_block": geometry[1],
-                              "chosen_by": "ac_fdtd_b200.autotune"}},
+                              "chosen_by": "--launch" if args.launch else "ac_fdtd_b200.autotune"}},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
@@ -341,6 +330,8 @@ def run_ours(args) -> None:
                         "recorded_pressure, get_state (pinned host)"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
+        "batched": batched,
+        "adjoint": adjoint,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -354,6 +345,125 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def _device_ms(fn, torch) -> float:
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    fn()
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def batched_vs_per_room(args) -> dict:
+    """64 uneven rooms (60-200 cells per axis, fp32, walls + ISO air): one RoomBatch against the
+    same rooms run one after another, each as its own CudaAcousticFDTD (CUDA graphs in both)."""
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, RoomBatch, gaussian_pulse
+    from ac_fdtd_b200.workloads import uneven_rooms
+
+    T = args.batch_steps
+    rooms = uneven_rooms()
+    specs = [r[0] for r in rooms]
+    cells = int(sum(spec["grid"].n_cells for spec in specs))
+    batch = RoomBatch(specs, dtype=np.float32)
+    for r, (spec, source, receivers) in enumerate(rooms):
+        batch.add_volume_source(r, source, gaussian_pulse(T, batch.dt(r), 2000.0))
+        for point in receivers:
+            batch.add_pressure_receiver(r, point)
+
+    def run_batch():
+        batch.step_index = 0
+        batch.run(T)
+
+    for _ in range(max(1, args.warmup - 1)):
+        run_batch()
+    batch_ms = min(_device_ms(run_batch, torch) for _ in range(2))
+    launches = batch.launch_count()
+    batch.close()
+
+    solvers = []
+    for spec, source, receivers in rooms:
+        solver = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
+                                  air_absorption=spec["air_absorption"])
+        solver.add_volume_source(source, gaussian_pulse(T, solver.dt, 2000.0))
+        for point in receivers:
+            solver.add_pressure_receiver(point)
+        solvers.append(solver)
+
+    def run_rooms():
+        for solver in solvers:
+            solver.step_index = 0
+            solver.run(T)
+
+    for _ in range(max(1, args.warmup - 1)):
+        run_rooms()
+    per_room_ms = min(_device_ms(run_rooms, torch) for _ in range(2))
+    for solver in solvers:
+        solver.close()
+    peak, _ = measured_peak_hbm()
+    batched_gcups = cells * T / (batch_ms * 1e-3) / 1e9
+    return {
+        "workload": f"64 rooms 3-10 m per axis at dx 5 cm ({cells} cells, 60-200 per axis), fp32, "
+                    f"walls alpha~U(0.05,0.5), ISO air T~U(15,25) C RH~U(30,70) %, 1 source + 2 "
+                    f"receivers per room, {T} steps (CUDA graphs in both arms)",
+        "batched_gcups": batched_gcups,
+        "per_room_gcups": cells * T / (per_room_ms * 1e-3) / 1e9,
+        "speedup": per_room_ms / batch_ms,
+        "batched_hbm_frac_of_measured": batched_gcups * 1e9 * 72 / (peak * 1e9),
+        "launches_in_setup_and_runs": launches,
+    }
+
+
+def adjoint_cost(args) -> dict:
+    """Cost of one gradient against one forward run: 128^3 fp32, 3000 steps, L2 misfit of four
+    receivers to the signals of the true admittances, from a start perturbed by up to 30 %."""
+    import torch
+
+    from ac_fdtd_b200 import AirAbsorption, CudaAcousticFDTD, WallAdmittances, gaussian_pulse
+    from ac_fdtd_b200.adjoint import DifferentiableRoom
+    from ac_fdtd_b200.workloads import differentiable_room
+
+    T = args.adjoint_steps
+    grid, true_xi, start_xi, source, receivers = differentiable_room()
+    out = {"workload": f"differentiable room 128^3 fp32, {T} steps, 4 receivers, gradient wrt 6 "
+                       f"wall admittances + {T} source samples"}
+    for label, air in (("walls_and_signal", None),
+                       ("walls_signal_and_air", AirAbsorption(temperature=20.0, relative_humidity=50.0))):
+        wrt = ("signal", "walls") if air is None else ("signal", "walls", "air")
+        forward = CudaAcousticFDTD(grid, dtype=np.float32, walls=WallAdmittances(*start_xi),
+                                   air_absorption=air)
+        room = DifferentiableRoom(grid, dtype=np.float32, walls=WallAdmittances(*true_xi),
+                                  air_absorption=air, max_steps=T, wrt=wrt)
+        signal = gaussian_pulse(T, room.dt, 2000.0)
+        for solver in (forward, room.solver):
+            solver.add_volume_source(source, signal)
+            for point in receivers:
+                solver.add_pressure_receiver(point)
+        target = room.forward(T).astype(np.float64)
+        room.set_parameters(walls=WallAdmittances(*start_xi))
+
+        def run_forward():
+            forward.step_index = 0
+            forward.run(T)
+
+        def gradient():
+            rec = room.forward(T)
+            room.backward(rec.astype(np.float64) - target)
+
+        run_forward()
+        gradient()
+        forward_ms = min(_device_ms(run_forward, torch) for _ in range(3))
+        gradient_ms = min(_device_ms(gradient, torch) for _ in range(3))
+        out[label] = {"forward_ms": forward_ms, "gradient_ms": gradient_ms,
+                      "ratio": gradient_ms / forward_ms,
+                      "checkpoint_every": room.checkpoint_every if air is not None else None}
+        forward.close()
+        room.solver.close()
+    return out
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -364,6 +474,12 @@ def main() -> None:
     parser.add_argument("--time-steps", type=int, default=4000)
     parser.add_argument("--cpu-budget", type=float, default=12.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--skip-extras", action="store_true",
+                        help="skip the batched-room and adjoint-cost measurements")
+    parser.add_argument("--batch-steps", type=int, default=600)
+    parser.add_argument("--launch", default="",
+                        help="fixed sweep geometry 'threads,planes' instead of the autotuner")
+    parser.add_argument("--adjoint-steps", type=int, default=3000)
     args = parser.parse_args()
     if args.impl == "reference":
         run_reference(args)
