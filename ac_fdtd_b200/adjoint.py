@@ -150,11 +150,9 @@ class DifferentiableRoom:
         if not 0 < n_steps <= self.max_steps:
             raise ValueError(f"n_steps must be in 1..{self.max_steps}")
         s = self.solver
-        shape = s.grid.shape if hasattr(s.grid, "shape") else (s.grid.nx, s.grid.ny, s.grid.nz)
-        zeros = np.zeros(shape, dtype=s.dtype)
-        s.set_state(p=zeros if p0 is None else p0,
-                    velocity=[np.zeros(s._field_shape(1 + a), dtype=s.dtype) for a in range(3)],
-                    relaxation=[zeros] * s.n_relax if s.n_relax else None)
+        s.reset_state()
+        if p0 is not None:
+            s.set_state(p=p0)
         s.step_index = 0
         s._flush()
         s._push_points()

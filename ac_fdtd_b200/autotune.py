@@ -15,10 +15,15 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["CANDIDATES", "tune", "apply_tuned"]
+__all__ = ["CANDIDATES", "BATCH_CANDIDATES", "tune", "apply_tuned", "tune_batch",
+           "apply_tuned_batch"]
 
 #: (threads per block, planes per block) tried by default.
 CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
+
+#: (threads per tile, planes per tile, CTAs per SM; 0 = one CTA per tile) for batches.
+BATCH_CANDIDATES = ((256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8, 0), (256, 4, 4),
+                    (128, 4, 8), (256, 2, 0))
 
 _cache: dict[str, tuple[int, int]] = {}
 
@@ -91,4 +96,41 @@ def apply_tuned(solver, candidates=CANDIDATES):
             _cache[key] = winner
             _store_file(key, winner)
     solver.set_launch(*_cache[key])
+    return _cache[key]
+
+
+def tune_batch(batch, candidates=BATCH_CANDIDATES, steps: int = 12, repeats: int = 2):
+    """Time each batch geometry on a scratch twin batch; return (best, {candidate: ms/step})."""
+    from .batch import RoomBatch
+
+    twin = RoomBatch(batch.specs, dtype=batch.dtype, steps_per_graph=0)
+    timings = {}
+    try:
+        for r in range(len(twin)):
+            twin.set_field(r, 0, np.random.default_rng(r).standard_normal(twin.shapes[r]) * 1e-3)
+        for candidate in candidates:
+            try:
+                twin.set_launch(*candidate)
+            except RuntimeError:
+                continue
+            twin.run(2)
+            best = float("inf")
+            for _ in range(repeats):
+                twin.profile(True)
+                twin.run(steps)
+                velocity_ms, pressure_ms, n = twin.profile_read()
+                twin.profile(False)
+                best = min(best, (velocity_ms + pressure_ms) / max(n, 1))
+            timings[candidate] = best
+    finally:
+        twin.close()
+    return min(timings, key=timings.get), timings
+
+
+def apply_tuned_batch(batch, candidates=BATCH_CANDIDATES):
+    key = json.dumps(["batch", [list(s) for s in batch.shapes], batch.dtype.name])
+    if key not in _cache:
+        winner, _ = tune_batch(batch, candidates)
+        _cache[key] = winner
+    batch.set_launch(*_cache[key])
     return _cache[key]

@@ -138,7 +138,8 @@ struct History {
     T *shell;                      // steps x shell_total pairs, or null
     int64_t shell_total, shell_step0, shell_steps;
     int64_t face_off[6];
-    T *fields;                     // slots x (1 + n_relax) fields (padded geometry), or null
+    T *fields;                     // slots x (1 + n_relax) fields (padded geometry), or null;
+                                   // step n uses slot (n - fields_step0) mod fields_slots
     int64_t fields_step0;
     int32_t fields_slots;
     int32_t reserved;
@@ -344,8 +345,9 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
         }
 
         if (REC && hist->fields) {
-            const int64_t slot = step - hist->fields_step0;
-            if (slot >= 0 && slot < hist->fields_slots) {
+            const int64_t rel = step - hist->fields_step0;
+            const int64_t slot = rel % hist->fields_slots;
+            if (rel >= 0) {
                 T *h = hist->fields + slot * (1 + NR) * s.field + base;
                 Vec4<T>::store(h, D);
 #pragma unroll
@@ -549,21 +551,25 @@ struct AdjointParams {
     History<T> hist;
     double *grad_shell;            // FP64 dL/da per boundary cell (shell index)
     double *air_partials;          // per block: G_r (R), m_r (R), delta_r (R), S
-    int64_t step;                  // forward step being reversed
+    const int64_t *step_base;      // the forward step reversed is *step_base + local_step
+    int32_t local_step;
     int32_t planes;
     int32_t air;                   // accumulate air gradients (needs hist.fields)
 };
 
-template <typename T, bool LAYER, bool WALLS, int NR>
-__global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParams<T> a) {
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 2 : 4)))
+    adjoint_pressure_sweep(const AdjointParams<T> a) {
     const Room<T> &s = a.room;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const bool active = c < s.nchunks && j < s.ny;
     constexpr int NA = 3 * NR + 1;
-    double air_acc[NA];
+    // Per-thread sums over this launch's few cells in the working precision; the block sums
+    // and the sums across blocks and steps are FP64.
+    T air_acc[NA];
 #pragma unroll
-    for (int t = 0; t < NA; t++) air_acc[t] = 0.0;
+    for (int t = 0; t < NA; t++) air_acc[t] = T(0);
 
     if (active) {
         const int k0 = c * kVec;
@@ -571,7 +577,7 @@ __global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParam
         const int i_end = min(s.nx, i_begin + a.planes);
         const int64_t column = (int64_t)j * s.pz + k0;
         const bool has_above = k0 + kVec <= s.nz;
-        const int64_t step = a.step;
+        const int64_t step = *a.step_base + a.local_step;
         const T scp = s.relax_scale - s.cp;
         T XL[kVec];
         Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
@@ -587,9 +593,10 @@ __global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParam
 #pragma unroll
             for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
             T HD[kVec], HS[NR > 0 ? NR : 1][kVec];
-            const bool air = NR > 0 && a.air;
+            constexpr bool air = AIR && NR > 0;
             if (air) {
-                const T *h = a.hist.fields + (step - a.hist.fields_step0) * (1 + NR) * s.field + base;
+                const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
+                const T *h = a.hist.fields + slot * (1 + NR) * s.field + base;
                 Vec4<T>::ldg(h, HD);
 #pragma unroll
                 for (int r = 0; r < NR; r++) Vec4<T>::ldg(h + (1 + r) * s.field, HS[r]);
@@ -599,25 +606,43 @@ __global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParam
                 fi = __ldg(s.cell[0] + i);
                 fj = __ldg(s.cell[1] + j);
             }
+            // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}, plus dL/drec[n]
+            T LPn[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                const int k = k0 + e;
+                const T up = e + 1 < kVec ? Z[e + 1] : above;
+                T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
+                dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
+                dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
+                LPn[e] = L[e] + s.cv * dmu;
+            }
+            for (int r = 0; r < s.n_rec; r++) {
+                const int64_t d = s.rec_off[r] - base;
+                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                    const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
+#pragma unroll
+                    for (int e = 0; e < kVec; e++)
+                        if (e == d) LPn[e] = LPn[e] + g;
+                }
+            }
+            for (int q = 0; q < s.n_src; q++) {
+                const int64_t d = s.src_off[q] - base;
+                if (d >= 0 && d < kVec && step < s.src_len[q]) {
+                    T v = LPn[0];
+#pragma unroll
+                    for (int e = 1; e < kVec; e++)
+                        if (e == d) v = LPn[e];
+                    a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
+                }
+            }
             T LD[kVec];
 #pragma unroll
             for (int e = 0; e < kVec; e++) {
                 const int k = k0 + e;
                 LD[e] = T(0);
                 if (k >= s.nz) continue;
-                // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}
-                const T up = e + 1 < kVec ? Z[e + 1] : above;
-                T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
-                dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
-                dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
-                T lp = L[e] + s.cv * dmu;
-                const int64_t cell = base + e;
-                for (int r = 0; r < s.n_rec; r++)
-                    if (s.rec_off[r] == cell && step >= s.rec_start[r])
-                        lp = lp + (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
-                for (int q = 0; q < s.n_src; q++)
-                    if (s.src_off[q] == cell && step < s.src_len[q])
-                        a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * lp);
+                const T lp = LPn[e];
                 T lph = lp;
                 if (LAYER) {
                     lph = lph * fi;
@@ -649,15 +674,14 @@ __global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParam
                     ld = ld + s.gain[r] * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
                     LS[r][e] = s.decay[r] * lpsi + s.mean[r] * lpt;
                     if (air) {
-                        const double d = (double)HD[e];
-                        const double off = (double)HS[r][e] - (double)s.gain[r] * d;
-                        air_acc[r] += d * ((1.0 - (double)s.decay[r]) * (double)lpsi -
-                                           (double)s.mean[r] * (double)lpt);
-                        air_acc[NR + r] += (double)lpt * off;
-                        air_acc[2 * NR + r] += (double)lpsi * off;
+                        const T d = HD[e];
+                        const T off = HS[r][e] - s.gain[r] * d;
+                        air_acc[r] += d * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
+                        air_acc[NR + r] += lpt * off;
+                        air_acc[2 * NR + r] += lpsi * off;
                     }
                 }
-                if (air) air_acc[3 * NR] += (double)HD[e] * (double)lpt;
+                if (air) air_acc[3 * NR] += HD[e] * lpt;
                 L[e] = lpart;
                 LD[e] = ld;
             }
@@ -670,14 +694,14 @@ __global__ void __launch_bounds__(256) adjoint_pressure_sweep(const AdjointParam
         }
     }
 
-    if (NR > 0 && a.air) {  // uniform per launch: every thread reaches the barrier
+    if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
         __shared__ double red[NA][8];
         const int tid = threadIdx.y * blockDim.x + threadIdx.x;
         const int lane = tid & 31, warp = tid >> 5;
         const int n_warps = (blockDim.x * blockDim.y + 31) >> 5;
 #pragma unroll
         for (int t = 0; t < NA; t++) {
-            double v = air_acc[t];
+            double v = (double)air_acc[t];
             for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
             if (lane == 0) red[t][warp] = v;
         }
@@ -1055,6 +1079,18 @@ struct acf_batch {
 
     int64_t launches = 0;
 
+    // CUDA graphs of the adjoint path: forward record, recompute, adjoint steps
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t steps = 0;
+        void release() {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+    };
+    Graph g_record, g_recompute, g_adjoint;
+    bool adj_graphs_dirty = true;
+
     // adjoint (single rooms)
     struct Adjoint {
         int32_t flags = 0;
@@ -1170,7 +1206,10 @@ int build_tiles(acf_batch *b) {
     ACF_CUDA(cudaMalloc(&b->tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
     ACF_CUDA(cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
     b->n_tiles = (int32_t)tiles.size();
-    b->batch_ctas = std::max(1, std::min(b->n_tiles, b->ctas_per_sm * b->sms));
+    // ctas_per_sm == 0: one CTA per tile, scheduled by the hardware; otherwise a persistent
+    // grid of ctas_per_sm CTAs per SM striding over the table.
+    b->batch_ctas = b->ctas_per_sm == 0 ? std::max(1, b->n_tiles)
+                                        : std::max(1, std::min(b->n_tiles, b->ctas_per_sm * b->sms));
     return ACF_OK;
 }
 
@@ -1417,6 +1456,9 @@ void free_batch(acf_batch *b) {
     if (!b) return;
     DeviceGuard guard(b->device);
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->g_record.release();
+    b->g_recompute.release();
+    b->g_adjoint.release();
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     for (auto &e : b->ring)
         if (e) cudaEventDestroy(e);
@@ -1600,7 +1642,7 @@ int set_sources(acf_batch *b, int room, int64_t n, const int64_t *cell, const in
     h.src_off = h.src_len = nullptr;
     h.src_sig = nullptr;
     h.n_src = 0;
-    b->graph_dirty = true;
+    b->graph_dirty = b->adj_graphs_dirty = true;
     b->room_table_dirty = true;
     if (n == 0) return ACF_OK;
     const size_t es = b->elem();
@@ -1657,7 +1699,7 @@ int set_receivers(acf_batch *b, int room, int64_t n, const int64_t *cell, const 
     cudaFree(h.rec_start);
     h.rec_off = h.rec_start = nullptr;
     h.n_rec = 0;
-    b->graph_dirty = true;
+    b->graph_dirty = b->adj_graphs_dirty = true;
     b->room_table_dirty = true;
     h.host_rec_start.assign(start_step, start_step + n);
     if (n == 0) return ACF_OK;
@@ -1713,7 +1755,7 @@ int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream str
         cudaFree(h.rec);
         h.rec = grown;
         h.rec_capacity = cap;
-        b->graph_dirty = true;
+        b->graph_dirty = b->adj_graphs_dirty = true;
         b->room_table_dirty = true;
     }
     return b->precision == 8 ? run_impl<double>(b, n_steps, step_offset, st)
@@ -1725,8 +1767,8 @@ int set_launch(acf_batch *b, int32_t block_threads, int32_t planes, int32_t ctas
     if (block_threads < 32 || block_threads > 256 || (block_threads & (block_threads - 1)))
         return fail(ACF_ERR_ARGUMENT, "block_threads must be a power of two in [32, 256], got %d", block_threads);
     if (planes < 1 || planes > 1024) return fail(ACF_ERR_ARGUMENT, "planes must be in [1, 1024], got %d", planes);
-    if (ctas_per_sm < 1 || ctas_per_sm > 32)
-        return fail(ACF_ERR_ARGUMENT, "ctas_per_sm must be in [1, 32], got %d", ctas_per_sm);
+    if (ctas_per_sm < 0 || ctas_per_sm > 32)
+        return fail(ACF_ERR_ARGUMENT, "ctas_per_sm must be in [0, 32] (0: one CTA per tile), got %d", ctas_per_sm);
     if (b->rooms.size() == 1 && (b->rooms[0].nx + planes - 1) / planes > 65535)
         return fail(ACF_ERR_ARGUMENT, "nx / planes exceeds the 65535 grid limit; use more planes per block");
     DeviceGuard guard(b->device);
@@ -1735,7 +1777,7 @@ int set_launch(acf_batch *b, int32_t block_threads, int32_t planes, int32_t ctas
     b->planes = planes;
     b->ctas_per_sm = ctas_per_sm;
     if (changed) {
-        b->graph_dirty = true;
+        b->graph_dirty = b->adj_graphs_dirty = true;
         if (b->rooms.size() > 1) {
             ACF_CUDA(cudaDeviceSynchronize());
             return build_tiles(b);
@@ -1788,7 +1830,15 @@ struct RecPressure {
 template <typename T, bool L, bool W, int NR>
 struct AdjPressure {
     static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
-        adjoint_pressure_sweep<T, L, W, NR><<<g, b, 0, st>>>(p);
+        adjoint_pressure_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct AdjPressureAir {
+    static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        if (NR > 0) adjoint_pressure_sweep<T, L, W, NR, NR != 0><<<g, b, 0, st>>>(p);
+        else adjoint_pressure_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
     }
 };
 
@@ -1800,12 +1850,45 @@ History<T> make_history(const acf_batch *b) {
     return h;
 }
 
-// Forward steps [step_offset, step_offset + n) on `state` (the room's own fields, or the
-// recompute copy), writing the history described by `hist`. Receivers record only when
-// `receivers` is set, so a recompute leaves the caller's recordings alone.
+// Replay `g` (a capture of `chunk` calls of launch(local) for local = 0..chunk-1 followed by
+// bump(step_base, bump)) `reps` times on `st`, capturing it first if needed.
+template <class F>
+int replay(acf_batch *b, acf_batch::Graph &g, int64_t chunk, int64_t bump, int64_t reps,
+           cudaStream_t st, F launch) {
+    if (reps <= 0) return ACF_OK;
+    if (b->adj_graphs_dirty) {
+        b->g_record.release();
+        b->g_recompute.release();
+        b->g_adjoint.release();
+        b->adj_graphs_dirty = false;
+    }
+    if (!g.exec || g.steps != chunk) {
+        g.release();
+        if (!b->capture_stream)
+            ACF_CUDA(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
+        ACF_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+        for (int64_t t = 0; t < chunk; t++) launch((int32_t)t, b->capture_stream);
+        bump_step_base<<<1, 1, 0, b->capture_stream>>>(b->step_base, bump);
+        cudaGraph_t graph = nullptr;
+        ACF_CUDA(cudaStreamEndCapture(b->capture_stream, &graph));
+        cudaError_t err = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (err != cudaSuccess) return fail(ACF_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(err));
+        g.steps = chunk;
+    }
+    for (int64_t r = 0; r < reps; r++) ACF_CUDA(cudaGraphLaunch(g.exec, st));
+    return ACF_OK;
+}
+
+constexpr int64_t kAdjointChunk = 64;
+
+// Forward steps [s0, s0 + n) on `state` (the room's own fields, or the recompute copy), writing
+// the history in `hist`. Receivers record only when `receivers` is set, so a recompute leaves
+// the caller's recordings alone. With `checkpoints`, the state at every multiple of the
+// checkpoint interval (counted from the recorded run's first step) is copied out first.
 template <typename T>
-void record_steps(acf_batch *b, const void *state, const History<T> &hist, int64_t step_offset,
-                  int64_t n, bool receivers, cudaStream_t st, bool checkpoints) {
+int record_steps(acf_batch *b, acf_batch::Graph &g, const void *state, const History<T> &hist,
+                 int64_t s0, int64_t n, bool receivers, cudaStream_t st, bool checkpoints) {
     const RoomHost &h = b->rooms[0];
     StepParams<T> p{};
     p.room = make_room<T>(b, 0, state);
@@ -1814,33 +1897,52 @@ void record_steps(acf_batch *b, const void *state, const History<T> &hist, int64
     p.step_base = b->step_base;
     p.planes = b->planes;
     const LaunchShape L = single_shape(b);
-    set_step_base<<<1, 1, 0, st>>>(b->step_base, step_offset);
+    auto launch = [&](int32_t local, cudaStream_t s) {
+        StepParams<T> q = p;
+        q.local_step = local;
+        if (h.has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, s>>>(q);
+        else velocity_sweep<T, false><<<L.grid, L.block, 0, s>>>(q);
+        dispatch_pressure<T, RecPressure>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+    };
+    const int64_t G = checkpoints ? b->adj.every : kAdjointChunk;
+    int64_t done = 0;
+    set_step_base<<<1, 1, 0, st>>>(b->step_base, s0);
     b->launches += 1;
-    for (int64_t t = 0; t < n; t++) {
-        const int64_t absolute = step_offset + t;
+    while (done < n) {
+        const int64_t absolute = s0 + done;
         if (checkpoints && (absolute - b->adj.step0) % b->adj.every == 0) {
             const int64_t slot = (absolute - b->adj.step0) / b->adj.every;
-            cudaMemcpyAsync((char *)b->adj.checkpoints + slot * b->room_block_bytes(0), state,
-                            b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st);
+            ACF_CUDA(cudaMemcpyAsync((char *)b->adj.checkpoints + slot * b->room_block_bytes(0), state,
+                                     b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st));
         }
-        p.local_step = (int32_t)t;
-        if (h.has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(p);
-        else velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(p);
-        dispatch_pressure<T, RecPressure>(h.has_layer, h.has_walls, h.n_relax, p, L.grid, L.block, st);
-        b->launches += 2;
+        if (n - done >= G) {
+            int rc = replay(b, g, G, G, 1, st, launch);
+            if (rc) return rc;
+            b->launches += 2 * G + 1;
+            done += G;
+        } else {
+            // the tail: launch step by step from the counter, then advance it past them
+            for (int64_t t = 0; done + t < n; t++) launch((int32_t)t, st);
+            bump_step_base<<<1, 1, 0, st>>>(b->step_base, n - done);
+            b->launches += 2 * (n - done) + 1;
+            done = n;
+        }
     }
+    return ACF_OK;
 }
 
 template <typename T>
 int forward_record_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
+    if (b->adj.step0 != step_offset) b->adj_graphs_dirty = true;
     b->adj.recorded = n_steps;
     b->adj.step0 = step_offset;
     History<T> hist = make_history<T>(b);
     hist.shell = (T *)b->adj.hist_shell;
     hist.shell_step0 = step_offset;
-    hist.shell_steps = b->adj.hist_shell ? n_steps : 0;
-    record_steps<T>(b, b->field_ptr(0, ACF_FIELD_P), hist, step_offset, n_steps, true, st,
-                    (b->adj.flags & ACF_GRAD_AIR) != 0);
+    hist.shell_steps = b->adj.hist_shell ? b->adj.capacity : 0;
+    int rc = record_steps<T>(b, b->g_record, b->field_ptr(0, ACF_FIELD_P), hist, step_offset, n_steps,
+                             true, st, (b->adj.flags & ACF_GRAD_AIR) != 0);
+    if (rc) return rc;
     ACF_CUDA(cudaGetLastError());
     return ACF_OK;
 }
@@ -1859,20 +1961,28 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     if (grad_air && !air)
         return fail(ACF_ERR_STATE, "air gradients need relaxation states and ACF_GRAD_AIR");
 
-    // Device inputs and zeroed accumulators.
-    if (h.n_rec > 0) {
+    // Device inputs and zeroed accumulators, sized for the prepared capacity so the captured
+    // graphs stay valid from call to call.
+    const int64_t cap = A.capacity;
+    if (h.n_rec > A.grad_rows_rec || !A.grad_rec) {
         cudaFree(A.grad_rec);
         A.grad_rec = nullptr;
-        ACF_CUDA(cudaMalloc(&A.grad_rec, (size_t)h.n_rec * n * sizeof(double)));
-        ACF_CUDA(cudaMemcpyAsync(A.grad_rec, grad_rec, (size_t)h.n_rec * n * sizeof(double),
-                                 cudaMemcpyHostToDevice, st));
+        A.grad_rows_rec = std::max<int64_t>(1, h.n_rec);
+        ACF_CUDA(cudaMalloc(&A.grad_rec, (size_t)A.grad_rows_rec * cap * sizeof(double)));
+        b->adj_graphs_dirty = true;
     }
-    cudaFree(A.grad_src);
-    A.grad_src = nullptr;
-    if (h.n_src > 0) {
-        ACF_CUDA(cudaMalloc(&A.grad_src, (size_t)h.n_src * n * sizeof(double)));
-        ACF_CUDA(cudaMemsetAsync(A.grad_src, 0, (size_t)h.n_src * n * sizeof(double), st));
+    if (h.n_src > A.grad_rows_src || !A.grad_src) {
+        cudaFree(A.grad_src);
+        A.grad_src = nullptr;
+        A.grad_rows_src = std::max<int64_t>(1, h.n_src);
+        ACF_CUDA(cudaMalloc(&A.grad_src, (size_t)A.grad_rows_src * cap * sizeof(double)));
+        b->adj_graphs_dirty = true;
     }
+    if (h.n_rec > 0)
+        ACF_CUDA(cudaMemcpy2DAsync(A.grad_rec, cap * sizeof(double), grad_rec, n * sizeof(double),
+                                   n * sizeof(double), (size_t)h.n_rec, cudaMemcpyHostToDevice, st));
+    if (h.n_src > 0)
+        ACF_CUDA(cudaMemsetAsync(A.grad_src, 0, (size_t)h.n_src * cap * sizeof(double), st));
     const size_t adj_bytes = ((size_t)(5 + h.n_relax) * h.field + h.pz) * es;
     ACF_CUDA(cudaMemsetAsync(A.fields, 0, adj_bytes, st));
     if (A.grad_shell) ACF_CUDA(cudaMemsetAsync(A.grad_shell, 0, A.shell_total * sizeof(double), st));
@@ -1885,6 +1995,7 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
             A.air_partials = nullptr;
             ACF_CUDA(cudaMalloc(&A.air_partials, (size_t)blocks * NA * sizeof(double)));
             A.air_blocks = blocks;
+            b->adj_graphs_dirty = true;
         }
         ACF_CUDA(cudaMemsetAsync(A.air_partials, 0, (size_t)blocks * NA * sizeof(double), st));
     }
@@ -1900,17 +2011,50 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     a.ld = f + (4 + h.n_relax) * h.field;
     a.grad_rec = A.grad_rec;
     a.grad_src = A.grad_src;
-    a.grad_stride = n;
+    a.grad_stride = cap;
     a.grad_step0 = A.step0;
     a.hist = make_history<T>(b);
     a.hist.shell = (T *)A.hist_shell;
     a.hist.shell_step0 = A.step0;
-    a.hist.shell_steps = n;
+    a.hist.shell_steps = A.capacity;
     a.hist.fields = (T *)A.segment;
+    a.hist.fields_step0 = A.step0;
+    a.hist.fields_slots = (int32_t)std::max(1, A.every);
     a.grad_shell = walls ? A.grad_shell : nullptr;
     a.air_partials = A.air_partials;
+    a.step_base = b->step_base;
     a.planes = b->planes;
     a.air = air ? 1 : 0;
+
+    // One adjoint step per call: reverse forward step *step_base + local.
+    auto adjoint_step = [&](int32_t local, cudaStream_t s) {
+        AdjointParams<T> q = a;
+        q.local_step = local;
+        if (air) dispatch_pressure<T, AdjPressureAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        else dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        if (h.has_layer) adjoint_velocity_sweep<T, true><<<L.grid, L.block, 0, s>>>(q);
+        else adjoint_velocity_sweep<T, false><<<L.grid, L.block, 0, s>>>(q);
+    };
+    // Steps [e - G, e) in reverse: graph locals are captured in launch order t = 0..G-1 and
+    // reverse step base + (G - 1 - t).
+    auto reverse_range = [&](int64_t s0, int64_t e) -> int {
+        int64_t end = e;
+        while (end > s0) {
+            const int64_t G = std::min<int64_t>(air ? A.every : kAdjointChunk, end - s0);
+            set_step_base<<<1, 1, 0, st>>>(b->step_base, end - G);
+            if (G == (air ? A.every : kAdjointChunk)) {
+                int rc = replay(b, b->g_adjoint, G, 0, 1, st,
+                                [&](int32_t t, cudaStream_t s) { adjoint_step((int32_t)(G - 1 - t), s); });
+                if (rc) return rc;
+                b->launches += 2 * G + 2;
+            } else {
+                for (int64_t t = 0; t < G; t++) adjoint_step((int32_t)(G - 1 - t), st);
+                b->launches += 2 * G + 1;
+            }
+            end -= G;
+        }
+        return ACF_OK;
+    };
 
     const int64_t K = air ? A.every : n;
     const int64_t n_seg = (n + K - 1) / K;
@@ -1923,27 +2067,22 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
                                      b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st));
             History<T> hist = make_history<T>(b);
             hist.fields = (T *)A.segment;
-            hist.fields_step0 = s0;
+            hist.fields_step0 = A.step0;
             hist.fields_slots = (int32_t)K;
-            record_steps<T>(b, A.scratch, hist, s0, s1 - s0, false, st, false);
-            a.hist.fields_step0 = s0;
-            a.hist.fields_slots = (int32_t)K;
+            int rc = record_steps<T>(b, b->g_recompute, A.scratch, hist, s0, s1 - s0, false, st, false);
+            if (rc) return rc;
         }
-        for (int64_t step = s1 - 1; step >= s0; step--) {
-            a.step = step;
-            dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, a, L.grid, L.block, st);
-            if (h.has_layer) adjoint_velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(a);
-            else adjoint_velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(a);
-            b->launches += 2;
-        }
+        int rc = reverse_range(s0, s1);
+        if (rc) return rc;
     }
+    a.local_step = 0;
     adjoint_finish<T><<<L.grid, L.block, 0, st>>>(a);
     b->launches += 1;
     ACF_CUDA(cudaGetLastError());
 
     if (grad_src && h.n_src > 0)
-        ACF_CUDA(cudaMemcpyAsync(grad_src, A.grad_src, (size_t)h.n_src * n * sizeof(double),
-                                 cudaMemcpyDeviceToHost, st));
+        ACF_CUDA(cudaMemcpy2DAsync(grad_src, n * sizeof(double), A.grad_src, cap * sizeof(double),
+                                   n * sizeof(double), (size_t)h.n_src, cudaMemcpyDeviceToHost, st));
     if (grad_shell)
         ACF_CUDA(cudaMemcpyAsync(grad_shell, A.grad_shell, A.shell_total * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
@@ -1971,6 +2110,7 @@ int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t ever
     DeviceGuard guard(b->device);
     ACF_CUDA(cudaDeviceSynchronize());
     auto &A = b->adj;
+    b->adj_graphs_dirty = true;
     void **buffers[] = {&A.hist_shell, &A.checkpoints, &A.scratch, &A.segment, &A.fields};
     for (void **p : buffers) {
         cudaFree(*p);
@@ -2061,7 +2201,7 @@ int set_coefficients(acf_batch *b, int room, const acf_config *c) {
         else cast_copy<double>(cast.data(), host.data(), host.size());
         ACF_CUDA(cudaMemcpy(h.shell, cast.data(), cast.size(), cudaMemcpyHostToDevice));
     }
-    b->graph_dirty = true;
+    b->graph_dirty = b->adj_graphs_dirty = true;
     b->room_table_dirty = true;
     return ACF_OK;
 }
@@ -2177,6 +2317,13 @@ int acf_set_coefficients(acf_solver *h, const acf_config *config) {
     return set_coefficients(h, 0, config);
 }
 
+int acf_reset_state(acf_solver *h, acf_stream stream) {
+    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
+    DeviceGuard guard(h->device);
+    ACF_CUDA(cudaMemsetAsync(h->field_ptr(0, ACF_FIELD_P), 0, h->room_block_bytes(0), (cudaStream_t)stream));
+    return ACF_OK;
+}
+
 int acf_adjoint_prepare(acf_solver *h, int32_t flags, int64_t max_steps, int32_t checkpoint_every) {
     return adjoint_prepare(h, flags, max_steps, checkpoint_every);
 }
@@ -2211,7 +2358,7 @@ int acf_forward_record(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_
         cudaFree(r.rec);
         r.rec = grown;
         r.rec_capacity = cap;
-        h->graph_dirty = true;
+        h->graph_dirty = h->adj_graphs_dirty = true;
     }
     rc = h->precision == 8 ? forward_record_impl<double>(h, n_steps, step_offset, st)
                            : forward_record_impl<float>(h, n_steps, step_offset, st);
@@ -2312,7 +2459,7 @@ int acf_batch_run(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream
 int acf_batch_set_graph(acf_batch *b, int32_t steps) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
     if (steps < 0 || steps > 4096) return fail(ACF_ERR_ARGUMENT, "steps_per_graph %d out of range", steps);
-    if (steps != b->graph_steps) b->graph_dirty = true;
+    if (steps != b->graph_steps) b->graph_dirty = b->adj_graphs_dirty = true;
     b->graph_steps = steps;
     return ACF_OK;
 }

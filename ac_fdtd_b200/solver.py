@@ -255,6 +255,12 @@ class CudaAcousticFDTD:
         self.synchronize()
         return total
 
+    def reset_state(self) -> None:
+        """Put the room at rest: p, v and the relaxation states to zero, on the device."""
+        self._flush()
+        _native.check(self._lib.acf_reset_state(self._handle, self._stream), "acf_reset_state")
+        self._mirror_current.clear()
+
     def get_state(self, p=None, velocity=None) -> int:
         """Download p and/or the velocities into caller arrays; returns bytes copied."""
         self._flush()

@@ -367,7 +367,10 @@ def batched_vs_per_room(args) -> dict:
     rooms = uneven_rooms()
     specs = [r[0] for r in rooms]
     cells = int(sum(spec["grid"].n_cells for spec in specs))
+    from ac_fdtd_b200.autotune import apply_tuned_batch
+
     batch = RoomBatch(specs, dtype=np.float32)
+    batch_geometry = apply_tuned_batch(batch)
     for r, (spec, source, receivers) in enumerate(rooms):
         batch.add_volume_source(r, source, gaussian_pulse(T, batch.dt(r), 2000.0))
         for point in receivers:
@@ -413,6 +416,8 @@ def batched_vs_per_room(args) -> dict:
         "speedup": per_room_ms / batch_ms,
         "batched_hbm_frac_of_measured": batched_gcups * 1e9 * 72 / (peak * 1e9),
         "launches_in_setup_and_runs": launches,
+        "batch_launch": {"block_threads": batch_geometry[0], "planes": batch_geometry[1],
+                         "ctas_per_sm": batch_geometry[2], "chosen_by": "ac_fdtd_b200.autotune"},
     }
 
 

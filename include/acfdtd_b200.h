@@ -162,6 +162,8 @@ int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream 
  * acf_set_coefficients swaps in new coefficients (same grid, precision, relaxation count and
  *                      the same presence of layer and walls) without touching the state. */
 enum { ACF_GRAD_WALLS = 1, ACF_GRAD_AIR = 2 };
+/* Set every field of the state to zero on the device (a room at rest). Asynchronous. */
+int acf_reset_state(acf_solver *solver, acf_stream stream);
 int acf_set_coefficients(acf_solver *solver, const acf_config *config);
 int acf_adjoint_prepare(acf_solver *solver, int32_t flags, int64_t max_steps,
                         int32_t checkpoint_every);
@@ -232,8 +234,8 @@ int acf_batch_upload(acf_batch *batch, int32_t room, int field, const void *src,
 int acf_batch_download(acf_batch *batch, int32_t room, int field, void *dst, acf_stream stream);
 int acf_batch_run(acf_batch *batch, int64_t n_steps, int64_t step_offset, acf_stream stream);
 int acf_batch_set_graph(acf_batch *batch, int32_t steps_per_graph);
-/* Threads per tile (power of two, 32..256), x planes per tile, resident CTAs per SM of the
- * persistent grid. */
+/* Threads per tile (power of two, 32..256), x planes per tile, and CTAs per SM of a persistent
+ * grid striding over the tile table (0: one CTA per tile, scheduled by the hardware). */
 int acf_batch_set_launch(acf_batch *batch, int32_t block_threads, int32_t planes,
                          int32_t ctas_per_sm);
 int acf_batch_energy_terms(acf_batch *batch, int32_t room, double dx, double terms[7],
