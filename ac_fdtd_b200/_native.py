@@ -33,8 +33,10 @@ EXPORTED_SYMBOLS = (
     "acf_batch_energy_terms", "acf_batch_profile_enable", "acf_batch_profile_read",
     "acf_batch_launch_count", "acf_set_coefficients", "acf_adjoint_prepare",
     "acf_adjoint_shell_size", "acf_forward_record", "acf_adjoint_run", "acf_adjoint_download",
-    "acf_reset_state",
+    "acf_reset_state", "acf_set_scheme", "acf_get_scheme",
 )
+
+SCHEME_TWO_SWEEPS, SCHEME_FUSED = 0, 1
 
 GRAD_WALLS, GRAD_AIR = 1, 2
 
@@ -121,6 +123,8 @@ _SIGNATURES = {
     "acf_adjoint_run": (ctypes.c_int, [_P, _DP, _DP, _DP, _DP, _P]),
     "acf_adjoint_download": (ctypes.c_int, [_P, ctypes.c_int, _P, _P]),
     "acf_reset_state": (ctypes.c_int, [_P, _P]),
+    "acf_set_scheme": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_get_scheme": (ctypes.c_int, [_P]),
 }
 
 

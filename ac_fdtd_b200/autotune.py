@@ -28,6 +28,10 @@ BATCH_CANDIDATES = ((256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8, 0), (256, 4,
 _cache: dict[str, tuple[int, int]] = {}
 
 
+#: Schemes raced by default; both give bit-identical results.
+SCHEMES = ("fused", "two_sweeps")
+
+
 def _key(solver) -> str:
     nx, ny, nz = solver._shape
     block = solver.coefficients
@@ -54,8 +58,9 @@ def _store_file(key: str, value) -> None:
     Path(path).write_text(json.dumps(data, indent=1))
 
 
-def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2):
-    """Time each candidate on a scratch twin of ``solver``; return (best, {candidate: ms/step})."""
+def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schemes=SCHEMES):
+    """Time each (scheme, threads, planes) on a scratch twin of ``solver``; return
+    (best, {candidate: ms/step})."""
     from .solver import CudaAcousticFDTD
 
     twin = CudaAcousticFDTD(solver.grid, solver.medium, solver.courant, solver.dtype,
@@ -64,9 +69,10 @@ def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2):
     twin.p[:] = np.random.default_rng(0).standard_normal(twin.p.shape) * 1e-3
     timings = {}
     try:
-        for candidate in candidates:
+        for candidate in [(sc, *geo) for sc in schemes for geo in candidates]:
             try:
-                twin.set_launch(*candidate)
+                twin.set_scheme(candidate[0])
+                twin.set_launch(*candidate[1:])
             except RuntimeError:
                 continue
             twin.run(2)
@@ -84,18 +90,21 @@ def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2):
     return winner, timings
 
 
-def apply_tuned(solver, candidates=CANDIDATES):
-    """Set the fastest geometry for this configuration (tuning once per shape class)."""
+def apply_tuned(solver, candidates=CANDIDATES, schemes=SCHEMES):
+    """Set the fastest scheme and geometry for this configuration (tuned once per shape
+    class); returns (scheme, threads, planes)."""
     key = _key(solver)
     if key not in _cache:
         stored = _load_file().get(key)
         if stored:
             _cache[key] = tuple(stored)
         else:
-            winner, _ = tune(solver, candidates)
+            winner, _ = tune(solver, candidates, schemes=schemes)
             _cache[key] = winner
             _store_file(key, winner)
-    solver.set_launch(*_cache[key])
+    scheme, threads, planes = _cache[key]
+    solver.set_scheme(scheme)
+    solver.set_launch(threads, planes)
     return _cache[key]
 
 

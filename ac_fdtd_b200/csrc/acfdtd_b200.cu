@@ -430,6 +430,213 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
 }
 
 // ------------------------------------------------------------------------------------------
+// (a)+(b) in one sweep. The step reads the current p and v and writes the next ones to a second
+// buffer, so a cell can compute the updated velocities of all six of its faces -- its own lower
+// faces, which it stores, and its upper faces, which their owners compute identically -- and
+// then its pressure. Per cell and step this moves (8 + 2R) elements instead of (12 + 2R); every
+// value is produced by the same operations as in the two sweeps, so the results are identical.
+
+template <typename T>
+struct FusedParams {
+    Room<T> room;                  // p, vx, vy, vz: current state (read); psi updated in place
+    T *np, *nvx, *nvy, *nvz;       // next state (written), same geometry
+    const int64_t *step_base;
+    int32_t local_step;
+    int32_t planes;
+};
+
+template <typename T, bool LAYER>
+__device__ __forceinline__ T damp3(T v, T fa, T fb, T fc) {
+    if (LAYER) {
+        v = v * fa;
+        v = v * fb;
+        v = v * fc;
+    }
+    return v;
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begin, int i_end, int j,
+                                             int c, int64_t step) {
+    const Room<T> &s = f.room;
+    const int k0 = c * kVec;
+    const T cv = s.cv, cp = s.cp;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool has_above = k0 + kVec < s.nz;   // p and vz at k0 + 4 are interior
+
+    // Layer profiles are read where used (L1-resident): holding the z profiles of the chunk
+    // across the march would cost registers the load phase needs.
+    T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
+    if (LAYER) {
+        fj_cell = __ldg(s.cell[1] + j);
+        fj_face = __ldg(s.face[1] + j);
+        fj1_face = __ldg(s.face[1] + j + 1);
+    }
+
+    // Carried from plane to plane: p(i) and the updated vx on face i.
+    T P[kVec], XL[kVec];
+    {
+        const int64_t base = (int64_t)i_begin * s.plane + column;
+        Vec4<T>::ldg(s.p + base, P);
+        T V[kVec], Q[kVec];
+        Vec4<T>::ldg(s.vx + base, V);
+        if (i_begin > 0) Vec4<T>::ldg(s.p + base - s.plane, Q);
+        const T fi_face = LAYER ? __ldg(s.face[0] + i_begin) : T(1);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            T v = V[e];
+            if (i_begin > 0) v = v - cv * (P[e] - Q[e]);
+            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell,
+                                    LAYER ? __ldg(s.cell[2] + min(k0 + e, s.nz - 1)) : T(1));
+        }
+    }
+
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        const bool x_inner = i + 1 < s.nx;
+        // ---- loads (all read-only: the next state goes to the other buffer)
+        T PX[kVec], VXo[kVec], PYm[kVec], PYp[kVec], VY[kVec], VYp[kVec], VZ[kVec], S[NR > 0 ? NR : 1][kVec];
+        if (x_inner) Vec4<T>::ldg(s.p + base + s.plane, PX);
+        Vec4<T>::ldg(s.vx + base + s.plane, VXo);
+        if (j > 0) Vec4<T>::ldg(s.p + base - s.pz, PYm);
+        if (j + 1 < s.ny) Vec4<T>::ldg(s.p + base + s.pz, PYp);
+        Vec4<T>::ldg(s.vy + base, VY);
+        Vec4<T>::ldg(s.vy + base + s.pz, VYp);
+        Vec4<T>::ldg(s.vz + base, VZ);
+        const T p_below = k0 > 0 ? __ldg(s.p + base - 1) : T(0);
+        const T p_above = has_above ? __ldg(s.p + base + kVec) : T(0);
+        const T vz_above = k0 + kVec <= s.nz ? __ldg(s.vz + base + kVec) : T(0);
+#pragma unroll
+        for (int r = 0; r < NR; r++) Vec4<T>::load(s.psi + r * s.field + base, S[r]);
+        T fi_cell = T(1), fi1_face = T(1);
+        if (LAYER) {
+            fi_cell = __ldg(s.cell[0] + i);
+            fi1_face = __ldg(s.face[0] + i + 1);
+        }
+
+        // ---- updated faces: x upper (carried on), y lower and upper, z lower and upper
+        T XH[kVec], YL[kVec], YH[kVec], ZL[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const T fkc = LAYER ? __ldg(s.cell[2] + min(k0 + e, s.nz - 1)) : T(1);
+            T v = VXo[e];
+            if (x_inner) v = v - cv * (PX[e] - P[e]);
+            XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc);
+            v = VY[e];
+            if (j > 0) v = v - cv * (P[e] - PYm[e]);
+            YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc);
+            v = VYp[e];
+            if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
+            YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc);
+            const int k = k0 + e;
+            v = VZ[e];
+            if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
+            ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell,
+                                    LAYER ? __ldg(s.face[2] + min(k0 + e, s.nz)) : T(1));
+        }
+        // z face k0 + 4: the next chunk's first lower face, or the top face z = nz.
+        T ZH3 = vz_above;
+        if (has_above) ZH3 = ZH3 - cv * (p_above - P[kVec - 1]);
+        ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell,
+                              LAYER ? __ldg(s.face[2] + min(k0 + kVec, s.nz)) : T(1));
+
+        // ---- pressure, as the pressure sweep computes it
+        T Pn[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            T pe = P[e];
+            if (k < s.nz) {
+                const T zh = e + 1 < kVec ? ZL[e + 1] : ZH3;
+                T d = XH[e] - XL[e];
+                d = d + (YH[e] - YL[e]);
+                d = d + (zh - ZL[e]);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const T target = d * s.gain[r];
+                    const T offset = S[r][e] - target;
+                    S[r][e] = offset * s.decay[r] + target;
+                    pe = pe + offset * s.mean[r];
+                }
+                if (NR > 0) pe = pe + d * s.relax_scale;
+                pe = pe - d * cp;
+                if (WALLS) {
+                    T fu, fp;
+                    if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
+                }
+                if (LAYER) {
+                    pe = pe * fi_cell;
+                    pe = pe * fj_cell;
+                    pe = pe * __ldg(s.cell[2] + k);
+                }
+            }
+            Pn[e] = pe;
+        }
+        if (any_point) {
+            for (int q = 0; q < s.n_src; q++) {
+                const int64_t d = s.src_off[q] - base;
+                if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
+#pragma unroll
+                    for (int e = 0; e < kVec; e++)
+                        if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+                }
+            }
+        }
+
+        // ---- stores: p, the three lower faces, the far boundary faces, psi in place. A z
+        // element k == nz inside this chunk is the top face, already updated in ZL (no
+        // gradient, damped by face profile nz); elements past it are padding.
+        T ZS[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) ZS[e] = k0 + e <= s.nz ? ZL[e] : VZ[e];
+        Vec4<T>::store(f.np + base, Pn);
+        Vec4<T>::store(f.nvx + base, XL);
+        Vec4<T>::store(f.nvy + base, YL);
+        Vec4<T>::store(f.nvz + base, ZS);
+        if (i == s.nx - 1) Vec4<T>::store(f.nvx + base + s.plane, XH);
+        if (j == s.ny - 1) Vec4<T>::store(f.nvy + base + s.pz, YH);
+        if (k0 + kVec == s.nz) f.nvz[base + kVec] = ZH3;
+#pragma unroll
+        for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, S[r]);
+
+        if (any_point) {
+            for (int r = 0; r < s.n_rec; r++) {
+                const int64_t d = s.rec_off[r] - base;
+                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                    T v = Pn[0];
+#pragma unroll
+                    for (int e = 1; e < kVec; e++)
+                        if (e == d) v = Pn[e];
+                    s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            XL[e] = XH[e];
+            P[e] = PX[e];
+        }
+    }
+}
+
+// Resident blocks of 256 threads the compiler must fit (register budget 65536 / (256 x this)).
+#ifndef ACF_FUSED_MIN_BLOCKS
+#define ACF_FUSED_MIN_BLOCKS(T, LAYER, NR) (sizeof(T) == 8 ? 2 : (LAYER || NR >= 4 ? 3 : 4))
+#endif
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(T, LAYER, NR)) fused_sweep(const FusedParams<T> f) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= f.room.nchunks || j >= f.room.ny) return;
+    const bool any_point = (f.room.n_src | f.room.n_rec) != 0;
+    const int64_t step = any_point ? (*f.step_base + f.local_step) : 0;
+    const int i_begin = blockIdx.z * f.planes;
+    fused_column<T, LAYER, WALLS, NR>(f, i_begin, min(f.room.nx, i_begin + f.planes), j, c, step);
+}
+
+// ------------------------------------------------------------------------------------------
 // One room: 2D grid of (chunk, row) threads; blockIdx.z selects a group of `planes` x planes.
 
 template <typename T, bool LAYER>
@@ -1014,6 +1221,8 @@ struct RoomHost {
     double decay[ACF_MAX_RELAXATION] = {}, mean[ACF_MAX_RELAXATION] = {},
            gain[ACF_MAX_RELAXATION] = {};
     size_t state_off = 0;            // byte offset of the room's fields in the state arena
+    void *second = nullptr;          // p, vx, vy, vz of the fused scheme's other buffer
+    int cur = 0;                     // 1 when the current p and v are in `second`
     void *profiles = nullptr;        // cell[3] then face[3], solver precision
     int64_t profile_off[6] = {};
     void *shell = nullptr;           // 6 faces of wall pairs, solver precision
@@ -1064,9 +1273,9 @@ struct acf_batch {
     int planes = 4;
     int ctas_per_sm = 4;
 
-    // graphs
+    // graphs (index: parity of the fused scheme's current buffer at the start of a replay)
     int32_t graph_steps = 0;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr, graph_odd = nullptr;
     cudaStream_t capture_stream = nullptr;
     bool graph_dirty = true;
 
@@ -1114,8 +1323,17 @@ struct acf_batch {
     size_t elem() const { return (size_t)precision; }
     int n_fields() const { return 4 + n_relax; }
     size_t room_block_bytes(int r) const { return (size_t)n_fields() * rooms[r].field * elem(); }
+    int scheme = ACF_SCHEME_TWO_SWEEPS;
     char *field_ptr(int r, int f) const {
-        return (char *)state + rooms[r].state_off + (size_t)f * rooms[r].field * elem();
+        const RoomHost &h = rooms[r];
+        if (h.cur && f < 4) return (char *)h.second + (size_t)f * h.field * elem();
+        return (char *)state + h.state_off + (size_t)f * h.field * elem();
+    }
+    // p, vx, vy, vz of the buffer that is not current (the fused step's destination)
+    char *other_ptr(int r, int f) const {
+        const RoomHost &h = rooms[r];
+        if (h.cur) return (char *)state + h.state_off + (size_t)f * h.field * elem();
+        return (char *)h.second + (size_t)f * h.field * elem();
     }
 };
 
@@ -1137,12 +1355,20 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     s.pz = h.pz;
     s.plane = h.plane;
     s.field = h.field;
-    T *fields = state ? (T *)state : (T *)b->field_ptr(r, ACF_FIELD_P);
-    s.p = fields;
-    s.vx = fields + h.field;
-    s.vy = fields + 2 * h.field;
-    s.vz = fields + 3 * h.field;
-    s.psi = fields + 4 * h.field;
+    if (state) {
+        T *fields = (T *)state;
+        s.p = fields;
+        s.vx = fields + h.field;
+        s.vy = fields + 2 * h.field;
+        s.vz = fields + 3 * h.field;
+        s.psi = fields + 4 * h.field;
+    } else {
+        s.p = (T *)b->field_ptr(r, ACF_FIELD_P);
+        s.vx = (T *)b->field_ptr(r, ACF_FIELD_VX);
+        s.vy = (T *)b->field_ptr(r, ACF_FIELD_VY);
+        s.vz = (T *)b->field_ptr(r, ACF_FIELD_VZ);
+        s.psi = (T *)b->field_ptr(r, ACF_FIELD_PSI0);
+    }
     s.cv = (T)h.coef[0];
     s.cp = (T)h.coef[1];
     s.cs = (T)h.coef[2];
@@ -1263,9 +1489,38 @@ struct BatchPressure {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct FusedStep {
+    static void launch(const FusedParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        fused_sweep<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+// Launch one step; the fused scheme flips the room's current buffer, as the kernel will have
+// done by the time anything queued after it runs.
 template <typename T>
-void launch_step(const acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
+void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
     if (events) cudaEventRecord(events[0], st);
+    if (b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED) {
+        RoomHost &h = b->rooms[0];
+        FusedParams<T> f{};
+        f.room = make_room<T>(b, 0);
+        f.np = (T *)b->other_ptr(0, ACF_FIELD_P);
+        f.nvx = (T *)b->other_ptr(0, ACF_FIELD_VX);
+        f.nvy = (T *)b->other_ptr(0, ACF_FIELD_VY);
+        f.nvz = (T *)b->other_ptr(0, ACF_FIELD_VZ);
+        f.step_base = b->step_base;
+        f.local_step = local;
+        f.planes = b->planes;
+        const LaunchShape L = single_shape(b);
+        dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
+        h.cur ^= 1;
+        if (events) {
+            cudaEventRecord(events[1], st);
+            cudaEventRecord(events[2], st);
+        }
+        return;
+    }
     if (b->rooms.size() == 1) {
         const RoomHost &h = b->rooms[0];
         StepParams<T> p{};
@@ -1327,7 +1582,7 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
             }
             launch_step<T>(b, 0, st, b->ring + 3 * slot);
             bump_step_base<<<1, 1, 0, st>>>(b->step_base, 1);
-            b->launches += 3;
+            b->launches += (b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED) ? 2 : 3;
         }
         for (int64_t t = std::max<int64_t>(0, n_steps - R); t < n_steps; t++) {
             int rc = drain(t % R);
@@ -1338,13 +1593,20 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
     }
 
     int64_t done = 0;
-    const int64_t G = b->graph_steps;
+    const bool fused = b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED;
+    // A fused graph holds an even number of steps, so a replay leaves the buffers as it found
+    // them; one graph is kept per starting buffer.
+    const int64_t G = fused ? (b->graph_steps + 1) / 2 * 2 : b->graph_steps;
+    const int kernels_per_step = fused ? 1 : 2;
     if (G > 0 && n_steps >= G) {
-        if (b->graph_dirty || !b->graph) {
-            if (b->graph) {
-                cudaGraphExecDestroy(b->graph);
-                b->graph = nullptr;
-            }
+        if (b->graph_dirty) {
+            if (b->graph) cudaGraphExecDestroy(b->graph);
+            if (b->graph_odd) cudaGraphExecDestroy(b->graph_odd);
+            b->graph = b->graph_odd = nullptr;
+            b->graph_dirty = false;
+        }
+        cudaGraphExec_t &exec = (fused && b->rooms[0].cur) ? b->graph_odd : b->graph;
+        if (!exec) {
             if (!b->capture_stream)
                 ACF_CUDA(cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
             ACF_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
@@ -1352,20 +1614,19 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
             bump_step_base<<<1, 1, 0, b->capture_stream>>>(b->step_base, G);
             cudaGraph_t graph = nullptr;
             ACF_CUDA(cudaStreamEndCapture(b->capture_stream, &graph));
-            cudaError_t err = cudaGraphInstantiate(&b->graph, graph, 0);
+            cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             if (err != cudaSuccess)
                 return fail(ACF_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(err));
-            b->graph_dirty = false;
         }
         for (; done + G <= n_steps; done += G) {
-            ACF_CUDA(cudaGraphLaunch(b->graph, st));
-            b->launches += 2 * G + 1;
+            ACF_CUDA(cudaGraphLaunch(exec, st));
+            b->launches += kernels_per_step * G + 1;
         }
     }
     for (int64_t t = 0; done + t < n_steps; t++) {
         launch_step<T>(b, (int32_t)t, st, nullptr);
-        b->launches += 2;
+        b->launches += kernels_per_step;
     }
     ACF_CUDA(cudaGetLastError());
     return ACF_OK;
@@ -1441,6 +1702,7 @@ int upload_cast(void **dst, const std::vector<double> &host, size_t es) {
 }
 
 void free_room(RoomHost &h) {
+    cudaFree(h.second);
     cudaFree(h.profiles);
     cudaFree(h.shell);
     cudaFree(h.src_off);
@@ -1456,6 +1718,7 @@ void free_batch(acf_batch *b) {
     if (!b) return;
     DeviceGuard guard(b->device);
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->graph_odd) cudaGraphExecDestroy(b->graph_odd);
     b->g_record.release();
     b->g_recompute.release();
     b->g_adjoint.release();
@@ -1811,6 +2074,51 @@ int energy_terms(acf_batch *b, int room, double dx, double terms[7], acf_stream 
     cudaStream_t st = (cudaStream_t)stream;
     return b->precision == 8 ? energy_impl<double>(b, room, dx, terms, st)
                              : energy_impl<float>(b, room, dx, terms, st);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Schemes. The fused step keeps a second copy of p and v; the current state alternates
+// between the two. Paths that work on the primary copy in place (the two sweeps, the adjoint's
+// recorded runs, checkpoints) first bring the state back to it.
+
+namespace {
+
+int make_primary(acf_batch *b, cudaStream_t st) {
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        RoomHost &h = b->rooms[r];
+        if (!h.cur) continue;
+        const size_t bytes = (size_t)4 * h.field * b->elem();
+        ACF_CUDA(cudaMemcpyAsync((char *)b->state + h.state_off, h.second, bytes, cudaMemcpyDeviceToDevice, st));
+        h.cur = 0;
+        b->graph_dirty = b->adj_graphs_dirty = true;
+    }
+    return ACF_OK;
+}
+
+int set_scheme(acf_batch *b, int32_t scheme) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED)
+        return fail(ACF_ERR_ARGUMENT, "unknown scheme %d", scheme);
+    if (scheme == ACF_SCHEME_FUSED && b->rooms.size() != 1)
+        return fail(ACF_ERR_STATE, "the fused scheme is for single rooms");
+    DeviceGuard guard(b->device);
+    if (scheme == ACF_SCHEME_FUSED && !b->rooms[0].second) {
+        RoomHost &h = b->rooms[0];
+        const size_t bytes = ((size_t)4 * h.field + (size_t)h.pz) * b->elem();
+        if (cudaMalloc(&h.second, bytes) != cudaSuccess)
+            return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes for the fused scheme failed", bytes);
+        ACF_CUDA(cudaMemset(h.second, 0, bytes));
+    }
+    if (scheme == ACF_SCHEME_TWO_SWEEPS) {
+        int rc = make_primary(b, 0);
+        if (rc) return rc;
+        ACF_CUDA(cudaStreamSynchronize(0));
+    }
+    if (scheme != b->scheme) b->graph_dirty = b->adj_graphs_dirty = true;
+    b->scheme = scheme;
+    return ACF_OK;
 }
 
 }  // namespace
@@ -2313,6 +2621,10 @@ int acf_profile_read(acf_solver *h, double *velocity_ms, double *pressure_ms, in
 
 int64_t acf_launch_count(const acf_solver *h) { return h ? h->launches : -1; }
 
+int acf_set_scheme(acf_solver *h, int32_t scheme) { return set_scheme(h, scheme); }
+
+int acf_get_scheme(const acf_solver *h) { return h ? h->scheme : -1; }
+
 int acf_set_coefficients(acf_solver *h, const acf_config *config) {
     return set_coefficients(h, 0, config);
 }
@@ -2320,6 +2632,8 @@ int acf_set_coefficients(acf_solver *h, const acf_config *config) {
 int acf_reset_state(acf_solver *h, acf_stream stream) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
     DeviceGuard guard(h->device);
+    h->rooms[0].cur = 0;
+    h->graph_dirty = h->adj_graphs_dirty = true;
     ACF_CUDA(cudaMemsetAsync(h->field_ptr(0, ACF_FIELD_P), 0, h->room_block_bytes(0), (cudaStream_t)stream));
     return ACF_OK;
 }
@@ -2339,6 +2653,10 @@ int acf_forward_record(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_
     if (step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step offset");
     DeviceGuard guard(h->device);
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        int rc0 = make_primary(h, st);
+        if (rc0) return rc0;
+    }
     // Recording capacity as acf_run ensures it.
     int rc = ACF_OK;
     for (RoomHost &r : h->rooms) {

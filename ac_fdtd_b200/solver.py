@@ -101,7 +101,7 @@ class CudaAcousticFDTD:
     def __init__(self, grid, medium=AIR, courant: float = 1.0, dtype=np.float64, walls=None,
                  absorbing_layer=None, air_absorption=None, *, stream: int = 0,
                  steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
-                 differentiable_walls: bool = False) -> None:
+                 differentiable_walls: bool = False, scheme: str = "two_sweeps") -> None:
         block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
                                   air_absorption, force_walls=differentiable_walls)
         self._force_walls = differentiable_walls
@@ -140,6 +140,7 @@ class CudaAcousticFDTD:
         self._receivers: list[tuple[int, int]] = []  # (flat cell, start step)
         self._sources_dirty = False
         self._receivers_dirty = False
+        self.set_scheme(scheme)
 
     # ------------------------------------------------------------------ geometry / time
     @property
@@ -428,6 +429,19 @@ class CudaAcousticFDTD:
         del keep
         self.walls, self.absorbing_layer, self.air_absorption = walls, absorbing_layer, air_absorption
         self.coefficients = block
+
+    SCHEMES = {"two_sweeps": _native.SCHEME_TWO_SWEEPS, "fused": _native.SCHEME_FUSED}
+
+    def set_scheme(self, scheme: str) -> None:
+        """``"two_sweeps"`` (velocity sweep, then pressure sweep, in place) or ``"fused"`` (one
+        sweep into a second copy of p and v). Results are bit-identical; the fused step moves
+        (8 + 2R) elements per cell instead of (12 + 2R) and needs four more fields of memory."""
+        if scheme not in self.SCHEMES:
+            raise ValueError(f"scheme must be one of {sorted(self.SCHEMES)}, got {scheme!r}")
+        self._flush()
+        _native.check(self._lib.acf_set_scheme(self._handle, self.SCHEMES[scheme]), "acf_set_scheme")
+        self.scheme = scheme
+        self._mirror_current.clear()
 
     def set_launch(self, block_threads: int = 256, planes: int = 4) -> None:
         """Launch geometry of the sweeps (threads per block, x planes per block)."""

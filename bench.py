@@ -115,13 +115,14 @@ def measured_peak_hbm() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_cell() -> float | None:
-    """DRAM bytes per cell of one pressure-sweep launch, from the committed ncu summary."""
-    path = ROOT / "profiles" / "pressure_sweep_traffic.json"
+def ncu_traffic_per_cell(kernel: str) -> float | None:
+    """DRAM bytes per cell of one launch of ``kernel``, from the committed ncu summary
+    (``profiles/dram_traffic.json``: one ncu capture on a 256^3 case, scaled per cell)."""
+    path = ROOT / "profiles" / "dram_traffic.json"
     if not path.exists():
         return None
     try:
-        return float(json.loads(path.read_text())["dram_bytes_per_cell"])
+        return float(json.loads(path.read_text())[kernel]["dram_bytes_per_cell"])
     except Exception:
         return None
 
@@ -216,8 +217,10 @@ def run_ours(args) -> None:
     grid, objects, points = workload(args.size)
     solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
     if args.launch:
-        geometry = tuple(int(v) for v in args.launch.split(","))
-        solver.set_launch(*geometry)
+        parts = args.launch.split(",")
+        geometry = (parts[0], int(parts[1]), int(parts[2]))
+        solver.set_scheme(geometry[0])
+        solver.set_launch(*geometry[1:])
     else:
         geometry = apply_tuned(solver)
     solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
@@ -261,31 +264,46 @@ def run_ours(args) -> None:
     cell_updates = grid.n_cells * T * args.steps * world
     value = cell_updates / (elapsed_ms * 1e-3) / 1e9
 
-    # ---- roofline of the dominant kernel (pressure sweep)
+    # ---- roofline of the dominant kernel: the fused step, or the pressure sweep
     R = 3
     itemsize = 4
-    pressure_bytes = grid.n_cells * (5 + 2 * R) * itemsize
-    velocity_bytes = grid.n_cells * 7 * itemsize
-    pres_avg = pres_ms / max(timed_steps, 1)
-    vel_avg = vel_ms / max(timed_steps, 1)
     peak, peak_kind = measured_peak_hbm()
-    achieved = pressure_bytes / (pres_avg * 1e-3) / 1e9
-    traffic_per_cell = ncu_traffic_per_cell()
-    roofline = {
-        "bound": "hbm", "kernel": "pressure_sweep<float,layer,walls,3>",
-        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-        else "fallback 6650 GB/s",
-        "algorithmic_bytes_per_launch": pressure_bytes,
-        "bytes_per_cell": (5 + 2 * R) * itemsize,
-        "avg_launch_ms": pres_avg,
-        "traffic": None if traffic_per_cell is None else traffic_per_cell * grid.n_cells,
-        "velocity_sweep": {"avg_launch_ms": vel_avg, "bytes_per_cell": 7 * itemsize,
-                           "achieved": velocity_bytes / (vel_avg * 1e-3) / 1e9},
-        "step": {"bytes_per_cell": (12 + 2 * R) * itemsize,
-                 "achieved": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9,
-                 "frac": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9 / peak},
-    }
+    peak_source = (f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                   else "fallback 6650 GB/s")
+    vel_avg = vel_ms / max(timed_steps, 1)
+    pres_avg = pres_ms / max(timed_steps, 1)
+    if geometry[0] == "fused":
+        step_bytes = grid.n_cells * (8 + 2 * R) * itemsize
+        step_avg = vel_avg + pres_avg          # one kernel; its time is in the first slot
+        achieved = step_bytes / (step_avg * 1e-3) / 1e9
+        traffic_per_cell = ncu_traffic_per_cell("fused_sweep")
+        roofline = {
+            "bound": "hbm", "kernel": "fused_sweep<float,layer,walls,3>",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_source, "algorithmic_bytes_per_launch": step_bytes,
+            "bytes_per_cell": (8 + 2 * R) * itemsize, "avg_launch_ms": step_avg,
+            "traffic": None if traffic_per_cell is None else traffic_per_cell * grid.n_cells,
+            "two_sweep_equivalent": {"bytes_per_cell": (12 + 2 * R) * itemsize,
+                                     "effective_GBps": grid.n_cells * (12 + 2 * R) * itemsize
+                                     / (step_avg * 1e-3) / 1e9},
+        }
+    else:
+        pressure_bytes = grid.n_cells * (5 + 2 * R) * itemsize
+        velocity_bytes = grid.n_cells * 7 * itemsize
+        achieved = pressure_bytes / (pres_avg * 1e-3) / 1e9
+        traffic_per_cell = ncu_traffic_per_cell("pressure_sweep")
+        roofline = {
+            "bound": "hbm", "kernel": "pressure_sweep<float,layer,walls,3>",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_source, "algorithmic_bytes_per_launch": pressure_bytes,
+            "bytes_per_cell": (5 + 2 * R) * itemsize, "avg_launch_ms": pres_avg,
+            "traffic": None if traffic_per_cell is None else traffic_per_cell * grid.n_cells,
+            "velocity_sweep": {"avg_launch_ms": vel_avg, "bytes_per_cell": 7 * itemsize,
+                               "achieved": velocity_bytes / (vel_avg * 1e-3) / 1e9},
+            "step": {"bytes_per_cell": (12 + 2 * R) * itemsize,
+                     "achieved": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9,
+                     "frac": (pressure_bytes + velocity_bytes) / ((pres_avg + vel_avg) * 1e-3) / 1e9 / peak},
+        }
 
     # ---- end to end through the public API with pinned host buffers
     p0 = pinned_array(grid.shape, np.float32)
@@ -321,7 +339,8 @@ def run_ours(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {**config_dict(args, grid),
-                   "launch": {"block_threads": geometry[0], "planes_per_block": geometry[1],
+                   "launch": {"scheme": geometry[0], "block_threads": geometry[1],
+                              "planes_per_block": geometry[2],
                               "chosen_by": "--launch" if args.launch else "ac_fdtd_b200.autotune"}},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,

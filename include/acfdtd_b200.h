@@ -129,6 +129,14 @@ int acf_download(acf_solver *solver, int field, void *dst, acf_stream stream);
  * source samples (src/ac_fdtd/c/acfdtd.c:358-371). Asynchronous on `stream`. */
 int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream stream);
 
+/* How a single room advances: two sweeps per step over one copy of the state, or one fused
+ * sweep that reads the current p and v and writes the next ones to a second copy (4 more
+ * fields of memory, (8 + 2R) instead of (12 + 2R) elements moved per cell). Both give
+ * bit-identical results. The adjoint's recorded runs use the two sweeps. */
+enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1 };
+int acf_set_scheme(acf_solver *solver, int32_t scheme);
+int acf_get_scheme(const acf_solver *solver);
+
 /* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
 int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);
 

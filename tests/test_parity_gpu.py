@@ -23,10 +23,13 @@ def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def paired(dtype=np.float64, steps_per_graph=64, **configuration):
+SCHEMES = ["two_sweeps", "fused"]
+
+
+def paired(dtype=np.float64, steps_per_graph=64, scheme="two_sweeps", **configuration):
     oracle = prepare(OracleFDTD(GRID, AIR, dtype=dtype, **configuration))
     cuda = prepare(CudaAcousticFDTD(GRID, dtype=dtype, steps_per_graph=steps_per_graph,
-                                    **configuration))
+                                    scheme=scheme, **configuration))
     return oracle, cuda
 
 
@@ -37,10 +40,11 @@ def assert_same_state(cuda, oracle):
     np.testing.assert_array_equal(cuda.recorded_pressure, oracle.recorded_pressure)
 
 
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("name", list(CONFIGURATIONS))
-def test_matches_the_oracle_bitwise(name, dtype, golden_meta, golden_trajectories):
-    oracle, cuda = paired(dtype=dtype, **CONFIGURATIONS[name])
+def test_matches_the_oracle_bitwise(name, dtype, scheme, golden_meta, golden_trajectories):
+    oracle, cuda = paired(dtype=dtype, scheme=scheme, **CONFIGURATIONS[name])
     oracle.run(150)
     cuda.run(150)
     assert_same_state(cuda, oracle)
@@ -76,9 +80,10 @@ def test_graphs_and_step_by_step_launches_agree_bitwise():
     np.testing.assert_array_equal(graphed.recorded_pressure, direct.recorded_pressure)
 
 
-def test_running_in_pieces_is_the_same_as_running_at_once():
-    _, whole = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16)
-    _, pieces = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16)
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_running_in_pieces_is_the_same_as_running_at_once(scheme):
+    _, whole = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16, scheme=scheme)
+    _, pieces = paired(walls=WallAdmittances.uniform(0.2), steps_per_graph=16, scheme=scheme)
     whole.run(120)
     for n in (30, 1, 16, 40, 33):
         pieces.run(n)
@@ -86,8 +91,9 @@ def test_running_in_pieces_is_the_same_as_running_at_once():
     np.testing.assert_array_equal(pieces.recorded_pressure, whole.recorded_pressure)
 
 
-def test_state_written_between_runs_is_used():
-    oracle, cuda = paired(walls=WallAdmittances.uniform(0.3))
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_state_written_between_runs_is_used(scheme):
+    oracle, cuda = paired(walls=WallAdmittances.uniform(0.3), scheme=scheme)
     oracle.run(20)
     cuda.run(20)
     rng = np.random.default_rng(9)
@@ -175,17 +181,18 @@ def test_walls_sponge_air_room_matches_the_reference(dtype, golden_meta, golden_
     assert np.max(np.abs(solver.recorded_pressure - c)) <= tol * scale
 
 
-def test_odd_and_degenerate_grids():
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_odd_and_degenerate_grids(scheme):
     """Sizes that are not multiples of the 4-element vector, and 1-cell-wide ducts."""
     from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid
 
-    for shape in ((1, 1, 9), (5, 1, 1), (3, 2, 7), (2, 3, 1), (7, 5, 13)):
+    for shape in ((1, 1, 9), (5, 1, 1), (3, 2, 7), (2, 3, 1), (7, 5, 13), (4, 4, 4), (3, 5, 8)):
         grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
         configuration = dict(walls=WallAdmittances(0.4, 0.1, 0.0, 0.7, 0.2, 0.0),
                              absorbing_layer=AbsorbingLayer(thickness=2),
                              air_absorption=AirAbsorption())
         oracle = OracleFDTD(grid, AIR, **configuration)
-        cuda = CudaAcousticFDTD(grid, **configuration)
+        cuda = CudaAcousticFDTD(grid, scheme=scheme, **configuration)
         rng = np.random.default_rng(sum(shape))
         initial = rng.standard_normal(shape)
         point = tuple((n - 0.5) * 0.02 for n in shape)
@@ -196,3 +203,22 @@ def test_odd_and_degenerate_grids():
         oracle.run(40)
         cuda.run(40)
         assert_same_state(cuda, oracle)
+
+
+def test_switching_schemes_mid_run_and_odd_step_counts():
+    """The fused scheme alternates between two copies of p and v; switching schemes, odd runs,
+    energy, state access and graph replays from either copy must all see the current state."""
+    configuration = CONFIGURATIONS["everything at once"]
+    oracle, cuda = paired(steps_per_graph=8, scheme="fused", **configuration)
+    plan = [("fused", 9), ("fused", 17), ("two_sweeps", 5), ("fused", 3), ("fused", 16),
+            ("two_sweeps", 8), ("fused", 1)]
+    total = 0
+    for scheme, n in plan:
+        cuda.set_scheme(scheme)
+        cuda.run(n)
+        oracle.run(n)
+        total += n
+        assert cuda.energy() == pytest.approx(oracle.energy(), rel=1e-12)
+        np.testing.assert_array_equal(cuda.p, oracle.p)
+    assert_same_state(cuda, oracle)
+    assert cuda.step_index == total
