@@ -18,6 +18,7 @@ from .boundaries import (
 )
 from .grid import Grid, max_stable_time_step
 from .medium import AIR, Medium
+from .room import ImpulseResponse, Room, simulate_impulse_response
 from .solver import CudaAcousticFDTD, pinned_array
 from .sources import band_limited_impulse, deconvolve, gaussian_derivative_pulse, gaussian_pulse
 
@@ -31,8 +32,10 @@ __all__ = [
     "AirAbsorption",
     "CudaAcousticFDTD",
     "Grid",
+    "ImpulseResponse",
     "Medium",
     "RelaxationProcess",
+    "Room",
     "RoomBatch",
     "WallAdmittances",
     "admittance_from_absorption",
@@ -43,4 +46,5 @@ __all__ = [
     "max_stable_time_step",
     "pinned_array",
     "reflection_coefficient",
+    "simulate_impulse_response",
 ]

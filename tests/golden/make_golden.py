@@ -12,6 +12,8 @@ shared library next to its own source. Outputs (all committed, all small):
 * ``trajectories.npz`` -- the five parity configurations of the reference's own backend tests
   (``tests/test_c_backend.py:15-42``) run for 150 steps in float64 and float32 by the NumPy
   reference: receiver recordings, energies, and SHA-256 digests plus norms of the final fields.
+* ``impulse.npz`` -- ``simulate_impulse_response`` on a small room (recordings, deconvolved
+  signals, excitation) with the statistical formulae and decay metrics of that run.
 * ``rooms.npz`` -- two small rooms in the shape of the benchmark configurations (64^3-like
   plain walls with a Gaussian-derivative source; a walls + sponge + ISO air room with four
   receivers), recordings from the NumPy reference and from the reference C backend.
@@ -208,6 +210,27 @@ def make_rooms(ref_pkg, c_backend) -> tuple[dict, dict]:
     return data, meta
 
 
+def make_impulse(ref_pkg) -> tuple[dict, dict]:
+    """The reference's room workflow end to end on a small room, plus its statistical formulae."""
+    from ac_fdtd import metrics
+
+    room = ref_pkg.Room((0.62, 0.5, 0.41), absorption=0.3)
+    source, receivers = (0.2, 0.17, 0.15), [(0.45, 0.33, 0.28), (0.1, 0.4, 0.3)]
+    ir = ref_pkg.simulate_impulse_response(room, source, receivers, max_frequency=1500.0)
+    data = {"signals": ir.signals, "recorded": ir.recorded, "excitation": ir.excitation}
+    formulae = {
+        "sabine": room.sabine_reverberation_time(), "eyring": room.eyring_reverberation_time(),
+        "diffuse_absorption": room.diffuse_absorption, "air_coefficient": room.air_coefficient(1000.0),
+        "t20": metrics.reverberation_time(ir.signals[0], ir.sample_rate, 20.0),
+        "edt": metrics.early_decay_time(ir.signals[0], ir.sample_rate),
+        "c2ms": metrics.clarity(ir.signals[0], ir.sample_rate, split=0.002),
+    }
+    meta = {"dimensions": room.dimensions, "absorption": room.absorption, "source": source,
+            "receivers": receivers, "max_frequency": 1500.0, "sample_rate": ir.sample_rate,
+            "shape": list(ir.grid.shape), "formulae": formulae}
+    return data, meta
+
+
 def main(reference: str = "/root/reference") -> None:
     scratch = Path(tempfile.mkdtemp(prefix="acfdtd_ref_"))
     shutil.copytree(Path(reference) / "src", scratch / "src")
@@ -221,7 +244,10 @@ def main(reference: str = "/root/reference") -> None:
     np.savez_compressed(HERE / "trajectories.npz", **traj)
     rooms, rooms_meta = make_rooms(ref_pkg, c_backend)
     np.savez_compressed(HERE / "rooms.npz", **rooms)
+    impulse, impulse_meta = make_impulse(ref_pkg)
+    np.savez_compressed(HERE / "impulse.npz", **impulse)
     meta = {"setup": setup_meta, "trajectories": traj_meta, "rooms": rooms_meta,
+            "impulse": impulse_meta,
             "generator": "tests/golden/make_golden.py", "numpy": np.__version__}
     (HERE / "golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     shutil.rmtree(scratch)
