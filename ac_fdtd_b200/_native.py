@@ -34,6 +34,8 @@ EXPORTED_SYMBOLS = (
     "acf_batch_launch_count", "acf_set_coefficients", "acf_adjoint_prepare",
     "acf_adjoint_shell_size", "acf_forward_record", "acf_adjoint_run", "acf_adjoint_download",
     "acf_reset_state", "acf_set_scheme", "acf_get_scheme",
+    "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
+    "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED = 0, 1
@@ -125,6 +127,12 @@ _SIGNATURES = {
     "acf_reset_state": (ctypes.c_int, [_P, _P]),
     "acf_set_scheme": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_get_scheme": (ctypes.c_int, [_P]),
+    "acf_batch_adjoint_prepare": (ctypes.c_int, [_P, _I64]),
+    "acf_batch_adjoint_shell_size": (ctypes.c_int64, [_P, ctypes.c_int32]),
+    "acf_batch_forward_record": (ctypes.c_int, [_P, _I64, _I64, _P]),
+    "acf_batch_adjoint_run": (ctypes.c_int, [_P, _DP, _DP, _DP, _P]),
+    "acf_batch_reset_state": (ctypes.c_int, [_P, _P]),
+    "acf_batch_set_coefficients": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(AcfConfig)]),
 }
 
 

@@ -31,8 +31,8 @@ from .boundaries import FACES, WallAdmittances, patch_index
 from .medium import AIR
 from .solver import CudaAcousticFDTD, _as_double_pointer
 
-__all__ = ["DifferentiableRoom", "RoomGradients", "FixedProcesses", "room_response",
-           "shell_face_gradients"]
+__all__ = ["DifferentiableRoom", "DifferentiableBatch", "RoomGradients", "FixedProcesses",
+           "room_response", "shell_face_gradients", "wall_gradients"]
 
 
 class FixedProcesses:
@@ -86,6 +86,22 @@ def _first_face_slots(shape):
 def shell_face_gradients(shape, grad_a, scale):
     """dL/dxi at every cell of each face from dL/da per shell slot (a = scale * sum xi)."""
     return [scale * grad_a[slot] for slot in _first_face_slots(shape)]
+
+
+def wall_gradients(walls, shape, grad_a, sound_speed, dt, dx):
+    """dL/dxi per wall (six values) or per patch ((6, P, P) for ``WallPatches``), and the
+    per-cell maps, from dL/da per shell slot."""
+    cells = shell_face_gradients(shape, grad_a, sound_speed * dt / (2.0 * dx))
+    if hasattr(walls, "patch_values"):
+        P = walls.patches
+        g = np.zeros((6, P, P))
+        for f, (axis, _) in enumerate(FACES):
+            b, c = [a for a in range(3) if a != axis]
+            ib = patch_index(shape[b], P)
+            ic = patch_index(shape[c], P)
+            np.add.at(g[f], (ib[:, None], ic[None, :]), cells[f])
+        return g, cells
+    return np.array([m.sum() for m in cells]), cells
 
 
 def _air_chain(processes, c, rho, dx, dt, dgain, dmean, ddecay, dscale):
@@ -182,21 +198,8 @@ class DifferentiableRoom:
         block = s.coefficients
         c, rho = float(s.medium.sound_speed), float(s.medium.density)
         if grad_shell is not None:
-            scale = c * block.dt / (2.0 * block.dx)
-            cells = shell_face_gradients(block.shape, grad_shell, scale)
-            out.wall_cells = cells
-            walls = s.walls
-            if hasattr(walls, "patch_values"):
-                P = walls.patches
-                g = np.zeros((6, P, P))
-                for f, (axis, _) in enumerate(FACES):
-                    b, cc = [a for a in range(3) if a != axis]
-                    ib = patch_index(block.shape[b], P)
-                    ic = patch_index(block.shape[cc], P)
-                    np.add.at(g[f], (ib[:, None], ic[None, :]), cells[f])
-                out.walls = g
-            else:
-                out.walls = np.array([m.sum() for m in cells])
+            out.walls, out.wall_cells = wall_gradients(s.walls, block.shape, grad_shell, c,
+                                                       block.dt, block.dx)
         if grad_air is not None:
             R = s.n_relax
             dgain, dmean, ddecay, dscale = grad_air[:R], grad_air[R:2 * R], grad_air[2 * R:3 * R], grad_air[3 * R]
@@ -208,6 +211,72 @@ class DifferentiableRoom:
         _native.check(s._lib.acf_adjoint_download(s._handle, _native.FIELD_P, p0.ctypes.data,
                                                   s._stream), "acf_adjoint_download")
         out.initial_p = p0
+        return out
+
+
+class DifferentiableBatch:
+    """Many rooms differentiated together: one batched forward and one batched adjoint per
+    gradient, with every room's walls (per wall or per patch) and sources as parameters."""
+
+    def __init__(self, rooms, dtype=np.float32, *, max_steps: int) -> None:
+        from .batch import RoomBatch
+
+        self.batch = RoomBatch(rooms, dtype=dtype, steps_per_graph=0, differentiable_walls=True)
+        self.max_steps = int(max_steps)
+        lib = self.batch._lib
+        _native.check(lib.acf_batch_adjoint_prepare(self.batch._handle, self.max_steps),
+                      "acf_batch_adjoint_prepare")
+        self._shell_sizes = [int(lib.acf_batch_adjoint_shell_size(self.batch._handle, r))
+                             for r in range(len(self.batch))]
+        self.n_steps = 0
+
+    def set_walls(self, room: int, walls) -> None:
+        spec = self.batch.specs[room]
+        self.batch.set_coefficients(room, walls, spec.get("absorbing_layer"),
+                                    spec.get("air_absorption"))
+
+    def forward(self, n_steps: int):
+        """Run every room from rest for n_steps; return each room's recordings."""
+        if not 0 < n_steps <= self.max_steps:
+            raise ValueError(f"n_steps must be in 1..{self.max_steps}")
+        b = self.batch
+        b.reset_state()
+        b.step_index = 0
+        b._push_points()
+        _native.check(b._lib.acf_batch_forward_record(b._handle, int(n_steps), 0, b._stream),
+                      "acf_batch_forward_record")
+        b.step_index = int(n_steps)
+        self.n_steps = int(n_steps)
+        return [b.recorded_pressure(r) for r in range(len(b))]
+
+    def backward(self, grad_recordings) -> list[RoomGradients]:
+        """Given dL/d(recordings) per room, the gradients of every room."""
+        b = self.batch
+        n = self.n_steps
+        grad = np.ascontiguousarray(np.concatenate(
+            [np.asarray(g, dtype=np.float64).reshape(len(b._receivers[r]), n)
+             for r, g in enumerate(grad_recordings)], axis=0))
+        n_src = sum(len(s) for s in b._sources)
+        grad_src = np.zeros((max(n_src, 1), n))
+        grad_shell = np.zeros(sum(self._shell_sizes))
+        _native.check(b._lib.acf_batch_adjoint_run(b._handle, _as_double_pointer(grad),
+                                                   _as_double_pointer(grad_src),
+                                                   _as_double_pointer(grad_shell), b._stream),
+                      "acf_batch_adjoint_run")
+        out = []
+        src_row = shell_at = 0
+        for r in range(len(b)):
+            block, spec = b.blocks[r], b.specs[r]
+            medium = spec.get("medium", AIR)
+            k = len(b._sources[r])
+            g = RoomGradients(signal=grad_src[src_row:src_row + k])
+            src_row += k
+            shell = grad_shell[shell_at:shell_at + self._shell_sizes[r]]
+            shell_at += self._shell_sizes[r]
+            g.walls, g.wall_cells = wall_gradients(spec.get("walls") or WallAdmittances(),
+                                                   block.shape, shell,
+                                                   float(medium.sound_speed), block.dt, block.dx)
+            out.append(g)
         return out
 
 

@@ -36,7 +36,8 @@ class RoomBatch:
     """A batch of rooms; ``rooms`` is a list of dicts of ``CudaAcousticFDTD`` arguments."""
 
     def __init__(self, rooms, dtype=np.float32, *, stream: int = 0,
-                 steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH) -> None:
+                 steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
+                 differentiable_walls: bool = False) -> None:
         if not rooms:
             raise ValueError("a batch needs at least one room")
         self.dtype = np.dtype(dtype)
@@ -47,12 +48,14 @@ class RoomBatch:
             raise RuntimeError("no CUDA device is visible; the cuda backend has no CPU path")
         self.specs = [dict(room) for room in rooms]
         self.blocks = []
+        self._force_walls = differentiable_walls
         configs = (_native.AcfConfig * len(rooms))()
         keep = []
         for r, spec in enumerate(self.specs):
             block = room_coefficients(spec["grid"], spec.get("medium", AIR),
                                       spec.get("courant", 1.0), self.dtype, spec.get("walls"),
-                                      spec.get("absorbing_layer"), spec.get("air_absorption"))
+                                      spec.get("absorbing_layer"), spec.get("air_absorption"),
+                                      force_walls=differentiable_walls)
             self.blocks.append(block)
             config = configs[r]
             config.nx, config.ny, config.nz = block.shape
@@ -198,6 +201,27 @@ class RoomBatch:
         _native.check(self._lib.acf_batch_run(self._handle, n_steps, self.step_index,
                                               self._stream), "acf_batch_run")
         self.step_index += n_steps
+
+    def set_coefficients(self, room: int, walls=None, absorbing_layer=None,
+                         air_absorption=None) -> None:
+        """Replace one room's walls, layer and air (same grid, relaxation count and features)."""
+        from .solver import config_from_block
+
+        spec = self.specs[room]
+        block = room_coefficients(spec["grid"], spec.get("medium", AIR), spec.get("courant", 1.0),
+                                  self.dtype, walls, absorbing_layer, air_absorption,
+                                  force_walls=self._force_walls)
+        config, keep = config_from_block(block)
+        _native.check(self._lib.acf_batch_set_coefficients(self._handle, room, ctypes.byref(config)),
+                      "acf_batch_set_coefficients")
+        del keep
+        spec.update(walls=walls, absorbing_layer=absorbing_layer, air_absorption=air_absorption)
+        self.blocks[room] = block
+
+    def reset_state(self) -> None:
+        """Every room at rest (all fields zero), on the device."""
+        _native.check(self._lib.acf_batch_reset_state(self._handle, self._stream),
+                      "acf_batch_reset_state")
 
     def synchronize(self) -> None:
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")

@@ -764,143 +764,148 @@ struct AdjointParams {
     int32_t air;                   // accumulate air gradients (needs hist.fields)
 };
 
+// One (row j, chunk c) column of the adjoint pressure sweep over planes [i_begin, i_end),
+// reversing forward step `step`; air-gradient terms are added to `air_acc`.
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
+__device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &a, int i_begin,
+                                                        int i_end, int j, int c, int64_t step,
+                                                        T *air_acc) {
+    const Room<T> &s = a.room;
+    const int k0 = c * kVec;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool has_above = k0 + kVec <= s.nz;
+    const T scp = s.relax_scale - s.cp;
+    T XL[kVec];
+    Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
+        Vec4<T>::ldg(a.lvx + base + s.plane, XH);
+        Vec4<T>::ldg(a.lvy + base, YL);
+        Vec4<T>::ldg(a.lvy + base + s.pz, YH);
+        Vec4<T>::ldg(a.lvz + base, Z);
+        const T above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+        Vec4<T>::load(a.lp + base, L);
+#pragma unroll
+        for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
+        T HD[kVec], HS[NR > 0 ? NR : 1][kVec];
+        constexpr bool air = AIR && NR > 0;
+        if (air) {
+            const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
+            const T *h = a.hist.fields + slot * (1 + NR) * s.field + base;
+            Vec4<T>::ldg(h, HD);
+#pragma unroll
+            for (int r = 0; r < NR; r++) Vec4<T>::ldg(h + (1 + r) * s.field, HS[r]);
+        }
+        T fi = T(1), fj = T(1);
+        if (LAYER) {
+            fi = __ldg(s.cell[0] + i);
+            fj = __ldg(s.cell[1] + j);
+        }
+        // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}, plus dL/drec[n]
+        T LPn[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            const T up = e + 1 < kVec ? Z[e + 1] : above;
+            T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
+            dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
+            dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
+            LPn[e] = L[e] + s.cv * dmu;
+        }
+        for (int r = 0; r < s.n_rec; r++) {
+            const int64_t d = s.rec_off[r] - base;
+            if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
+#pragma unroll
+                for (int e = 0; e < kVec; e++)
+                    if (e == d) LPn[e] = LPn[e] + g;
+            }
+        }
+        for (int q = 0; q < s.n_src; q++) {
+            const int64_t d = s.src_off[q] - base;
+            if (d >= 0 && d < kVec && step < s.src_len[q]) {
+                T v = LPn[0];
+#pragma unroll
+                for (int e = 1; e < kVec; e++)
+                    if (e == d) v = LPn[e];
+                a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
+            }
+        }
+        T LD[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            LD[e] = T(0);
+            if (k >= s.nz) continue;
+            const T lp = LPn[e];
+            T lph = lp;
+            if (LAYER) {
+                lph = lph * fi;
+                lph = lph * fj;
+                lph = lph * __ldg(s.cell[2] + k);
+            }
+            T lpt = lph, lpart = lph;
+            if (WALLS) {
+                int64_t idx;
+                const int f = shell_face(s, i, j, k, idx);
+                if (f >= 0) {
+                    const T *entry = s.shell[f] + 2 * idx;
+                    const T u = __ldg(entry), q = __ldg(entry + 1);
+                    lpt = u * lph;
+                    lpart = lpt - q * lph;
+                    if (a.grad_shell) {
+                        const T *h = a.hist.shell + 2 * ((step - a.hist.shell_step0) * a.hist.shell_total +
+                                                         a.hist.face_off[f] + idx);
+                        const double uu = (double)u;
+                        a.grad_shell[a.hist.face_off[f] + idx] +=
+                            -(double)lph * uu * uu * ((double)h[1] + (double)h[0]);
+                    }
+                }
+            }
+            T ld = scp * lpt;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const T lpsi = LS[r][e];
+                ld = ld + s.gain[r] * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
+                LS[r][e] = s.decay[r] * lpsi + s.mean[r] * lpt;
+                if (air) {
+                    const T d = HD[e];
+                    const T off = HS[r][e] - s.gain[r] * d;
+                    air_acc[r] += d * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
+                    air_acc[NR + r] += lpt * off;
+                    air_acc[2 * NR + r] += lpsi * off;
+                }
+            }
+            if (air) air_acc[3 * NR] += HD[e] * lpt;
+            L[e] = lpart;
+            LD[e] = ld;
+        }
+        Vec4<T>::store(a.lp + base, L);
+        Vec4<T>::store(a.ld + base, LD);
+#pragma unroll
+        for (int r = 0; r < NR; r++) Vec4<T>::store(a.lpsi + r * s.field + base, LS[r]);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+    }
+}
+
 template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
 __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 2 : 4)))
     adjoint_pressure_sweep(const AdjointParams<T> a) {
-    const Room<T> &s = a.room;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const bool active = c < s.nchunks && j < s.ny;
     constexpr int NA = 3 * NR + 1;
     // Per-thread sums over this launch's few cells in the working precision; the block sums
     // and the sums across blocks and steps are FP64.
     T air_acc[NA];
 #pragma unroll
     for (int t = 0; t < NA; t++) air_acc[t] = T(0);
-
-    if (active) {
-        const int k0 = c * kVec;
+    if (c < a.room.nchunks && j < a.room.ny) {
         const int i_begin = blockIdx.z * a.planes;
-        const int i_end = min(s.nx, i_begin + a.planes);
-        const int64_t column = (int64_t)j * s.pz + k0;
-        const bool has_above = k0 + kVec <= s.nz;
-        const int64_t step = *a.step_base + a.local_step;
-        const T scp = s.relax_scale - s.cp;
-        T XL[kVec];
-        Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
-        for (int i = i_begin; i < i_end; i++) {
-            const int64_t base = (int64_t)i * s.plane + column;
-            T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
-            Vec4<T>::ldg(a.lvx + base + s.plane, XH);
-            Vec4<T>::ldg(a.lvy + base, YL);
-            Vec4<T>::ldg(a.lvy + base + s.pz, YH);
-            Vec4<T>::ldg(a.lvz + base, Z);
-            const T above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
-            Vec4<T>::load(a.lp + base, L);
-#pragma unroll
-            for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
-            T HD[kVec], HS[NR > 0 ? NR : 1][kVec];
-            constexpr bool air = AIR && NR > 0;
-            if (air) {
-                const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
-                const T *h = a.hist.fields + slot * (1 + NR) * s.field + base;
-                Vec4<T>::ldg(h, HD);
-#pragma unroll
-                for (int r = 0; r < NR; r++) Vec4<T>::ldg(h + (1 + r) * s.field, HS[r]);
-            }
-            T fi = T(1), fj = T(1);
-            if (LAYER) {
-                fi = __ldg(s.cell[0] + i);
-                fj = __ldg(s.cell[1] + j);
-            }
-            // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}, plus dL/drec[n]
-            T LPn[kVec];
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                const int k = k0 + e;
-                const T up = e + 1 < kVec ? Z[e + 1] : above;
-                T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
-                dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
-                dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
-                LPn[e] = L[e] + s.cv * dmu;
-            }
-            for (int r = 0; r < s.n_rec; r++) {
-                const int64_t d = s.rec_off[r] - base;
-                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
-                    const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
-#pragma unroll
-                    for (int e = 0; e < kVec; e++)
-                        if (e == d) LPn[e] = LPn[e] + g;
-                }
-            }
-            for (int q = 0; q < s.n_src; q++) {
-                const int64_t d = s.src_off[q] - base;
-                if (d >= 0 && d < kVec && step < s.src_len[q]) {
-                    T v = LPn[0];
-#pragma unroll
-                    for (int e = 1; e < kVec; e++)
-                        if (e == d) v = LPn[e];
-                    a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
-                }
-            }
-            T LD[kVec];
-#pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                const int k = k0 + e;
-                LD[e] = T(0);
-                if (k >= s.nz) continue;
-                const T lp = LPn[e];
-                T lph = lp;
-                if (LAYER) {
-                    lph = lph * fi;
-                    lph = lph * fj;
-                    lph = lph * __ldg(s.cell[2] + k);
-                }
-                T lpt = lph, lpart = lph;
-                if (WALLS) {
-                    int64_t idx;
-                    const int f = shell_face(s, i, j, k, idx);
-                    if (f >= 0) {
-                        const T *entry = s.shell[f] + 2 * idx;
-                        const T u = __ldg(entry), q = __ldg(entry + 1);
-                        lpt = u * lph;
-                        lpart = lpt - q * lph;
-                        if (a.grad_shell) {
-                            const T *h = a.hist.shell + 2 * ((step - a.hist.shell_step0) * a.hist.shell_total +
-                                                             a.hist.face_off[f] + idx);
-                            const double uu = (double)u;
-                            a.grad_shell[a.hist.face_off[f] + idx] +=
-                                -(double)lph * uu * uu * ((double)h[1] + (double)h[0]);
-                        }
-                    }
-                }
-                T ld = scp * lpt;
-#pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    const T lpsi = LS[r][e];
-                    ld = ld + s.gain[r] * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
-                    LS[r][e] = s.decay[r] * lpsi + s.mean[r] * lpt;
-                    if (air) {
-                        const T d = HD[e];
-                        const T off = HS[r][e] - s.gain[r] * d;
-                        air_acc[r] += d * ((T(1) - s.decay[r]) * lpsi - s.mean[r] * lpt);
-                        air_acc[NR + r] += lpt * off;
-                        air_acc[2 * NR + r] += lpsi * off;
-                    }
-                }
-                if (air) air_acc[3 * NR] += HD[e] * lpt;
-                L[e] = lpart;
-                LD[e] = ld;
-            }
-            Vec4<T>::store(a.lp + base, L);
-            Vec4<T>::store(a.ld + base, LD);
-#pragma unroll
-            for (int r = 0; r < NR; r++) Vec4<T>::store(a.lpsi + r * s.field + base, LS[r]);
-#pragma unroll
-            for (int e = 0; e < kVec; e++) XL[e] = XH[e];
-        }
+        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR>(a, i_begin, min(a.room.nx, i_begin + a.planes),
+                                                          j, c, *a.step_base + a.local_step, air_acc);
     }
-
     if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
         __shared__ double red[NA][8];
         const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -923,14 +928,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 
 }
 
 template <typename T, bool LAYER>
-__global__ void __launch_bounds__(256) adjoint_velocity_sweep(const AdjointParams<T> a) {
+__device__ __forceinline__ void adjoint_velocity_column(const AdjointParams<T> &a, int i_begin,
+                                                        int i_end, int j, int c) {
     const Room<T> &s = a.room;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= s.nchunks || j >= s.ny) return;
     const int k0 = c * kVec;
-    const int i_begin = blockIdx.z * a.planes;
-    const int i_end = min(s.nx, i_begin + a.planes);
     const int64_t column = (int64_t)j * s.pz + k0;
     T Dm[kVec];  // lambda_D at plane i - 1
     if (i_begin > 0) Vec4<T>::ldg(a.ld + (int64_t)(i_begin - 1) * s.plane + column, Dm);
@@ -1007,6 +1008,104 @@ __global__ void __launch_bounds__(256) adjoint_velocity_sweep(const AdjointParam
         }
 #pragma unroll
         for (int e = 0; e < kVec; e++) Dm[e] = Dc[e];
+    }
+}
+
+template <typename T, bool LAYER>
+__global__ void __launch_bounds__(256) adjoint_velocity_sweep(const AdjointParams<T> a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= a.room.nchunks || j >= a.room.ny) return;
+    const int i_begin = blockIdx.z * a.planes;
+    adjoint_velocity_column<T, LAYER>(a, i_begin, min(a.room.nx, i_begin + a.planes), j, c);
+}
+
+// ---- batches: per-room adjoint descriptions in a device table, staged like Room in the
+// forward batch kernels. Walls and sources only (no air terms).
+
+template <typename T>
+struct BatchAdjointParams {
+    const AdjointParams<T> *rooms;
+    const Tile *tiles;
+    int32_t n_tiles;
+    int32_t local_step;
+    const int64_t *step_base;
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_adjoint(const AdjointParams<T> *src, AdjointParams<T> *dst) {
+    static_assert(sizeof(AdjointParams<T>) % sizeof(int) == 0, "whole words");
+    const int *from = reinterpret_cast<const int *>(src);
+    int *to = reinterpret_cast<int *>(dst);
+    for (int w = threadIdx.x; w < (int)(sizeof(AdjointParams<T>) / sizeof(int)); w += blockDim.x)
+        to[w] = __ldg(from + w);
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) pressure_batch_rec(const BatchAdjointParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(AdjointParams<T>)];
+    AdjointParams<T> *room = reinterpret_cast<AdjointParams<T> *>(raw);
+    const int64_t step = *b.step_base + b.local_step;
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_adjoint(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            pressure_column<T, LAYER, WALLS, NR, true>(room->room, tile.i_begin, tile.i_end,
+                                                        pair / room->room.nchunks,
+                                                        pair % room->room.nchunks, step, &room->hist);
+        }
+    }
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) adjoint_pressure_batch(const BatchAdjointParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(AdjointParams<T>)];
+    AdjointParams<T> *room = reinterpret_cast<AdjointParams<T> *>(raw);
+    const int64_t step = *b.step_base + b.local_step;
+    T unused[1];
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_adjoint(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            adjoint_pressure_column<T, LAYER, WALLS, NR, false>(*room, tile.i_begin, tile.i_end,
+                                                                pair / room->room.nchunks,
+                                                                pair % room->room.nchunks, step, unused);
+        }
+    }
+}
+
+template <typename T, bool LAYER>
+__global__ void __launch_bounds__(256, 3) adjoint_velocity_batch(const BatchAdjointParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(AdjointParams<T>)];
+    AdjointParams<T> *room = reinterpret_cast<AdjointParams<T> *>(raw);
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_adjoint(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            adjoint_velocity_column<T, LAYER>(*room, tile.i_begin, tile.i_end,
+                                              pair / room->room.nchunks, pair % room->room.nchunks);
+        }
     }
 }
 
@@ -1319,6 +1418,16 @@ struct acf_batch {
         double *grad_rec = nullptr, *grad_src = nullptr;
         int64_t grad_rows_rec = 0, grad_rows_src = 0;
     } adj;
+
+    // adjoint of a batch of rooms (walls and sources): per-room history and adjoint fields
+    struct RoomAdjoint {
+        void *hist_shell = nullptr, *fields = nullptr;
+        double *grad_shell = nullptr, *grad_rec = nullptr, *grad_src = nullptr;
+        int64_t shell_total = 0, face_off[6] = {}, rows_rec = 0, rows_src = 0;
+    };
+    std::vector<RoomAdjoint> badj;
+    int64_t badj_capacity = 0, badj_recorded = 0, badj_step0 = 0;
+    void *badj_table = nullptr;      // device array of AdjointParams<T>, one per room
 
     size_t elem() const { return (size_t)precision; }
     int n_fields() const { return 4 + n_relax; }
@@ -1735,6 +1844,14 @@ void free_batch(acf_batch *b) {
     cudaFree(b->adj.air_partials);
     cudaFree(b->adj.grad_rec);
     cudaFree(b->adj.grad_src);
+    for (auto &ra : b->badj) {
+        cudaFree(ra.hist_shell);
+        cudaFree(ra.fields);
+        cudaFree(ra.grad_shell);
+        cudaFree(ra.grad_rec);
+        cudaFree(ra.grad_src);
+    }
+    cudaFree(b->badj_table);
     cudaFree(b->state);
     cudaFree(b->room_table);
     cudaFree(b->tiles);
@@ -1869,8 +1986,11 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
         return fail(ACF_ERR_MEMORY, "cudaMalloc of energy scratch failed");
     for (auto &ev : b->ring) ACF_CUDA(cudaEventCreate(&ev));
     if (batched) {
-        b->block_threads = 256;
-        b->planes = 4;
+        // one CTA per tile of 128 (row, chunk) pairs x 8 planes: the best measured schedule on
+        // uneven-room batches (persistent grids lose to the hardware scheduler here)
+        b->block_threads = 128;
+        b->planes = 8;
+        b->ctas_per_sm = 0;
     } else {
         b->block_threads = 128;
         b->planes = 4;
@@ -2516,6 +2636,197 @@ int set_coefficients(acf_batch *b, int room, const acf_config *c) {
 
 }  // namespace
 
+// ------------------------------------------------------------------------------------------
+// Adjoint of a batch of rooms: the forward records every room's boundary-shell history with
+// one persistent launch per sweep; the backward runs the adjoint sweeps of all rooms together.
+
+namespace {
+
+template <typename T, bool L, bool W, int NR>
+struct BatchRecPressure {
+    static void launch(const BatchAdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        pressure_batch_rec<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct BatchAdjPressure {
+    static void launch(const BatchAdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        adjoint_pressure_batch<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+int batch_adjoint_prepare(acf_batch *b, int64_t max_steps) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
+    if (max_steps < 1) return fail(ACF_ERR_ARGUMENT, "max_steps must be >= 1");
+    if (!b->any_walls) return fail(ACF_ERR_STATE, "wall gradients need rooms with wall coefficients");
+    DeviceGuard guard(b->device);
+    ACF_CUDA(cudaDeviceSynchronize());
+    for (auto &ra : b->badj) {
+        cudaFree(ra.hist_shell);
+        cudaFree(ra.fields);
+        cudaFree(ra.grad_shell);
+        cudaFree(ra.grad_rec);
+        cudaFree(ra.grad_src);
+    }
+    b->badj.assign(b->rooms.size(), acf_batch::RoomAdjoint());
+    const size_t es = b->elem();
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        const RoomHost &h = b->rooms[r];
+        auto &ra = b->badj[r];
+        const int64_t sizes[6] = {(int64_t)h.ny * h.nz, (int64_t)h.ny * h.nz, (int64_t)h.nx * h.nz,
+                                  (int64_t)h.nx * h.nz, (int64_t)h.nx * h.ny, (int64_t)h.nx * h.ny};
+        for (int q = 0; q < 6; q++) {
+            ra.face_off[q] = ra.shell_total;
+            ra.shell_total += sizes[q];
+        }
+        const size_t hist = (size_t)max_steps * ra.shell_total * 2 * es;
+        if (cudaMalloc(&ra.hist_shell, hist) != cudaSuccess)
+            return fail(ACF_ERR_MEMORY, "room %zu: cudaMalloc of %zu bytes of wall history failed", r, hist);
+        ACF_CUDA(cudaMalloc(&ra.fields, ((size_t)(5 + h.n_relax) * h.field + h.pz) * es));
+        ACF_CUDA(cudaMalloc(&ra.grad_shell, ra.shell_total * sizeof(double)));
+    }
+    b->badj_capacity = max_steps;
+    b->badj_recorded = 0;
+    return ACF_OK;
+}
+
+// Fill the device table of per-room adjoint descriptions for the current run.
+template <typename T>
+int upload_adjoint_table(acf_batch *b, int64_t n) {
+    std::vector<AdjointParams<T>> table(b->rooms.size());
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        const RoomHost &h = b->rooms[r];
+        auto &ra = b->badj[r];
+        AdjointParams<T> &a = table[r];
+        a = AdjointParams<T>{};
+        a.room = make_room<T>(b, (int)r);
+        T *f = (T *)ra.fields;
+        a.lp = f;
+        a.lvx = f + h.field;
+        a.lvy = f + 2 * h.field;
+        a.lvz = f + 3 * h.field;
+        a.lpsi = f + 4 * h.field;
+        a.ld = f + (4 + h.n_relax) * h.field;
+        a.grad_rec = ra.grad_rec;
+        a.grad_src = ra.grad_src;
+        a.grad_stride = b->badj_capacity;
+        a.grad_step0 = b->badj_step0;
+        a.hist.shell = (T *)ra.hist_shell;
+        a.hist.shell_total = ra.shell_total;
+        a.hist.shell_step0 = b->badj_step0;
+        a.hist.shell_steps = b->badj_capacity;
+        for (int q = 0; q < 6; q++) a.hist.face_off[q] = ra.face_off[q];
+        a.hist.fields_slots = 1;
+        a.grad_shell = h.has_walls ? ra.grad_shell : nullptr;
+        a.planes = b->planes;
+        (void)n;
+    }
+    if (!b->badj_table) ACF_CUDA(cudaMalloc(&b->badj_table, table.size() * sizeof(AdjointParams<T>)));
+    ACF_CUDA(cudaMemcpy(b->badj_table, table.data(), table.size() * sizeof(AdjointParams<T>),
+                        cudaMemcpyHostToDevice));
+    return ACF_OK;
+}
+
+template <typename T>
+int batch_forward_record_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
+    b->badj_step0 = step_offset;
+    b->badj_recorded = n_steps;
+    if (b->room_table_dirty) {
+        int rc = upload_room_table<T>(b);
+        if (rc) return rc;
+    }
+    int rc = upload_adjoint_table<T>(b, n_steps);
+    if (rc) return rc;
+    BatchParams<T> v{};
+    v.rooms = (const Room<T> *)b->room_table;
+    v.tiles = b->tiles;
+    v.n_tiles = b->n_tiles;
+    v.step_base = b->step_base;
+    BatchAdjointParams<T> p{};
+    p.rooms = (const AdjointParams<T> *)b->badj_table;
+    p.tiles = b->tiles;
+    p.n_tiles = b->n_tiles;
+    p.step_base = b->step_base;
+    const dim3 grid(b->batch_ctas), block(b->block_threads);
+    set_step_base<<<1, 1, 0, st>>>(b->step_base, step_offset);
+    for (int64_t t = 0; t < n_steps; t++) {
+        v.local_step = p.local_step = (int32_t)t;
+        if (b->any_layer) velocity_batch<T, true><<<grid, block, 0, st>>>(v);
+        else velocity_batch<T, false><<<grid, block, 0, st>>>(v);
+        dispatch_pressure<T, BatchRecPressure>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+    }
+    b->launches += 2 * n_steps + 1;
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+template <typename T>
+int batch_adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double *grad_shell,
+                       cudaStream_t st) {
+    const int64_t n = b->badj_recorded, cap = b->badj_capacity;
+    const size_t es = b->elem();
+    // Inputs and zeroed accumulators, room by room.
+    int64_t rec_row = 0;
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        const RoomHost &h = b->rooms[r];
+        auto &ra = b->badj[r];
+        if (h.n_rec > ra.rows_rec || !ra.grad_rec) {
+            cudaFree(ra.grad_rec);
+            ra.rows_rec = std::max<int64_t>(1, h.n_rec);
+            ACF_CUDA(cudaMalloc(&ra.grad_rec, (size_t)ra.rows_rec * cap * sizeof(double)));
+        }
+        if (h.n_src > ra.rows_src || !ra.grad_src) {
+            cudaFree(ra.grad_src);
+            ra.rows_src = std::max<int64_t>(1, h.n_src);
+            ACF_CUDA(cudaMalloc(&ra.grad_src, (size_t)ra.rows_src * cap * sizeof(double)));
+        }
+        if (h.n_rec > 0)
+            ACF_CUDA(cudaMemcpy2DAsync(ra.grad_rec, cap * sizeof(double), grad_rec + rec_row * n,
+                                       n * sizeof(double), n * sizeof(double), (size_t)h.n_rec,
+                                       cudaMemcpyHostToDevice, st));
+        rec_row += h.n_rec;
+        ACF_CUDA(cudaMemsetAsync(ra.grad_src, 0, (size_t)ra.rows_src * cap * sizeof(double), st));
+        ACF_CUDA(cudaMemsetAsync(ra.fields, 0, ((size_t)(5 + h.n_relax) * h.field + h.pz) * es, st));
+        ACF_CUDA(cudaMemsetAsync(ra.grad_shell, 0, ra.shell_total * sizeof(double), st));
+    }
+    int rc = upload_adjoint_table<T>(b, n);
+    if (rc) return rc;
+    BatchAdjointParams<T> p{};
+    p.rooms = (const AdjointParams<T> *)b->badj_table;
+    p.tiles = b->tiles;
+    p.n_tiles = b->n_tiles;
+    p.step_base = b->step_base;
+    const dim3 grid(b->batch_ctas), block(b->block_threads);
+    set_step_base<<<1, 1, 0, st>>>(b->step_base, b->badj_step0);
+    for (int64_t t = n - 1; t >= 0; t--) {
+        p.local_step = (int32_t)t;
+        dispatch_pressure<T, BatchAdjPressure>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        if (b->any_layer) adjoint_velocity_batch<T, true><<<grid, block, 0, st>>>(p);
+        else adjoint_velocity_batch<T, false><<<grid, block, 0, st>>>(p);
+    }
+    b->launches += 2 * n + 1;
+    ACF_CUDA(cudaGetLastError());
+    int64_t src_row = 0, shell_at = 0;
+    for (size_t r = 0; r < b->rooms.size(); r++) {
+        const RoomHost &h = b->rooms[r];
+        auto &ra = b->badj[r];
+        if (grad_src && h.n_src > 0)
+            ACF_CUDA(cudaMemcpy2DAsync(grad_src + src_row * n, n * sizeof(double), ra.grad_src,
+                                       cap * sizeof(double), n * sizeof(double), (size_t)h.n_src,
+                                       cudaMemcpyDeviceToHost, st));
+        src_row += h.n_src;
+        if (grad_shell)
+            ACF_CUDA(cudaMemcpyAsync(grad_shell + shell_at, ra.grad_shell, ra.shell_total * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        shell_at += ra.shell_total;
+    }
+    ACF_CUDA(cudaStreamSynchronize(st));
+    return ACF_OK;
+}
+
+}  // namespace
+
 // ==========================================================================================
 // C ABI
 
@@ -2797,6 +3108,70 @@ int acf_batch_profile_read(acf_batch *b, double *velocity_ms, double *pressure_m
 }
 
 int64_t acf_batch_launch_count(const acf_batch *b) { return b ? b->launches : -1; }
+
+int acf_batch_adjoint_prepare(acf_batch *b, int64_t max_steps) { return batch_adjoint_prepare(b, max_steps); }
+
+int64_t acf_batch_adjoint_shell_size(const acf_batch *b, int32_t room) {
+    if (!b || room < 0 || room >= (int)b->badj.size()) return -1;
+    return b->badj[room].shell_total;
+}
+
+int acf_batch_forward_record(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
+    if (b->badj.empty()) return fail(ACF_ERR_STATE, "call acf_batch_adjoint_prepare first");
+    if (b->rooms.size() < 2) return fail(ACF_ERR_STATE, "single rooms use acf_forward_record");
+    if (n_steps < 1 || n_steps > b->badj_capacity)
+        return fail(ACF_ERR_ARGUMENT, "n_steps %lld outside 1..%lld prepared", (long long)n_steps,
+                    (long long)b->badj_capacity);
+    if (step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step offset");
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    // recording capacity, as for a run
+    for (RoomHost &r : b->rooms) {
+        if (r.n_rec == 0) continue;
+        const int64_t need = step_offset + n_steps - r.rec_origin;
+        if (need <= r.rec_capacity) continue;
+        int64_t cap = round_up(std::max<int64_t>(need, 2 * r.rec_capacity), 256);
+        const size_t es = b->elem();
+        void *grown = nullptr;
+        ACF_CUDA(cudaStreamSynchronize(st));
+        ACF_CUDA(cudaMalloc(&grown, (size_t)r.n_rec * cap * es));
+        ACF_CUDA(cudaMemset(grown, 0, (size_t)r.n_rec * cap * es));
+        if (r.rec && r.rec_capacity > 0)
+            ACF_CUDA(cudaMemcpy2D(grown, (size_t)cap * es, r.rec, (size_t)r.rec_capacity * es,
+                                  (size_t)r.rec_capacity * es, (size_t)r.n_rec, cudaMemcpyDeviceToDevice));
+        cudaFree(r.rec);
+        r.rec = grown;
+        r.rec_capacity = cap;
+        b->graph_dirty = b->adj_graphs_dirty = true;
+        b->room_table_dirty = true;
+    }
+    return b->precision == 8 ? batch_forward_record_impl<double>(b, n_steps, step_offset, st)
+                             : batch_forward_record_impl<float>(b, n_steps, step_offset, st);
+}
+
+int acf_batch_adjoint_run(acf_batch *b, const double *grad_rec, double *grad_src, double *grad_shell,
+                          acf_stream stream) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
+    if (b->badj.empty() || b->badj_recorded < 1) return fail(ACF_ERR_STATE, "no recorded forward run");
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    return b->precision == 8 ? batch_adjoint_impl<double>(b, grad_rec, grad_src, grad_shell, st)
+                             : batch_adjoint_impl<float>(b, grad_rec, grad_src, grad_shell, st);
+}
+
+int acf_batch_reset_state(acf_batch *b, acf_stream stream) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
+    DeviceGuard guard(b->device);
+    ACF_CUDA(cudaMemsetAsync(b->state, 0, b->state_bytes, (cudaStream_t)stream));
+    return ACF_OK;
+}
+
+int acf_batch_set_coefficients(acf_batch *b, int32_t room, const acf_config *config) {
+    return set_coefficients(b, room, config);
+}
+
+
 
 // ---- utilities --------------------------------------------------------------------------
 

@@ -9,6 +9,9 @@ full-size tests use, from ``numpy.random.default_rng(seed)``:
   faces, ISO air 20 C / 50 % RH (3 relaxation states), Gaussian pulse to 4 kHz, 4 receivers.
 * ``differentiable_room`` -- 128^3, six "true" admittances from absorption U(0.05, 0.5), a
   start perturbed by up to +-30 % per wall, Gaussian pulse to 2 kHz, four receivers, 3000 steps.
+* ``patch_inversion_rooms`` -- 16 rooms of 96-160 cells per axis, each wall split into 4 x 4
+  patches (96 admittances per room, absorption U(0.05, 0.5)), air at 20 C with seeded RH, a
+  16-cell sponge on one face, one source and eight receivers per room.
 * ``uneven_rooms`` -- 64 rooms, 3-10 m per axis at dx = 5 cm (60-200 cells per axis; the
   reference's 10 points per wavelength at 2 kHz would give 175-583), per-wall absorption
   U(0.05, 0.5), air at U(15, 25) C and U(30, 70) % RH, one source and two receivers at least
@@ -24,7 +27,7 @@ from .boundaries import AbsorbingLayer, WallAdmittances, admittance_from_absorpt
 from .grid import Grid
 
 __all__ = ["plain_room_small", "plain_room_large", "uneven_rooms", "differentiable_room",
-           "UNEVEN_DX"]
+           "patch_inversion_rooms", "UNEVEN_DX"]
 
 UNEVEN_DX = 0.05
 
@@ -87,3 +90,28 @@ def differentiable_room(size: int = 128, seed: int = 4, n_receivers: int = 4):
              for _ in range(1 + n_receivers)]
     points = [tuple((i + 0.5) * dx for i in c) for c in cells]
     return grid, true_xi, start_xi, points[0], points[1:]
+
+
+def patch_inversion_rooms(n_rooms: int = 16, seed: int = 5, patches: int = 4,
+                          cells=(96, 160), n_receivers: int = 8):
+    """List of (spec with true WallPatches, start WallPatches (+-30 %), source, receivers)."""
+    from .boundaries import WallPatches
+
+    rng = np.random.default_rng(seed)
+    dx = 343.2 / (10 * 2000.0)
+    out = []
+    for _ in range(n_rooms):
+        shape = rng.integers(cells[0], cells[1] + 1, 3)
+        grid = Grid(dx=dx, nx=int(shape[0]), ny=int(shape[1]), nz=int(shape[2]))
+        alphas = rng.uniform(0.05, 0.5, (6, patches, patches))
+        true = WallPatches(np.vectorize(admittance_from_absorption)(alphas))
+        start = WallPatches(true.patch_values * (1.0 + rng.uniform(-0.3, 0.3, true.patch_values.shape)))
+        face = (int(rng.integers(0, 3)), int(rng.integers(0, 2)))
+        spec = dict(grid=grid, walls=true,
+                    absorbing_layer=AbsorbingLayer(thickness=16, faces=(face,)),
+                    air_absorption=AirAbsorption(temperature=20.0,
+                                                 relative_humidity=float(rng.uniform(30.0, 70.0))))
+        inner = [(0.2 * L, 0.8 * L) for L in grid.lengths]
+        points = [tuple(float(rng.uniform(lo, hi)) for lo, hi in inner) for _ in range(1 + n_receivers)]
+        out.append((spec, start, points[0], points[1:]))
+    return out

@@ -332,6 +332,7 @@ def run_ours(args) -> None:
 
     batched = None if args.skip_extras else batched_vs_per_room(args)
     adjoint = None if args.skip_extras else adjoint_cost(args)
+    inversion = None if args.skip_extras else batched_adjoint_cost(args)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -351,6 +352,7 @@ def run_ours(args) -> None:
         "clocks": clocks.summary(),
         "batched": batched,
         "adjoint": adjoint,
+        "batched_inversion": inversion,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -488,6 +490,55 @@ def adjoint_cost(args) -> dict:
     return out
 
 
+def batched_adjoint_cost(args) -> dict:
+    """One gradient of the batched patch inversion: 16 rooms (96-160 cells per axis), 4 x 4
+    patches per wall (1536 admittances), air + one sponge face, 8 receivers per room, L2 misfit
+    to the signals of the true patches from a start perturbed by up to 30 %."""
+    import torch
+
+    from ac_fdtd_b200 import RoomBatch, gaussian_pulse
+    from ac_fdtd_b200.adjoint import DifferentiableBatch
+    from ac_fdtd_b200.workloads import patch_inversion_rooms
+
+    T = args.inversion_steps
+    rooms = patch_inversion_rooms()
+    specs = [r[0] for r in rooms]
+    cells = int(sum(spec["grid"].n_cells for spec in specs))
+    inversion = DifferentiableBatch(specs, dtype=np.float32, max_steps=T)
+    forward = RoomBatch([dict(spec, walls=start) for spec, start, _, _ in rooms], dtype=np.float32)
+    for r, (spec, start, source, receivers) in enumerate(rooms):
+        for batch in (inversion.batch, forward):
+            batch.add_volume_source(r, source, gaussian_pulse(T, batch.dt(r), 2000.0))
+            for point in receivers:
+                batch.add_pressure_receiver(r, point)
+    targets = [rec.astype(np.float64) for rec in inversion.forward(T)]
+    for r, (_, start, _, _) in enumerate(rooms):
+        inversion.set_walls(r, start)
+
+    def gradient():
+        recordings = inversion.forward(T)
+        inversion.backward([rec.astype(np.float64) - tgt for rec, tgt in zip(recordings, targets)])
+
+    def run_forward():
+        forward.step_index = 0
+        forward.run(T)
+
+    run_forward()
+    forward_ms = min(_device_ms(run_forward, torch) for _ in range(2))
+    gradient()
+    gradient_ms = min(_device_ms(gradient, torch) for _ in range(2))
+    inversion.batch.close()
+    forward.close()
+    return {
+        "workload": f"16 rooms 96-160 cells per axis ({cells} cells), fp32, 4x4 patches per wall "
+                    f"(1536 admittances), ISO air 20 C, 16-cell sponge on one face, 8 receivers "
+                    f"per room, {T} steps; gradient wrt all patches and source samples",
+        "forward_ms": forward_ms, "gradient_ms": gradient_ms, "ratio": gradient_ms / forward_ms,
+        "gradient_steps_per_s": 1000.0 / gradient_ms,
+        "forward_gcups": cells * T / (forward_ms * 1e-3) / 1e9,
+    }
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -504,6 +555,7 @@ def main() -> None:
     parser.add_argument("--launch", default="",
                         help="fixed sweep geometry 'threads,planes' instead of the autotuner")
     parser.add_argument("--adjoint-steps", type=int, default=3000)
+    parser.add_argument("--inversion-steps", type=int, default=2500)
     args = parser.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -253,6 +253,19 @@ int acf_batch_profile_read(acf_batch *batch, double *velocity_ms, double *pressu
                            int64_t *launches);
 int64_t acf_batch_launch_count(const acf_batch *batch);
 
+/* Adjoint of a batch (wall and source gradients; no counterpart in the reference): as the
+ * single-room acf_adjoint_* calls, for every room at once. grad_rec concatenates each room's
+ * (n_receivers x n_steps) block in room order; grad_src likewise (n_sources x n_steps); grad_shell
+ * concatenates each room's acf_batch_adjoint_shell_size(room) entries. */
+int acf_batch_adjoint_prepare(acf_batch *batch, int64_t max_steps);
+int64_t acf_batch_adjoint_shell_size(const acf_batch *batch, int32_t room);
+int acf_batch_forward_record(acf_batch *batch, int64_t n_steps, int64_t step_offset,
+                             acf_stream stream);
+int acf_batch_adjoint_run(acf_batch *batch, const double *grad_rec, double *grad_src,
+                          double *grad_shell, acf_stream stream);
+int acf_batch_reset_state(acf_batch *batch, acf_stream stream);
+int acf_batch_set_coefficients(acf_batch *batch, int32_t room, const acf_config *config);
+
 /* Block until all work queued on `stream` is done. */
 int acf_synchronize(acf_stream stream);
 

@@ -1,0 +1,96 @@
+"""Batched adjoint: every room's gradients equal the single-room adjoint's, bit for bit, and a
+patch gradient matches central finite differences (float64)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid, WallAdmittances, gaussian_pulse
+from ac_fdtd_b200.adjoint import DifferentiableBatch, DifferentiableRoom
+from ac_fdtd_b200.boundaries import WallPatches
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 70
+
+
+def rooms():
+    rng = np.random.default_rng(11)
+    return [
+        dict(grid=Grid(dx=0.05, nx=13, ny=11, nz=9),
+             walls=WallPatches(rng.uniform(0.05, 0.6, (6, 2, 2))),
+             air_absorption=AirAbsorption(temperature=20.0, relative_humidity=40.0)),
+        dict(grid=Grid(dx=0.05, nx=9, ny=14, nz=12), walls=WallAdmittances(0.2, 0.1, 0.3, 0.05, 0.4, 0.15),
+             absorbing_layer=AbsorbingLayer(thickness=3, faces=((1, 1),)),
+             air_absorption=AirAbsorption(temperature=20.0, relative_humidity=60.0)),
+        dict(grid=Grid(dx=0.05, nx=16, ny=7, nz=10),
+             walls=WallPatches(rng.uniform(0.05, 0.6, (6, 3, 3))),
+             air_absorption=AirAbsorption(temperature=20.0, relative_humidity=50.0)),
+    ]
+
+
+def points(spec, seed):
+    rng = np.random.default_rng(seed)
+    L = spec["grid"].lengths
+    return [tuple(float(rng.uniform(0.2, 0.8)) * x for x in L) for _ in range(4)]
+
+
+def setup_batch(specs):
+    batch = DifferentiableBatch(specs, dtype=np.float64, max_steps=STEPS)
+    for r, spec in enumerate(specs):
+        pts = points(spec, r)
+        batch.batch.add_volume_source(r, pts[0], gaussian_pulse(STEPS, batch.batch.dt(r), 2000.0))
+        for p in pts[1:]:
+            batch.batch.add_pressure_receiver(r, p)
+    return batch
+
+
+def test_batched_gradients_equal_single_room_gradients():
+    specs = rooms()
+    batch = setup_batch(specs)
+    recs = batch.forward(STEPS)
+    weights = [np.random.default_rng(20 + r).standard_normal(rec.shape) for r, rec in enumerate(recs)]
+    grads = batch.backward([w * rec for w, rec in zip(weights, recs, strict=True)])
+    for r, spec in enumerate(specs):
+        room = DifferentiableRoom(spec["grid"], dtype=np.float64, walls=spec["walls"],
+                                  absorbing_layer=spec.get("absorbing_layer"),
+                                  air_absorption=spec["air_absorption"], max_steps=STEPS)
+        pts = points(spec, r)
+        room.solver.add_volume_source(pts[0], gaussian_pulse(STEPS, room.dt, 2000.0))
+        for p in pts[1:]:
+            room.solver.add_pressure_receiver(p)
+        rec = room.forward(STEPS)
+        np.testing.assert_array_equal(rec, recs[r])
+        single = room.backward(weights[r] * rec)
+        np.testing.assert_array_equal(grads[r].walls, single.walls)
+        np.testing.assert_array_equal(grads[r].signal, single.signal)
+        room.solver.close()
+
+
+def test_batched_patch_gradient_matches_central_differences():
+    specs = rooms()
+    batch = setup_batch(specs)
+    recs = batch.forward(STEPS)
+    weights = [np.random.default_rng(30 + r).standard_normal(rec.shape) for r, rec in enumerate(recs)]
+    grads = batch.backward([w * rec for w, rec in zip(weights, recs, strict=True)])
+
+    def loss():
+        out = batch.forward(STEPS)
+        return sum(0.5 * float(np.sum(w * o**2)) for w, o in zip(weights, out, strict=True))
+
+    values = specs[2]["walls"].patch_values
+    checked = ((1, 2, 0), (4, 0, 1), (5, 1, 1))
+    fds = []
+    for f, a, b in checked:
+        h = 1e-6 * values[f, a, b]
+        plus, minus = values.copy(), values.copy()
+        plus[f, a, b] += h
+        minus[f, a, b] -= h
+        batch.set_walls(2, WallPatches(plus))
+        lp = loss()
+        batch.set_walls(2, WallPatches(minus))
+        lm = loss()
+        fds.append((lp - lm) / (2 * h))
+    got = np.array([grads[2].walls[c] for c in checked])
+    assert np.max(np.abs(got - np.array(fds))) <= 1e-6 * np.max(np.abs(grads[2].walls)), (got, fds)
