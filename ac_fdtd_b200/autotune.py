@@ -22,7 +22,7 @@ __all__ = ["CANDIDATES", "BATCH_CANDIDATES", "tune", "apply_tuned", "tune_batch"
 CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
 
 #: (threads per tile, planes per tile, CTAs per SM; 0 = one CTA per tile) for batches.
-BATCH_CANDIDATES = ((256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8, 0), (256, 4, 4),
+BATCH_CANDIDATES = ((128, 8, 0), (256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8, 0), (256, 4, 4),
                     (128, 4, 8), (256, 2, 0))
 
 _cache: dict[str, tuple[int, int]] = {}

@@ -2,9 +2,9 @@
 
 Each room is described by the arguments of ``CudaAcousticFDTD`` (grid, medium, courant, walls,
 absorbing_layer, air_absorption); all rooms share the precision and the number of ISO
-relaxation processes and step in lockstep. Both sweeps of a step are single persistent launches
-over a flat tile table that covers every room, and long runs replay CUDA graphs of those
-launches. Per room, the arithmetic is exactly that of the single-room solver, so every room's
+relaxation processes and step in lockstep. Both sweeps of a step are single launches over a
+flat tile table that covers every room (one CTA per tile, or a persistent grid striding over
+the table), and long runs replay CUDA graphs of those launches. Per room, the arithmetic is exactly that of the single-room solver, so every room's
 fields and recordings equal a ``CudaAcousticFDTD`` run of that room alone, bit for bit.
 
 The reference solves one room per solver object (``src/ac_fdtd/scheme.py:82``); batching is
@@ -226,7 +226,7 @@ class RoomBatch:
     def synchronize(self) -> None:
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")
 
-    def set_launch(self, block_threads: int = 256, planes: int = 4, ctas_per_sm: int = 4) -> None:
+    def set_launch(self, block_threads: int = 128, planes: int = 8, ctas_per_sm: int = 0) -> None:
         _native.check(self._lib.acf_batch_set_launch(self._handle, int(block_threads), int(planes),
                                                      int(ctas_per_sm)), "acf_batch_set_launch")
 
