@@ -15,8 +15,8 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["CANDIDATES", "BATCH_CANDIDATES", "tune", "apply_tuned", "tune_batch",
-           "apply_tuned_batch"]
+__all__ = ["CANDIDATES", "BATCH_CANDIDATES", "STAGED_CANDIDATES", "tune", "apply_tuned",
+           "tune_batch", "apply_tuned_batch"]
 
 #: (threads per block, planes per block) tried by default.
 CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
@@ -28,8 +28,28 @@ BATCH_CANDIDATES = ((128, 8, 0), (256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8,
 _cache: dict[str, tuple[int, int]] = {}
 
 
-#: Schemes raced by default; both give bit-identical results.
-SCHEMES = ("fused", "two_sweeps")
+#: (rows per CTA, ring buffers (0: automatic), planes per CTA) tried for the staged scheme.
+STAGED_CANDIDATES = ((2, 0, 8), (2, 0, 16), (2, 0, 32), (1, 0, 16), (2, 3, 16), (4, 0, 16))
+
+#: Schemes raced by default; all give bit-identical results.
+SCHEMES = ("staged", "fused", "two_sweeps")
+
+
+def _apply(solver, candidate) -> None:
+    """Put ``solver`` on ``candidate`` = (scheme, *geometry); RuntimeError if it cannot run."""
+    scheme, *geometry = candidate
+    if scheme == "staged":
+        rows, stages, planes = geometry
+        solver.set_staging(rows, stages, planes)
+    else:
+        solver.set_launch(*geometry)
+    solver.set_scheme(scheme)
+
+
+def _candidates(schemes, candidates, staged_candidates):
+    for scheme in schemes:
+        for geometry in (staged_candidates if scheme == "staged" else candidates):
+            yield (scheme, *geometry)
 
 
 def _key(solver) -> str:
@@ -58,9 +78,10 @@ def _store_file(key: str, value) -> None:
     Path(path).write_text(json.dumps(data, indent=1))
 
 
-def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schemes=SCHEMES):
-    """Time each (scheme, threads, planes) on a scratch twin of ``solver``; return
-    (best, {candidate: ms/step})."""
+def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schemes=SCHEMES,
+         staged_candidates=STAGED_CANDIDATES):
+    """Time each (scheme, threads, planes) -- (scheme, rows, stages, planes) for the staged
+    scheme -- on a scratch twin of ``solver``; return (best, {candidate: ms/step})."""
     from .solver import CudaAcousticFDTD
 
     twin = CudaAcousticFDTD(solver.grid, solver.medium, solver.courant, solver.dtype,
@@ -69,10 +90,9 @@ def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schem
     twin.p[:] = np.random.default_rng(0).standard_normal(twin.p.shape) * 1e-3
     timings = {}
     try:
-        for candidate in [(sc, *geo) for sc in schemes for geo in candidates]:
+        for candidate in _candidates(schemes, candidates, staged_candidates):
             try:
-                twin.set_scheme(candidate[0])
-                twin.set_launch(*candidate[1:])
+                _apply(twin, candidate)
             except RuntimeError:
                 continue
             twin.run(2)
@@ -90,21 +110,21 @@ def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schem
     return winner, timings
 
 
-def apply_tuned(solver, candidates=CANDIDATES, schemes=SCHEMES):
+def apply_tuned(solver, candidates=CANDIDATES, schemes=SCHEMES,
+                staged_candidates=STAGED_CANDIDATES):
     """Set the fastest scheme and geometry for this configuration (tuned once per shape
-    class); returns (scheme, threads, planes)."""
+    class); returns (scheme, threads, planes) or ("staged", rows, stages, planes)."""
     key = _key(solver)
     if key not in _cache:
         stored = _load_file().get(key)
         if stored:
             _cache[key] = tuple(stored)
         else:
-            winner, _ = tune(solver, candidates, schemes=schemes)
+            winner, _ = tune(solver, candidates, schemes=schemes,
+                             staged_candidates=staged_candidates)
             _cache[key] = winner
             _store_file(key, winner)
-    scheme, threads, planes = _cache[key]
-    solver.set_scheme(scheme)
-    solver.set_launch(threads, planes)
+    _apply(solver, _cache[key])
     return _cache[key]
 
 

@@ -637,6 +637,351 @@ __global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(T, LAYER, NR)) fused
 }
 
 // ------------------------------------------------------------------------------------------
+// The fused step with its inputs staged in shared memory by the bulk-copy engine.
+//
+// A CTA owns `rows` consecutive y rows (whole padded z rows) over a range of x planes. Rows
+// j..j+n of one plane of a field are adjacent in the padded layout, so each field's share of a
+// plane is ONE contiguous cp.async.bulk: p over rows j0-1 .. j0+rows (the y halo), vy over
+// j0 .. j0+rows, vx, vz and the relaxation states over j0 .. j0+rows-1. One thread issues the
+// copies of a plane into a ring of `stages` buffers, each completing its own mbarrier; every
+// thread computes plane i from buffers i and i+1 (p and vx of the next plane) while the next
+// stages-2 planes are already in flight, so the bytes in flight no longer depend on how many
+// registers the arithmetic needs. The arithmetic is fused_column's, element for element, so the
+// results are identical to the two-sweep and fused schemes.
+//
+// Every wait is bounded (about two seconds). A CTA whose wait runs out raises the room's error
+// flag, waits (bounded again) for the copies it has issued and returns; the host reports the
+// flag as an error.
+
+constexpr int kStagedBarrierBytes = 128;       // room for up to 16 mbarriers
+constexpr int kStagedMaxStages = 8;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+constexpr int kWaitLimitIterations = 1 << 21;
+
+template <typename T>
+struct StagedParams {
+    FusedParams<T> f;
+    int32_t rows, stages;
+    int64_t stage_elems;            // elements of one ring buffer
+    int64_t off_vx, off_vy, off_vz, off_psi;
+    int32_t *error;                 // set to 1 when a wait ran out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// One try with a suspend-time hint of a microsecond: true once the phase of `parity` completed.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, P;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false when the phase completed neither within kWaitLimitNs nor within
+// kWaitLimitIterations tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t start = global_ns();
+    for (int it = 0; it < kWaitLimitIterations; it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - start > kWaitLimitNs) return false;
+    }
+    return false;
+}
+
+// Global -> shared bulk copy (no multicast), completing `bytes` on the mbarrier. Both addresses
+// are 16-byte aligned and bytes is a multiple of 16: every copy here starts on a padded row.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void lds4(const T *a, T v[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(a);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else {
+        const double2 t0 = *reinterpret_cast<const double2 *>(a);
+        const double2 t1 = *reinterpret_cast<const double2 *>(a + 2);
+        v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+    }
+}
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<T> g) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const FusedParams<T> &f = g.f;
+    const Room<T> &s = f.room;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    T *ring = reinterpret_cast<T *>(smem + kStagedBarrierBytes);
+    T *zcell = ring + (int64_t)g.stages * g.stage_elems;   // LAYER: cell[2], then face[2]
+    T *zface = zcell + s.pz;
+
+    const int S = g.stages;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int j0 = blockIdx.x * g.rows;
+    const int i_begin = blockIdx.y * f.planes;
+    const int i_end = min(s.nx, i_begin + f.planes);
+    // Rows each copy covers. Own rows stop at the last real row; the p halo stops at ny - 1.
+    const int n_own = min(g.rows, s.ny - j0);
+    const int p_lo = max(j0 - 1, 0);
+    const int p_hi = min(j0 + n_own, s.ny - 1);
+    const uint32_t row_bytes = (uint32_t)(s.pz * (int64_t)sizeof(T));
+    const uint32_t bytes_p = (uint32_t)(p_hi - p_lo + 1) * row_bytes;
+    const uint32_t bytes_own = (uint32_t)n_own * row_bytes;
+    const uint32_t bytes_vy = (uint32_t)(n_own + 1) * row_bytes;
+
+    // Plane i into buffer `slot`. Plane i_end (<= nx, inside every field's nx + 1 planes) is
+    // only read for p and vx, and its relaxation states belong to the next CTA along x.
+    auto issue = [&](int i, int slot) {
+        T *dst = ring + (int64_t)slot * g.stage_elems;
+        const int64_t plane = (int64_t)i * s.plane;
+        const int64_t own = plane + (int64_t)j0 * s.pz;
+        const bool whole = i < i_end;
+        const uint32_t total = bytes_p + bytes_own + (whole ? bytes_vy + bytes_own * (1 + NR) : 0u);
+        mbar_arrive_expect_tx(full + slot, total);
+        bulk_load(dst + (int64_t)(p_lo - j0 + 1) * s.pz, s.p + plane + (int64_t)p_lo * s.pz, bytes_p,
+                  full + slot);
+        bulk_load(dst + g.off_vx, s.vx + own, bytes_own, full + slot);
+        if (whole) {
+            bulk_load(dst + g.off_vy, s.vy + own, bytes_vy, full + slot);
+            bulk_load(dst + g.off_vz, s.vz + own, bytes_own, full + slot);
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+                bulk_load(dst + g.off_psi + (int64_t)r * g.rows * s.pz, s.psi + r * s.field + own,
+                          bytes_own, full + slot);
+        }
+    };
+
+    if (tid == 0) {
+        for (int q = 0; q < S; q++) mbar_init(full + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (LAYER) {
+        const int nthreads = blockDim.x * blockDim.y;
+        for (int k = tid; k <= s.nz; k += nthreads) {
+            zcell[k] = __ldg(s.cell[2] + min(k, s.nz - 1));
+            zface[k] = __ldg(s.face[2] + k);
+        }
+    }
+    __syncthreads();
+    int issued = i_begin - 1;   // last plane issued (thread 0)
+    if (tid == 0) {
+        for (int q = 0; q < S && i_begin + q <= i_end; q++) issue(i_begin + q, q);
+        issued = min(i_begin + S - 1, i_end);
+    }
+
+    const int c = threadIdx.x;
+    const int ry = threadIdx.y;
+    const int j = j0 + ry;
+    const bool active = c < s.nchunks && j < s.ny;
+    const int k0 = c * kVec;
+    const T cv = s.cv, cp = s.cp;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    const int64_t step = any_point ? (*f.step_base + f.local_step) : 0;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool has_above = k0 + kVec < s.nz;
+
+    T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
+    T XL[kVec];
+    if (active) {
+        if (LAYER) {
+            fj_cell = __ldg(s.cell[1] + j);
+            fj_face = __ldg(s.face[1] + j);
+            fj1_face = __ldg(s.face[1] + j + 1);
+        }
+        // The updated vx on face i_begin, as fused_column starts its march.
+        const int64_t base = (int64_t)i_begin * s.plane + column;
+        T P0[kVec], V[kVec], Q[kVec];
+        Vec4<T>::ldg(s.p + base, P0);
+        Vec4<T>::ldg(s.vx + base, V);
+        if (i_begin > 0) Vec4<T>::ldg(s.p + base - s.plane, Q);
+        const T fi_face = LAYER ? __ldg(s.face[0] + i_begin) : T(1);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            T v = V[e];
+            if (i_begin > 0) v = v - cv * (P0[e] - Q[e]);
+            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell, LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1));
+        }
+    }
+
+    int i = i_begin;
+    bool ok = true;
+    for (; i < i_end; i++) {
+        const int u = i - i_begin;
+        const int slot = u % S, nslot = (u + 1) % S;
+        const bool ready = mbar_wait(full + slot, (uint32_t)(u / S) & 1u) &&
+                           mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u);
+        if (ready && active) {
+            const T *cur = ring + (int64_t)slot * g.stage_elems;
+            const T *nxt = ring + (int64_t)nslot * g.stage_elems;
+            const int64_t base = (int64_t)i * s.plane + column;
+            const bool x_inner = i + 1 < s.nx;
+            const T *prow = cur + (int64_t)(ry + 1) * s.pz + k0;
+            const T *vyrow = cur + g.off_vy + (int64_t)ry * s.pz + k0;
+            const T *vzrow = cur + g.off_vz + (int64_t)ry * s.pz + k0;
+            T P[kVec], PX[kVec], VXo[kVec], PYm[kVec], PYp[kVec], VY[kVec], VYp[kVec], VZ[kVec];
+            T Sg[NR > 0 ? NR : 1][kVec];
+            lds4<T>(prow, P);
+            if (x_inner) lds4<T>(nxt + (int64_t)(ry + 1) * s.pz + k0, PX);
+            lds4<T>(nxt + g.off_vx + (int64_t)ry * s.pz + k0, VXo);
+            if (j > 0) lds4<T>(prow - s.pz, PYm);
+            if (j + 1 < s.ny) lds4<T>(prow + s.pz, PYp);
+            lds4<T>(vyrow, VY);
+            lds4<T>(vyrow + s.pz, VYp);
+            lds4<T>(vzrow, VZ);
+            const T p_below = k0 > 0 ? prow[-1] : T(0);
+            const T p_above = has_above ? prow[kVec] : T(0);
+            const T vz_above = k0 + kVec <= s.nz ? vzrow[kVec] : T(0);
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+                lds4<T>(cur + g.off_psi + ((int64_t)r * g.rows + ry) * s.pz + k0, Sg[r]);
+            T fi_cell = T(1), fi1_face = T(1);
+            if (LAYER) {
+                fi_cell = __ldg(s.cell[0] + i);
+                fi1_face = __ldg(s.face[0] + i + 1);
+            }
+
+            T XH[kVec], YL[kVec], YH[kVec], ZL[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                const T fkc = LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1);
+                T v = VXo[e];
+                if (x_inner) v = v - cv * (PX[e] - P[e]);
+                XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc);
+                v = VY[e];
+                if (j > 0) v = v - cv * (P[e] - PYm[e]);
+                YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc);
+                v = VYp[e];
+                if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
+                YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc);
+                const int k = k0 + e;
+                v = VZ[e];
+                if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
+                ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, LAYER ? zface[min(k0 + e, s.nz)] : T(1));
+            }
+            T ZH3 = vz_above;
+            if (has_above) ZH3 = ZH3 - cv * (p_above - P[kVec - 1]);
+            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, LAYER ? zface[min(k0 + kVec, s.nz)] : T(1));
+
+            T Pn[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                const int k = k0 + e;
+                T pe = P[e];
+                if (k < s.nz) {
+                    const T zh = e + 1 < kVec ? ZL[e + 1] : ZH3;
+                    T d = XH[e] - XL[e];
+                    d = d + (YH[e] - YL[e]);
+                    d = d + (zh - ZL[e]);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const T target = d * s.gain[r];
+                        const T offset = Sg[r][e] - target;
+                        Sg[r][e] = offset * s.decay[r] + target;
+                        pe = pe + offset * s.mean[r];
+                    }
+                    if (NR > 0) pe = pe + d * s.relax_scale;
+                    pe = pe - d * cp;
+                    if (WALLS) {
+                        T fu, fp;
+                        if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
+                    }
+                    if (LAYER) {
+                        pe = pe * fi_cell;
+                        pe = pe * fj_cell;
+                        pe = pe * zcell[k];
+                    }
+                }
+                Pn[e] = pe;
+            }
+            if (any_point) {
+                for (int q = 0; q < s.n_src; q++) {
+                    const int64_t d = s.src_off[q] - base;
+                    if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
+#pragma unroll
+                        for (int e = 0; e < kVec; e++)
+                            if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+                    }
+                }
+            }
+
+            T ZS[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) ZS[e] = k0 + e <= s.nz ? ZL[e] : VZ[e];
+            Vec4<T>::store(f.np + base, Pn);
+            Vec4<T>::store(f.nvx + base, XL);
+            Vec4<T>::store(f.nvy + base, YL);
+            Vec4<T>::store(f.nvz + base, ZS);
+            if (i == s.nx - 1) Vec4<T>::store(f.nvx + base + s.plane, XH);
+            if (j == s.ny - 1) Vec4<T>::store(f.nvy + base + s.pz, YH);
+            if (k0 + kVec == s.nz) f.nvz[base + kVec] = ZH3;
+#pragma unroll
+            for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, Sg[r]);
+
+            if (any_point) {
+                for (int r = 0; r < s.n_rec; r++) {
+                    const int64_t d = s.rec_off[r] - base;
+                    if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                        T v = Pn[0];
+#pragma unroll
+                        for (int e = 1; e < kVec; e++)
+                            if (e == d) v = Pn[e];
+                        s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
+                    }
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+        }
+        // Every thread is done with buffer `slot` (plane i); refill it with plane i + S.
+        if (__syncthreads_or(!ready)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0 && i + S <= i_end) {
+            issue(i + S, slot);
+            issued = i + S;
+        }
+    }
+    if (!ok && tid == 0) {
+        atomicExch(g.error, 1);
+        // Let the copies still in flight land before the CTA's shared memory is released.
+        for (int q = i; q <= issued; q++) {
+            const int u = q - i_begin;
+            mbar_wait(full + u % S, (uint32_t)(u / S) & 1u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // One room: 2D grid of (chunk, row) threads; blockIdx.z selects a group of `planes` x planes.
 
 template <typename T, bool LAYER>
@@ -1362,7 +1707,8 @@ struct acf_batch {
     Tile *tiles = nullptr;
     int32_t n_tiles = 0;
     int32_t batch_ctas = 0;
-    int64_t *step_base = nullptr;    // one int64 in device memory
+    int64_t *step_base = nullptr;    // two int64 in device memory: the step counter, then
+                                     // the error flag of the staged sweep (an int32)
     double *energy_scratch = nullptr;
     int energy_blocks = 0;
     int sms = 148;
@@ -1371,6 +1717,9 @@ struct acf_batch {
     int block_threads = 256;
     int planes = 4;
     int ctas_per_sm = 4;
+    int staged_rows = 2;             // staged scheme: y rows per CTA
+    int staged_stages = 0;           // staged scheme: ring buffers per CTA (0: automatic)
+    int smem_per_sm = 233472, smem_per_block = 232448;
 
     // graphs (index: parity of the fused scheme's current buffer at the start of a replay)
     int32_t graph_steps = 0;
@@ -1433,6 +1782,11 @@ struct acf_batch {
     int n_fields() const { return 4 + n_relax; }
     size_t room_block_bytes(int r) const { return (size_t)n_fields() * rooms[r].field * elem(); }
     int scheme = ACF_SCHEME_TWO_SWEEPS;
+    // one sweep per step into the second copy of p and v (fused or fused-staged)
+    bool fused() const {
+        return rooms.size() == 1 && (scheme == ACF_SCHEME_FUSED || scheme == ACF_SCHEME_FUSED_STAGED);
+    }
+    int32_t *error_flag() const { return reinterpret_cast<int32_t *>(step_base + 1); }
     char *field_ptr(int r, int f) const {
         const RoomHost &h = rooms[r];
         if (h.cur && f < 4) return (char *)h.second + (size_t)f * h.field * elem();
@@ -1605,12 +1959,66 @@ struct FusedStep {
     }
 };
 
+// Ring layout and shared memory of the staged sweep for `rows` y rows per CTA.
+struct StagedLayout {
+    int64_t stage_elems = 0, off_vx = 0, off_vy = 0, off_vz = 0, off_psi = 0;
+    size_t smem(int stages, bool layer, int64_t pz, size_t es) const {
+        return kStagedBarrierBytes + (size_t)stages * stage_elems * es + (layer ? 2 * (size_t)pz * es : 0);
+    }
+};
+
+inline StagedLayout staged_layout(const RoomHost &h, int rows) {
+    StagedLayout L;
+    L.off_vx = (int64_t)(rows + 2) * h.pz;             // p: rows + 2 (y halo)
+    L.off_vy = L.off_vx + (int64_t)rows * h.pz;        // vx: rows
+    L.off_vz = L.off_vy + (int64_t)(rows + 1) * h.pz;  // vy: rows + 1
+    L.off_psi = L.off_vz + (int64_t)rows * h.pz;       // vz: rows
+    L.stage_elems = L.off_psi + (int64_t)h.n_relax * rows * h.pz;
+    return L;
+}
+
+inline int staged_block_x(const RoomHost &h) { return (int)round_up((h.nz + kVec - 1) / kVec, 32); }
+
+// Ring buffers for (rows, requested): the request if it fits, else 0; for 0, the most (<= 4)
+// that let two CTAs share an SM, else the most that fit one CTA per SM.
+inline int staged_stages(const acf_batch *b, int rows, int requested) {
+    const RoomHost &h = b->rooms[0];
+    const StagedLayout L = staged_layout(h, rows);
+    auto fits = [&](int S, size_t limit) { return L.smem(S, h.has_layer, h.pz, b->elem()) <= limit; };
+    const size_t one = (size_t)b->smem_per_block;
+    const size_t two = (size_t)b->smem_per_sm / 2 - 1024;
+    if (requested) return fits(requested, one) ? requested : 0;
+    for (int S = 4; S >= 3; S--)
+        if (fits(S, two)) return S;
+    for (int S = 4; S >= 2; S--)
+        if (fits(S, one)) return S;
+    return 0;
+}
+
+template <typename T, bool L, bool W, int NR>
+struct StagedStep {
+    static void launch(const StagedParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        const size_t smem = kStagedBarrierBytes + (size_t)p.stages * p.stage_elems * sizeof(T) +
+                            (L ? 2 * (size_t)p.f.room.pz * sizeof(T) : 0);
+        static bool opted_in = false;
+        if (!opted_in) {
+            int optin = 0, device = 0;
+            cudaGetDevice(&device);
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin);
+            opted_in = true;
+        }
+        fused_staged_sweep<T, L, W, NR><<<g, b, smem, st>>>(p);
+    }
+};
+
 // Launch one step; the fused scheme flips the room's current buffer, as the kernel will have
 // done by the time anything queued after it runs.
 template <typename T>
 void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
     if (events) cudaEventRecord(events[0], st);
-    if (b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED) {
+    if (b->fused()) {
         RoomHost &h = b->rooms[0];
         FusedParams<T> f{};
         f.room = make_room<T>(b, 0);
@@ -1621,8 +2029,25 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
         f.step_base = b->step_base;
         f.local_step = local;
         f.planes = b->planes;
-        const LaunchShape L = single_shape(b);
-        dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
+        if (b->scheme == ACF_SCHEME_FUSED_STAGED) {
+            StagedParams<T> g{};
+            g.f = f;
+            g.rows = b->staged_rows;
+            g.stages = staged_stages(b, b->staged_rows, b->staged_stages);
+            const StagedLayout lay = staged_layout(h, b->staged_rows);
+            g.stage_elems = lay.stage_elems;
+            g.off_vx = lay.off_vx;
+            g.off_vy = lay.off_vy;
+            g.off_vz = lay.off_vz;
+            g.off_psi = lay.off_psi;
+            g.error = b->error_flag();
+            const dim3 block(staged_block_x(h), b->staged_rows);
+            const dim3 grid((h.ny + b->staged_rows - 1) / b->staged_rows, (h.nx + b->planes - 1) / b->planes);
+            dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
+        } else {
+            const LaunchShape L = single_shape(b);
+            dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
+        }
         h.cur ^= 1;
         if (events) {
             cudaEventRecord(events[1], st);
@@ -1691,7 +2116,7 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
             }
             launch_step<T>(b, 0, st, b->ring + 3 * slot);
             bump_step_base<<<1, 1, 0, st>>>(b->step_base, 1);
-            b->launches += (b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED) ? 2 : 3;
+            b->launches += b->fused() ? 2 : 3;
         }
         for (int64_t t = std::max<int64_t>(0, n_steps - R); t < n_steps; t++) {
             int rc = drain(t % R);
@@ -1702,7 +2127,7 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
     }
 
     int64_t done = 0;
-    const bool fused = b->rooms.size() == 1 && b->scheme == ACF_SCHEME_FUSED;
+    const bool fused = b->fused();
     // A fused graph holds an even number of steps, so a replay leaves the buffers as it found
     // them; one graph is kept per starting buffer.
     const int64_t G = fused ? (b->graph_steps + 1) / 2 * 2 : b->graph_steps;
@@ -1977,9 +2402,11 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
         }
     }
 
-    if (cudaMalloc(&b->step_base, sizeof(int64_t)) != cudaSuccess)
+    if (cudaMalloc(&b->step_base, 2 * sizeof(int64_t)) != cudaSuccess)
         return fail(ACF_ERR_MEMORY, "cudaMalloc of step counter failed");
-    ACF_CUDA(cudaMemset(b->step_base, 0, sizeof(int64_t)));
+    ACF_CUDA(cudaMemset(b->step_base, 0, 2 * sizeof(int64_t)));
+    cudaDeviceGetAttribute(&b->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, b->device);
+    cudaDeviceGetAttribute(&b->smem_per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
     b->energy_blocks = 4 * b->sms;
     const size_t scratch = ((size_t)b->energy_blocks + 1) * kEnergyTerms * sizeof(double);
     if (cudaMalloc(&b->energy_scratch, scratch) != cudaSuccess)
@@ -2219,12 +2646,21 @@ int make_primary(acf_batch *b, cudaStream_t st) {
 
 int set_scheme(acf_batch *b, int32_t scheme) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED)
+    if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED && scheme != ACF_SCHEME_FUSED_STAGED)
         return fail(ACF_ERR_ARGUMENT, "unknown scheme %d", scheme);
-    if (scheme == ACF_SCHEME_FUSED && b->rooms.size() != 1)
-        return fail(ACF_ERR_STATE, "the fused scheme is for single rooms");
+    if (scheme != ACF_SCHEME_TWO_SWEEPS && b->rooms.size() != 1)
+        return fail(ACF_ERR_STATE, "the fused schemes are for single rooms");
+    if (scheme == ACF_SCHEME_FUSED_STAGED) {
+        const RoomHost &h = b->rooms[0];
+        if (staged_block_x(h) * b->staged_rows > 256)
+            return fail(ACF_ERR_ARGUMENT, "staged scheme: %d rows of %d threads exceed 256 threads per CTA",
+                        b->staged_rows, staged_block_x(h));
+        if (!staged_stages(b, b->staged_rows, b->staged_stages))
+            return fail(ACF_ERR_ARGUMENT, "staged scheme: %d rows x %d stages do not fit in shared memory",
+                        b->staged_rows, b->staged_stages);
+    }
     DeviceGuard guard(b->device);
-    if (scheme == ACF_SCHEME_FUSED && !b->rooms[0].second) {
+    if (scheme != ACF_SCHEME_TWO_SWEEPS && !b->rooms[0].second) {
         RoomHost &h = b->rooms[0];
         const size_t bytes = ((size_t)4 * h.field + (size_t)h.pz) * b->elem();
         if (cudaMalloc(&h.second, bytes) != cudaSuccess)
@@ -2935,6 +3371,34 @@ int64_t acf_launch_count(const acf_solver *h) { return h ? h->launches : -1; }
 int acf_set_scheme(acf_solver *h, int32_t scheme) { return set_scheme(h, scheme); }
 
 int acf_get_scheme(const acf_solver *h) { return h ? h->scheme : -1; }
+
+int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages) {
+    if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (rows < 1 || rows > 16) return fail(ACF_ERR_ARGUMENT, "rows must be in [1, 16], got %d", rows);
+    if (stages != 0 && (stages < 2 || stages > kStagedMaxStages))
+        return fail(ACF_ERR_ARGUMENT, "stages must be 0 or in [2, %d], got %d", kStagedMaxStages, stages);
+    const RoomHost &room = h->rooms[0];
+    if (staged_block_x(room) * rows > 256)
+        return fail(ACF_ERR_ARGUMENT, "%d rows of %d threads exceed 256 threads per CTA", rows,
+                    staged_block_x(room));
+    if (!staged_stages(h, rows, stages))
+        return fail(ACF_ERR_ARGUMENT, "%d rows x %d stages do not fit in shared memory", rows, stages);
+    if (rows != h->staged_rows || stages != h->staged_stages) h->graph_dirty = h->adj_graphs_dirty = true;
+    h->staged_rows = rows;
+    h->staged_stages = stages;
+    return ACF_OK;
+}
+
+int acf_device_status(acf_solver *h, int32_t *status) {
+    if (!h || !status) return fail(ACF_ERR_ARGUMENT, "null argument");
+    DeviceGuard guard(h->device);
+    ACF_CUDA(cudaDeviceSynchronize());
+    int32_t flag = 0;
+    ACF_CUDA(cudaMemcpy(&flag, h->error_flag(), sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag) ACF_CUDA(cudaMemset(h->error_flag(), 0, sizeof(flag)));
+    *status = flag;
+    return ACF_OK;
+}
 
 int acf_set_coefficients(acf_solver *h, const acf_config *config) {
     return set_coefficients(h, 0, config);

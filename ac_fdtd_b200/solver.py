@@ -388,6 +388,17 @@ class CudaAcousticFDTD:
 
     def synchronize(self) -> None:
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")
+        if self.scheme == "staged":
+            self.check_device()
+
+    def check_device(self) -> None:
+        """Raise if a staged sweep gave up waiting for its copies (the state is then invalid)."""
+        status = ctypes.c_int32(0)
+        _native.check(self._lib.acf_device_status(self._handle, ctypes.byref(status)),
+                      "acf_device_status")
+        if status.value:
+            raise RuntimeError("a staged sweep timed out waiting for its bulk copies; "
+                               "the solver state is not valid")
 
     # ------------------------------------------------------------------ diagnostics
     def energy_terms(self) -> np.ndarray:
@@ -430,12 +441,15 @@ class CudaAcousticFDTD:
         self.walls, self.absorbing_layer, self.air_absorption = walls, absorbing_layer, air_absorption
         self.coefficients = block
 
-    SCHEMES = {"two_sweeps": _native.SCHEME_TWO_SWEEPS, "fused": _native.SCHEME_FUSED}
+    SCHEMES = {"two_sweeps": _native.SCHEME_TWO_SWEEPS, "fused": _native.SCHEME_FUSED,
+               "staged": _native.SCHEME_FUSED_STAGED}
 
     def set_scheme(self, scheme: str) -> None:
-        """``"two_sweeps"`` (velocity sweep, then pressure sweep, in place) or ``"fused"`` (one
-        sweep into a second copy of p and v). Results are bit-identical; the fused step moves
-        (8 + 2R) elements per cell instead of (12 + 2R) and needs four more fields of memory."""
+        """``"two_sweeps"`` (velocity sweep, then pressure sweep, in place), ``"fused"`` (one
+        sweep into a second copy of p and v) or ``"staged"`` (the fused sweep with its inputs
+        streamed into shared memory by bulk copies). Results are bit-identical; the fused steps
+        move (8 + 2R) elements per cell instead of (12 + 2R) and need four more fields of
+        memory."""
         if scheme not in self.SCHEMES:
             raise ValueError(f"scheme must be one of {sorted(self.SCHEMES)}, got {scheme!r}")
         self._flush()
@@ -447,6 +461,15 @@ class CudaAcousticFDTD:
         """Launch geometry of the sweeps (threads per block, x planes per block)."""
         _native.check(self._lib.acf_set_launch(self._handle, int(block_threads), int(planes)),
                       "acf_set_launch")
+
+    def set_staging(self, rows: int = 2, stages: int = 0, planes: int | None = None) -> None:
+        """Geometry of the staged scheme: y rows per CTA, ring buffers (0: automatic) and, if
+        given, x planes per CTA (which also sets 128 threads per block for the other schemes)."""
+        _native.check(self._lib.acf_set_staging(self._handle, int(rows), int(stages)),
+                      "acf_set_staging")
+        if planes is not None:
+            _native.check(self._lib.acf_set_launch(self._handle, 128, int(planes)),
+                          "acf_set_launch")
 
     def launch_count(self) -> int:
         return int(self._lib.acf_launch_count(self._handle))

@@ -127,6 +127,13 @@ def ncu_traffic_per_cell(kernel: str) -> float | None:
         return None
 
 
+def launch_dict(geometry) -> dict:
+    if geometry[0] == "staged":
+        return {"scheme": "staged", "rows_per_cta": geometry[1],
+                "stages": geometry[2] or "auto", "planes_per_cta": geometry[3]}
+    return {"scheme": geometry[0], "block_threads": geometry[1], "planes_per_block": geometry[2]}
+
+
 # --------------------------------------------------------------------------- CPU baseline
 def cpu_baseline(size: int, budget_s: float = 12.0) -> dict:
     """The reference C backend on this host's cores, on a bounded sample of the workload."""
@@ -212,15 +219,15 @@ def run_ours(args) -> None:
 
     from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse, pinned_array
 
+    from ac_fdtd_b200.autotune import _apply as apply_geometry
     from ac_fdtd_b200.autotune import apply_tuned
 
     grid, objects, points = workload(args.size)
     solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
     if args.launch:
         parts = args.launch.split(",")
-        geometry = (parts[0], int(parts[1]), int(parts[2]))
-        solver.set_scheme(geometry[0])
-        solver.set_launch(*geometry[1:])
+        geometry = (parts[0], *map(int, parts[1:]))
+        apply_geometry(solver, geometry)
     else:
         geometry = apply_tuned(solver)
     solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
@@ -272,13 +279,14 @@ def run_ours(args) -> None:
                    else "fallback 6650 GB/s")
     vel_avg = vel_ms / max(timed_steps, 1)
     pres_avg = pres_ms / max(timed_steps, 1)
-    if geometry[0] == "fused":
+    if geometry[0] in ("fused", "staged"):
+        kernel = "fused_sweep" if geometry[0] == "fused" else "fused_staged_sweep"
         step_bytes = grid.n_cells * (8 + 2 * R) * itemsize
         step_avg = vel_avg + pres_avg          # one kernel; its time is in the first slot
         achieved = step_bytes / (step_avg * 1e-3) / 1e9
-        traffic_per_cell = ncu_traffic_per_cell("fused_sweep")
+        traffic_per_cell = ncu_traffic_per_cell(kernel)
         roofline = {
-            "bound": "hbm", "kernel": "fused_sweep<float,layer,walls,3>",
+            "bound": "hbm", "kernel": f"{kernel}<float,layer,walls,3>",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_source, "algorithmic_bytes_per_launch": step_bytes,
             "bytes_per_cell": (8 + 2 * R) * itemsize, "avg_launch_ms": step_avg,
@@ -340,8 +348,7 @@ def run_ours(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {**config_dict(args, grid),
-                   "launch": {"scheme": geometry[0], "block_threads": geometry[1],
-                              "planes_per_block": geometry[2],
+                   "launch": {**launch_dict(geometry),
                               "chosen_by": "--launch" if args.launch else "ac_fdtd_b200.autotune"}},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
@@ -551,9 +558,10 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--skip-extras", action="store_true",
                         help="skip the batched-room and adjoint-cost measurements")
-    parser.add_argument("--batch-steps", type=int, default=600)
+    parser.add_argument("--batch-steps", type=int, default=3000)
     parser.add_argument("--launch", default="",
-                        help="fixed sweep geometry 'threads,planes' instead of the autotuner")
+                        help="fixed geometry instead of the autotuner: 'two_sweeps|fused,threads,planes' "
+                             "or 'staged,rows,stages,planes'")
     parser.add_argument("--adjoint-steps", type=int, default=3000)
     parser.add_argument("--inversion-steps", type=int, default=2500)
     args = parser.parse_args()

@@ -132,10 +132,25 @@ int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream
 /* How a single room advances: two sweeps per step over one copy of the state, or one fused
  * sweep that reads the current p and v and writes the next ones to a second copy (4 more
  * fields of memory, (8 + 2R) instead of (12 + 2R) elements moved per cell). Both give
- * bit-identical results. The adjoint's recorded runs use the two sweeps. */
-enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1 };
+ * bit-identical results. The adjoint's recorded runs use the two sweeps.
+ * ACF_SCHEME_FUSED_STAGED is the fused sweep with each CTA's share of every x plane streamed
+ * into a shared-memory ring by bulk copies (see acf_set_staging); same memory, same results.
+ * No counterpart in the reference (its C loop runs the two sweeps, acfdtd.c:355-376). */
+enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1, ACF_SCHEME_FUSED_STAGED = 2 };
 int acf_set_scheme(acf_solver *solver, int32_t scheme);
 int acf_get_scheme(const acf_solver *solver);
+
+/* Geometry of the staged scheme: y rows per CTA (1..16, each a whole padded z row) and ring
+ * buffers per CTA (2..8; 0 picks the most that still lets two CTAs share an SM). The x planes
+ * per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the CTA would need more than 256
+ * threads or more shared memory than an SM offers; results never depend on it. No counterpart
+ * in the reference. */
+int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages);
+
+/* 0 when no kernel of this solver reported a failed wait; 1 (and the flag cleared) when a
+ * staged sweep gave up waiting for its copies, in which case the state is not valid.
+ * Synchronizes the solver's device. No counterpart in the reference. */
+int acf_device_status(acf_solver *solver, int32_t *status);
 
 /* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
 int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);

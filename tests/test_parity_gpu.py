@@ -23,7 +23,7 @@ def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-SCHEMES = ["two_sweeps", "fused"]
+SCHEMES = ["two_sweeps", "fused", "staged"]
 
 
 def paired(dtype=np.float64, steps_per_graph=64, scheme="two_sweeps", **configuration):
@@ -161,11 +161,12 @@ def test_plain_room_matches_the_reference(golden_meta, golden_rooms):
     assert digest(solver.p) == golden_meta["rooms"]["plain/numpy/p"]
 
 
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_walls_sponge_air_room_matches_the_reference(dtype, golden_meta, golden_rooms):
+def test_walls_sponge_air_room_matches_the_reference(dtype, scheme, golden_meta, golden_rooms):
     meta = golden_meta["rooms"]["full"]
     grid, objects = full_room(meta)
-    solver = CudaAcousticFDTD(grid, dtype=dtype, **objects)
+    solver = CudaAcousticFDTD(grid, dtype=dtype, scheme=scheme, **objects)
     solver.add_volume_source(meta["points"][0], gaussian_pulse(meta["steps"], solver.dt, 4000.0))
     for point in meta["points"][1:]:
         solver.add_pressure_receiver(point)
@@ -210,8 +211,8 @@ def test_switching_schemes_mid_run_and_odd_step_counts():
     energy, state access and graph replays from either copy must all see the current state."""
     configuration = CONFIGURATIONS["everything at once"]
     oracle, cuda = paired(steps_per_graph=8, scheme="fused", **configuration)
-    plan = [("fused", 9), ("fused", 17), ("two_sweeps", 5), ("fused", 3), ("fused", 16),
-            ("two_sweeps", 8), ("fused", 1)]
+    plan = [("fused", 9), ("fused", 17), ("two_sweeps", 5), ("fused", 3), ("staged", 16),
+            ("two_sweeps", 8), ("fused", 1), ("staged", 7), ("fused", 2), ("staged", 1)]
     total = 0
     for scheme, n in plan:
         cuda.set_scheme(scheme)
@@ -222,3 +223,34 @@ def test_switching_schemes_mid_run_and_odd_step_counts():
         np.testing.assert_array_equal(cuda.p, oracle.p)
     assert_same_state(cuda, oracle)
     assert cuda.step_index == total
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_staged_geometries_match_the_oracle(dtype):
+    """Rows per CTA, ring depth and planes per CTA change only which CTA computes a cell and
+    when its inputs arrive; every geometry must give the oracle's bits, on grids whose rows and
+    planes do not divide evenly, and no wait may run out."""
+    from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid
+
+    configuration = dict(walls=WallAdmittances(0.4, 0.1, 0.0, 0.7, 0.2, 0.05),
+                         absorbing_layer=AbsorbingLayer(thickness=3),
+                         air_absorption=AirAbsorption())
+    for shape in ((13, 11, 23), (6, 1, 5), (1, 7, 3), (9, 10, 40)):
+        grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
+        initial = np.random.default_rng(sum(shape)).standard_normal(shape)
+        receiver = tuple((n - 0.5) * 0.02 for n in shape)
+        oracle = OracleFDTD(grid, AIR, dtype=dtype, **configuration)
+        oracle.p[:] = initial
+        oracle.add_volume_source((0.01, 0.01, 0.01), np.hanning(9))
+        oracle.add_pressure_receiver(receiver)
+        oracle.run(21)
+        for rows, stages, planes in ((1, 2, 1), (2, 0, 3), (3, 3, 4), (4, 4, 64), (2, 8, 5)):
+            cuda = CudaAcousticFDTD(grid, dtype=dtype, steps_per_graph=6, **configuration)
+            cuda.set_staging(rows, stages, planes)
+            cuda.set_scheme("staged")
+            cuda.p[:] = initial
+            cuda.add_volume_source((0.01, 0.01, 0.01), np.hanning(9))
+            cuda.add_pressure_receiver(receiver)
+            cuda.run(21)
+            cuda.check_device()
+            assert_same_state(cuda, oracle)

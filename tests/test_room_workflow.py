@@ -70,7 +70,7 @@ def test_workflow_with_the_oracle_solver_reproduces_the_reference(impulse):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("scheme", ["two_sweeps", "fused"])
+@pytest.mark.parametrize("scheme", ["two_sweeps", "fused", "staged"])
 def test_workflow_on_the_gpu_reproduces_the_reference_bitwise(impulse, scheme):
     data = _golden_impulse()
     ir = simulate_impulse_response(make_room(impulse), tuple(impulse["source"]),
