@@ -127,7 +127,7 @@ _SIGNATURES = {
     "acf_reset_state": (ctypes.c_int, [_P, _P]),
     "acf_set_scheme": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_get_scheme": (ctypes.c_int, [_P]),
-    "acf_set_staging": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "acf_set_staging": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "acf_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "acf_batch_adjoint_prepare": (ctypes.c_int, [_P, _I64]),
     "acf_batch_adjoint_shell_size": (ctypes.c_int64, [_P, ctypes.c_int32]),

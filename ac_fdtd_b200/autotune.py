@@ -28,8 +28,10 @@ BATCH_CANDIDATES = ((128, 8, 0), (256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8,
 _cache: dict[str, tuple[int, int]] = {}
 
 
-#: (rows per CTA, ring buffers (0: automatic), planes per CTA) tried for the staged scheme.
-STAGED_CANDIDATES = ((2, 0, 8), (2, 0, 16), (2, 0, 32), (1, 0, 16), (2, 3, 16), (4, 0, 16))
+#: (rows per CTA, ring buffers (0: automatic), planes per CTA, z elements per thread) tried
+#: for the staged scheme.
+STAGED_CANDIDATES = ((1, 3, 16, 2), (1, 4, 16, 2), (1, 3, 32, 2), (1, 3, 8, 2), (2, 3, 16, 4),
+                     (1, 2, 16, 2))
 
 #: Schemes raced by default; all give bit-identical results.
 SCHEMES = ("staged", "fused", "two_sweeps")
@@ -39,8 +41,8 @@ def _apply(solver, candidate) -> None:
     """Put ``solver`` on ``candidate`` = (scheme, *geometry); RuntimeError if it cannot run."""
     scheme, *geometry = candidate
     if scheme == "staged":
-        rows, stages, planes = geometry
-        solver.set_staging(rows, stages, planes)
+        rows, stages, planes, vector = geometry
+        solver.set_staging(rows, stages, planes, vector)
     else:
         solver.set_launch(*geometry)
     solver.set_scheme(scheme)
@@ -80,8 +82,8 @@ def _store_file(key: str, value) -> None:
 
 def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schemes=SCHEMES,
          staged_candidates=STAGED_CANDIDATES):
-    """Time each (scheme, threads, planes) -- (scheme, rows, stages, planes) for the staged
-    scheme -- on a scratch twin of ``solver``; return (best, {candidate: ms/step})."""
+    """Time each (scheme, threads, planes) -- (scheme, rows, stages, planes, vector) for the
+    staged scheme -- on a scratch twin of ``solver``; return (best, {candidate: ms/step})."""
     from .solver import CudaAcousticFDTD
 
     twin = CudaAcousticFDTD(solver.grid, solver.medium, solver.courant, solver.dtype,
@@ -113,7 +115,7 @@ def tune(solver, candidates=CANDIDATES, steps: int = 12, repeats: int = 2, schem
 def apply_tuned(solver, candidates=CANDIDATES, schemes=SCHEMES,
                 staged_candidates=STAGED_CANDIDATES):
     """Set the fastest scheme and geometry for this configuration (tuned once per shape
-    class); returns (scheme, threads, planes) or ("staged", rows, stages, planes)."""
+    class); returns (scheme, threads, planes) or ("staged", rows, stages, planes, vector)."""
     key = _key(solver)
     if key not in _cache:
         stored = _load_file().get(key)

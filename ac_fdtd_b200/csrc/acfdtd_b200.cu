@@ -646,8 +646,11 @@ __global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(T, LAYER, NR)) fused
 // copies of a plane into a ring of `stages` buffers, each completing its own mbarrier; every
 // thread computes plane i from buffers i and i+1 (p and vx of the next plane) while the next
 // stages-2 planes are already in flight, so the bytes in flight no longer depend on how many
-// registers the arithmetic needs. The arithmetic is fused_column's, element for element, so the
-// results are identical to the two-sweep and fused schemes.
+// registers the arithmetic needs. A thread owns VW = 2 or 4 consecutive z elements of one row:
+// shared memory per thread is what bounds the warps an SM holds (the ring takes about 70 bytes
+// per thread and stage at VW = 2), so the narrower vector keeps twice as many warps resident
+// to hide the arithmetic's latency. The arithmetic is fused_column's, element for element, so
+// the results are identical to the two-sweep and fused schemes.
 //
 // Every wait is bounded (about two seconds). A CTA whose wait runs out raises the room's error
 // flag, waits (bounded again) for the copies it has issued and returns; the host reports the
@@ -661,7 +664,7 @@ constexpr int kWaitLimitIterations = 1 << 21;
 template <typename T>
 struct StagedParams {
     FusedParams<T> f;
-    int32_t rows, stages;
+    int32_t rows, stages, vector;   // vector: z elements per thread, 2 or 4
     int64_t stage_elems;            // elements of one ring buffer
     int64_t off_vx, off_vy, off_vz, off_psi;
     int32_t *error;                 // set to 1 when a wait ran out
@@ -734,8 +737,50 @@ __device__ __forceinline__ void lds4(const T *a, T v[4]) {
     }
 }
 
-template <typename T, bool LAYER, bool WALLS, int NR>
-__global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<T> g) {
+// W consecutive elements (W = 2 or 4) of global or shared memory: one 8- or 16-byte access
+// for float, one or two 16-byte accesses for double.
+template <typename T, int W>
+struct VecW;
+
+template <typename T>
+struct VecW<T, 4> {
+    __device__ __forceinline__ static void ldg(const T *__restrict__ a, T v[4]) { Vec4<T>::ldg(a, v); }
+    __device__ __forceinline__ static void store(T *__restrict__ a, const T v[4]) { Vec4<T>::store(a, v); }
+    __device__ __forceinline__ static void lds(const T *a, T v[4]) { lds4<T>(a, v); }
+};
+
+template <>
+struct VecW<float, 2> {
+    __device__ __forceinline__ static void ldg(const float *__restrict__ a, float v[2]) {
+        const float2 t = __ldg(reinterpret_cast<const float2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void store(float *__restrict__ a, const float v[2]) {
+        *reinterpret_cast<float2 *>(a) = make_float2(v[0], v[1]);
+    }
+    __device__ __forceinline__ static void lds(const float *a, float v[2]) {
+        const float2 t = *reinterpret_cast<const float2 *>(a);
+        v[0] = t.x; v[1] = t.y;
+    }
+};
+
+template <>
+struct VecW<double, 2> {
+    __device__ __forceinline__ static void ldg(const double *__restrict__ a, double v[2]) {
+        const double2 t = __ldg(reinterpret_cast<const double2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void store(double *__restrict__ a, const double v[2]) {
+        *reinterpret_cast<double2 *>(a) = make_double2(v[0], v[1]);
+    }
+    __device__ __forceinline__ static void lds(const double *a, double v[2]) {
+        const double2 t = *reinterpret_cast<const double2 *>(a);
+        v[0] = t.x; v[1] = t.y;
+    }
+};
+
+template <typename T, bool LAYER, bool WALLS, int NR, int VW>
+__global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const StagedParams<T> g) {
     extern __shared__ __align__(128) unsigned char smem[];
     const FusedParams<T> &f = g.f;
     const Room<T> &s = f.room;
@@ -801,16 +846,16 @@ __global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<
     const int c = threadIdx.x;
     const int ry = threadIdx.y;
     const int j = j0 + ry;
-    const bool active = c < s.nchunks && j < s.ny;
-    const int k0 = c * kVec;
+    const bool active = c < (s.nz + VW - 1) / VW && j < s.ny;
+    const int k0 = c * VW;
     const T cv = s.cv, cp = s.cp;
     const bool any_point = (s.n_src | s.n_rec) != 0;
     const int64_t step = any_point ? (*f.step_base + f.local_step) : 0;
     const int64_t column = (int64_t)j * s.pz + k0;
-    const bool has_above = k0 + kVec < s.nz;
+    const bool has_above = k0 + VW < s.nz;
 
     T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
-    T XL[kVec];
+    T XL[VW];
     if (active) {
         if (LAYER) {
             fj_cell = __ldg(s.cell[1] + j);
@@ -819,13 +864,13 @@ __global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<
         }
         // The updated vx on face i_begin, as fused_column starts its march.
         const int64_t base = (int64_t)i_begin * s.plane + column;
-        T P0[kVec], V[kVec], Q[kVec];
-        Vec4<T>::ldg(s.p + base, P0);
-        Vec4<T>::ldg(s.vx + base, V);
-        if (i_begin > 0) Vec4<T>::ldg(s.p + base - s.plane, Q);
+        T P0[VW], V[VW], Q[VW];
+        VecW<T, VW>::ldg(s.p + base, P0);
+        VecW<T, VW>::ldg(s.vx + base, V);
+        if (i_begin > 0) VecW<T, VW>::ldg(s.p + base - s.plane, Q);
         const T fi_face = LAYER ? __ldg(s.face[0] + i_begin) : T(1);
 #pragma unroll
-        for (int e = 0; e < kVec; e++) {
+        for (int e = 0; e < VW; e++) {
             T v = V[e];
             if (i_begin > 0) v = v - cv * (P0[e] - Q[e]);
             XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell, LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1));
@@ -847,31 +892,31 @@ __global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<
             const T *prow = cur + (int64_t)(ry + 1) * s.pz + k0;
             const T *vyrow = cur + g.off_vy + (int64_t)ry * s.pz + k0;
             const T *vzrow = cur + g.off_vz + (int64_t)ry * s.pz + k0;
-            T P[kVec], PX[kVec], VXo[kVec], PYm[kVec], PYp[kVec], VY[kVec], VYp[kVec], VZ[kVec];
-            T Sg[NR > 0 ? NR : 1][kVec];
-            lds4<T>(prow, P);
-            if (x_inner) lds4<T>(nxt + (int64_t)(ry + 1) * s.pz + k0, PX);
-            lds4<T>(nxt + g.off_vx + (int64_t)ry * s.pz + k0, VXo);
-            if (j > 0) lds4<T>(prow - s.pz, PYm);
-            if (j + 1 < s.ny) lds4<T>(prow + s.pz, PYp);
-            lds4<T>(vyrow, VY);
-            lds4<T>(vyrow + s.pz, VYp);
-            lds4<T>(vzrow, VZ);
+            T P[VW], PX[VW], VXo[VW], PYm[VW], PYp[VW], VY[VW], VYp[VW], VZ[VW];
+            T Sg[NR > 0 ? NR : 1][VW];
+            VecW<T, VW>::lds(prow, P);
+            if (x_inner) VecW<T, VW>::lds(nxt + (int64_t)(ry + 1) * s.pz + k0, PX);
+            VecW<T, VW>::lds(nxt + g.off_vx + (int64_t)ry * s.pz + k0, VXo);
+            if (j > 0) VecW<T, VW>::lds(prow - s.pz, PYm);
+            if (j + 1 < s.ny) VecW<T, VW>::lds(prow + s.pz, PYp);
+            VecW<T, VW>::lds(vyrow, VY);
+            VecW<T, VW>::lds(vyrow + s.pz, VYp);
+            VecW<T, VW>::lds(vzrow, VZ);
             const T p_below = k0 > 0 ? prow[-1] : T(0);
-            const T p_above = has_above ? prow[kVec] : T(0);
-            const T vz_above = k0 + kVec <= s.nz ? vzrow[kVec] : T(0);
+            const T p_above = has_above ? prow[VW] : T(0);
+            const T vz_above = k0 + VW <= s.nz ? vzrow[VW] : T(0);
 #pragma unroll
             for (int r = 0; r < NR; r++)
-                lds4<T>(cur + g.off_psi + ((int64_t)r * g.rows + ry) * s.pz + k0, Sg[r]);
+                VecW<T, VW>::lds(cur + g.off_psi + ((int64_t)r * g.rows + ry) * s.pz + k0, Sg[r]);
             T fi_cell = T(1), fi1_face = T(1);
             if (LAYER) {
                 fi_cell = __ldg(s.cell[0] + i);
                 fi1_face = __ldg(s.face[0] + i + 1);
             }
 
-            T XH[kVec], YL[kVec], YH[kVec], ZL[kVec];
+            T XH[VW], YL[VW], YH[VW], ZL[VW];
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
+            for (int e = 0; e < VW; e++) {
                 const T fkc = LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1);
                 T v = VXo[e];
                 if (x_inner) v = v - cv * (PX[e] - P[e]);
@@ -888,16 +933,16 @@ __global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<
                 ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, LAYER ? zface[min(k0 + e, s.nz)] : T(1));
             }
             T ZH3 = vz_above;
-            if (has_above) ZH3 = ZH3 - cv * (p_above - P[kVec - 1]);
-            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, LAYER ? zface[min(k0 + kVec, s.nz)] : T(1));
+            if (has_above) ZH3 = ZH3 - cv * (p_above - P[VW - 1]);
+            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, LAYER ? zface[min(k0 + VW, s.nz)] : T(1));
 
-            T Pn[kVec];
+            T Pn[VW];
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
+            for (int e = 0; e < VW; e++) {
                 const int k = k0 + e;
                 T pe = P[e];
                 if (k < s.nz) {
-                    const T zh = e + 1 < kVec ? ZL[e + 1] : ZH3;
+                    const T zh = e + 1 < VW ? ZL[e + 1] : ZH3;
                     T d = XH[e] - XL[e];
                     d = d + (YH[e] - YL[e]);
                     d = d + (zh - ZL[e]);
@@ -925,41 +970,41 @@ __global__ void __launch_bounds__(256, 2) fused_staged_sweep(const StagedParams<
             if (any_point) {
                 for (int q = 0; q < s.n_src; q++) {
                     const int64_t d = s.src_off[q] - base;
-                    if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
+                    if (d >= 0 && d < VW && k0 + d < s.nz && step < s.src_len[q]) {
 #pragma unroll
-                        for (int e = 0; e < kVec; e++)
+                        for (int e = 0; e < VW; e++)
                             if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
                     }
                 }
             }
 
-            T ZS[kVec];
+            T ZS[VW];
 #pragma unroll
-            for (int e = 0; e < kVec; e++) ZS[e] = k0 + e <= s.nz ? ZL[e] : VZ[e];
-            Vec4<T>::store(f.np + base, Pn);
-            Vec4<T>::store(f.nvx + base, XL);
-            Vec4<T>::store(f.nvy + base, YL);
-            Vec4<T>::store(f.nvz + base, ZS);
-            if (i == s.nx - 1) Vec4<T>::store(f.nvx + base + s.plane, XH);
-            if (j == s.ny - 1) Vec4<T>::store(f.nvy + base + s.pz, YH);
-            if (k0 + kVec == s.nz) f.nvz[base + kVec] = ZH3;
+            for (int e = 0; e < VW; e++) ZS[e] = k0 + e <= s.nz ? ZL[e] : VZ[e];
+            VecW<T, VW>::store(f.np + base, Pn);
+            VecW<T, VW>::store(f.nvx + base, XL);
+            VecW<T, VW>::store(f.nvy + base, YL);
+            VecW<T, VW>::store(f.nvz + base, ZS);
+            if (i == s.nx - 1) VecW<T, VW>::store(f.nvx + base + s.plane, XH);
+            if (j == s.ny - 1) VecW<T, VW>::store(f.nvy + base + s.pz, YH);
+            if (k0 + VW == s.nz) f.nvz[base + VW] = ZH3;
 #pragma unroll
-            for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, Sg[r]);
+            for (int r = 0; r < NR; r++) VecW<T, VW>::store(s.psi + r * s.field + base, Sg[r]);
 
             if (any_point) {
                 for (int r = 0; r < s.n_rec; r++) {
                     const int64_t d = s.rec_off[r] - base;
-                    if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                    if (d >= 0 && d < VW && step >= s.rec_start[r]) {
                         T v = Pn[0];
 #pragma unroll
-                        for (int e = 1; e < kVec; e++)
+                        for (int e = 1; e < VW; e++)
                             if (e == d) v = Pn[e];
                         s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
                     }
                 }
             }
 #pragma unroll
-            for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+            for (int e = 0; e < VW; e++) XL[e] = XH[e];
         }
         // Every thread is done with buffer `slot` (plane i); refill it with plane i + S.
         if (__syncthreads_or(!ready)) {
@@ -1717,8 +1762,9 @@ struct acf_batch {
     int block_threads = 256;
     int planes = 4;
     int ctas_per_sm = 4;
-    int staged_rows = 2;             // staged scheme: y rows per CTA
+    int staged_rows = 1;             // staged scheme: y rows per CTA
     int staged_stages = 0;           // staged scheme: ring buffers per CTA (0: automatic)
+    int staged_vector = 2;           // staged scheme: z elements per thread (2 or 4)
     int smem_per_sm = 233472, smem_per_block = 232448;
 
     // graphs (index: parity of the fused scheme's current buffer at the start of a replay)
@@ -1977,21 +2023,19 @@ inline StagedLayout staged_layout(const RoomHost &h, int rows) {
     return L;
 }
 
-inline int staged_block_x(const RoomHost &h) { return (int)round_up((h.nz + kVec - 1) / kVec, 32); }
+inline int staged_block_x(const RoomHost &h, int vector) {
+    return (int)round_up((h.nz + vector - 1) / vector, 32);
+}
 
-// Ring buffers for (rows, requested): the request if it fits, else 0; for 0, the most (<= 4)
-// that let two CTAs share an SM, else the most that fit one CTA per SM.
+// Ring buffers for (rows, requested): the request if it fits one CTA's shared memory, else 0;
+// for 0, three (one plane in flight beyond the two being read) or, if three do not fit, two.
 inline int staged_stages(const acf_batch *b, int rows, int requested) {
     const RoomHost &h = b->rooms[0];
     const StagedLayout L = staged_layout(h, rows);
-    auto fits = [&](int S, size_t limit) { return L.smem(S, h.has_layer, h.pz, b->elem()) <= limit; };
-    const size_t one = (size_t)b->smem_per_block;
-    const size_t two = (size_t)b->smem_per_sm / 2 - 1024;
-    if (requested) return fits(requested, one) ? requested : 0;
-    for (int S = 4; S >= 3; S--)
-        if (fits(S, two)) return S;
-    for (int S = 4; S >= 2; S--)
-        if (fits(S, one)) return S;
+    auto fits = [&](int S) { return L.smem(S, h.has_layer, h.pz, b->elem()) <= (size_t)b->smem_per_block; };
+    if (requested) return fits(requested) ? requested : 0;
+    for (int S = 3; S >= 2; S--)
+        if (fits(S)) return S;
     return 0;
 }
 
@@ -2005,11 +2049,14 @@ struct StagedStep {
             int optin = 0, device = 0;
             cudaGetDevice(&device);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 optin);
+            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  optin);
             opted_in = true;
         }
-        fused_staged_sweep<T, L, W, NR><<<g, b, smem, st>>>(p);
+        if (p.vector == 2) fused_staged_sweep<T, L, W, NR, 2><<<g, b, smem, st>>>(p);
+        else fused_staged_sweep<T, L, W, NR, 4><<<g, b, smem, st>>>(p);
     }
 };
 
@@ -2034,6 +2081,7 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
             g.f = f;
             g.rows = b->staged_rows;
             g.stages = staged_stages(b, b->staged_rows, b->staged_stages);
+            g.vector = b->staged_vector;
             const StagedLayout lay = staged_layout(h, b->staged_rows);
             g.stage_elems = lay.stage_elems;
             g.off_vx = lay.off_vx;
@@ -2041,7 +2089,7 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
             g.off_vz = lay.off_vz;
             g.off_psi = lay.off_psi;
             g.error = b->error_flag();
-            const dim3 block(staged_block_x(h), b->staged_rows);
+            const dim3 block(staged_block_x(h, b->staged_vector), b->staged_rows);
             const dim3 grid((h.ny + b->staged_rows - 1) / b->staged_rows, (h.nx + b->planes - 1) / b->planes);
             dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
         } else {
@@ -2652,9 +2700,9 @@ int set_scheme(acf_batch *b, int32_t scheme) {
         return fail(ACF_ERR_STATE, "the fused schemes are for single rooms");
     if (scheme == ACF_SCHEME_FUSED_STAGED) {
         const RoomHost &h = b->rooms[0];
-        if (staged_block_x(h) * b->staged_rows > 256)
+        if (staged_block_x(h, b->staged_vector) * b->staged_rows > 256)
             return fail(ACF_ERR_ARGUMENT, "staged scheme: %d rows of %d threads exceed 256 threads per CTA",
-                        b->staged_rows, staged_block_x(h));
+                        b->staged_rows, staged_block_x(h, b->staged_vector));
         if (!staged_stages(b, b->staged_rows, b->staged_stages))
             return fail(ACF_ERR_ARGUMENT, "staged scheme: %d rows x %d stages do not fit in shared memory",
                         b->staged_rows, b->staged_stages);
@@ -3372,20 +3420,23 @@ int acf_set_scheme(acf_solver *h, int32_t scheme) { return set_scheme(h, scheme)
 
 int acf_get_scheme(const acf_solver *h) { return h ? h->scheme : -1; }
 
-int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages) {
+int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages, int32_t vector) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
     if (rows < 1 || rows > 16) return fail(ACF_ERR_ARGUMENT, "rows must be in [1, 16], got %d", rows);
     if (stages != 0 && (stages < 2 || stages > kStagedMaxStages))
         return fail(ACF_ERR_ARGUMENT, "stages must be 0 or in [2, %d], got %d", kStagedMaxStages, stages);
+    if (vector != 2 && vector != 4) return fail(ACF_ERR_ARGUMENT, "vector must be 2 or 4, got %d", vector);
     const RoomHost &room = h->rooms[0];
-    if (staged_block_x(room) * rows > 256)
+    if (staged_block_x(room, vector) * rows > 256)
         return fail(ACF_ERR_ARGUMENT, "%d rows of %d threads exceed 256 threads per CTA", rows,
-                    staged_block_x(room));
+                    staged_block_x(room, vector));
     if (!staged_stages(h, rows, stages))
         return fail(ACF_ERR_ARGUMENT, "%d rows x %d stages do not fit in shared memory", rows, stages);
-    if (rows != h->staged_rows || stages != h->staged_stages) h->graph_dirty = h->adj_graphs_dirty = true;
+    if (rows != h->staged_rows || stages != h->staged_stages || vector != h->staged_vector)
+        h->graph_dirty = h->adj_graphs_dirty = true;
     h->staged_rows = rows;
     h->staged_stages = stages;
+    h->staged_vector = vector;
     return ACF_OK;
 }
 

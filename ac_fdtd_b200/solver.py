@@ -462,10 +462,12 @@ class CudaAcousticFDTD:
         _native.check(self._lib.acf_set_launch(self._handle, int(block_threads), int(planes)),
                       "acf_set_launch")
 
-    def set_staging(self, rows: int = 2, stages: int = 0, planes: int | None = None) -> None:
-        """Geometry of the staged scheme: y rows per CTA, ring buffers (0: automatic) and, if
-        given, x planes per CTA (which also sets 128 threads per block for the other schemes)."""
-        _native.check(self._lib.acf_set_staging(self._handle, int(rows), int(stages)),
+    def set_staging(self, rows: int = 1, stages: int = 0, planes: int | None = None,
+                    vector: int = 2) -> None:
+        """Geometry of the staged scheme: y rows per CTA, ring buffers (0: automatic), z
+        elements per thread (2 or 4) and, if given, x planes per CTA (which also sets 128
+        threads per block for the other schemes)."""
+        _native.check(self._lib.acf_set_staging(self._handle, int(rows), int(stages), int(vector)),
                       "acf_set_staging")
         if planes is not None:
             _native.check(self._lib.acf_set_launch(self._handle, 128, int(planes)),

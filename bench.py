@@ -129,8 +129,8 @@ def ncu_traffic_per_cell(kernel: str) -> float | None:
 
 def launch_dict(geometry) -> dict:
     if geometry[0] == "staged":
-        return {"scheme": "staged", "rows_per_cta": geometry[1],
-                "stages": geometry[2] or "auto", "planes_per_cta": geometry[3]}
+        return {"scheme": "staged", "rows_per_cta": geometry[1], "stages": geometry[2] or "auto",
+                "planes_per_cta": geometry[3], "z_elements_per_thread": geometry[4]}
     return {"scheme": geometry[0], "block_threads": geometry[1], "planes_per_block": geometry[2]}
 
 
@@ -561,7 +561,7 @@ def main() -> None:
     parser.add_argument("--batch-steps", type=int, default=3000)
     parser.add_argument("--launch", default="",
                         help="fixed geometry instead of the autotuner: 'two_sweeps|fused,threads,planes' "
-                             "or 'staged,rows,stages,planes'")
+                             "or 'staged,rows,stages,planes,vector'")
     parser.add_argument("--adjoint-steps", type=int, default=3000)
     parser.add_argument("--inversion-steps", type=int, default=2500)
     args = parser.parse_args()

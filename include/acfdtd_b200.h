@@ -140,12 +140,13 @@ enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1, ACF_SCHEME_FUSED_STAGED 
 int acf_set_scheme(acf_solver *solver, int32_t scheme);
 int acf_get_scheme(const acf_solver *solver);
 
-/* Geometry of the staged scheme: y rows per CTA (1..16, each a whole padded z row) and ring
- * buffers per CTA (2..8; 0 picks the most that still lets two CTAs share an SM). The x planes
- * per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the CTA would need more than 256
- * threads or more shared memory than an SM offers; results never depend on it. No counterpart
- * in the reference. */
-int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages);
+/* Geometry of the staged scheme: y rows per CTA (1..16, each a whole padded z row), ring
+ * buffers per CTA (2..8; 0 picks three, or two where three do not fit) and z elements per
+ * thread (2 or 4). The x planes per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the
+ * CTA would need more than 256 threads or more shared memory than an SM offers; results never
+ * depend on it. Default: 1 row, automatic stages, 2 elements. No counterpart in the
+ * reference. */
+int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages, int32_t vector);
 
 /* 0 when no kernel of this solver reported a failed wait; 1 (and the flag cleared) when a
  * staged sweep gave up waiting for its copies, in which case the state is not valid.

@@ -244,9 +244,10 @@ def test_staged_geometries_match_the_oracle(dtype):
         oracle.add_volume_source((0.01, 0.01, 0.01), np.hanning(9))
         oracle.add_pressure_receiver(receiver)
         oracle.run(21)
-        for rows, stages, planes in ((1, 2, 1), (2, 0, 3), (3, 3, 4), (4, 4, 64), (2, 8, 5)):
+        for rows, stages, planes, vector in ((1, 2, 1, 2), (2, 0, 3, 4), (3, 3, 4, 2),
+                                             (4, 4, 64, 4), (2, 8, 5, 2), (1, 0, 7, 4)):
             cuda = CudaAcousticFDTD(grid, dtype=dtype, steps_per_graph=6, **configuration)
-            cuda.set_staging(rows, stages, planes)
+            cuda.set_staging(rows, stages, planes, vector)
             cuda.set_scheme("staged")
             cuda.p[:] = initial
             cuda.add_volume_source((0.01, 0.01, 0.01), np.hanning(9))
