@@ -779,18 +779,33 @@ struct VecW<double, 2> {
     }
 };
 
+// Sources and receivers inside one CTA's tile, gathered once per launch so that the march
+// does not scan every point at every plane. Sorted by index: sources (q < n_src) come first, in
+// the order they were added, so several sources in one cell add up in the reference's order and
+// receivers read the finished pressure.
+constexpr int kStagedPointCap = 32;
+
+struct TilePoint {
+    int32_t q;      // source index, or n_src + receiver index
+    int32_t i;      // x plane
+    int32_t row;    // y row within the tile
+    int32_t k;      // z index
+};
+
 template <typename T, bool LAYER, bool WALLS, int NR, int VW>
-__global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const StagedParams<T> g) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? (VW == 2 ? 2 : 1) : (VW == 2 ? 3 : 2))
+fused_staged_sweep(const StagedParams<T> g) {
     extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ TilePoint points[kStagedPointCap];
+    __shared__ int n_points;
     const FusedParams<T> &f = g.f;
     const Room<T> &s = f.room;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     T *ring = reinterpret_cast<T *>(smem + kStagedBarrierBytes);
-    T *zcell = ring + (int64_t)g.stages * g.stage_elems;   // LAYER: cell[2], then face[2]
-    T *zface = zcell + s.pz;
 
     const int S = g.stages;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nthreads = blockDim.x * blockDim.y;
     const int j0 = blockIdx.x * g.rows;
     const int i_begin = blockIdx.y * f.planes;
     const int i_end = min(s.nx, i_begin + f.planes);
@@ -828,13 +843,7 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
     if (tid == 0) {
         for (int q = 0; q < S; q++) mbar_init(full + q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (LAYER) {
-        const int nthreads = blockDim.x * blockDim.y;
-        for (int k = tid; k <= s.nz; k += nthreads) {
-            zcell[k] = __ldg(s.cell[2] + min(k, s.nz - 1));
-            zface[k] = __ldg(s.face[2] + k);
-        }
+        n_points = 0;
     }
     __syncthreads();
     int issued = i_begin - 1;   // last plane issued (thread 0)
@@ -843,24 +852,66 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
         issued = min(i_begin + S - 1, i_end);
     }
 
+    // Points of this tile (while the first planes are in flight).
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    if (any_point) {
+        const int total = s.n_src + s.n_rec;
+        for (int q = tid; q < total; q += nthreads) {
+            const int64_t off = q < s.n_src ? s.src_off[q] : s.rec_off[q - s.n_src];
+            const int pi = (int)(off / s.plane);
+            const int64_t rem = off - (int64_t)pi * s.plane;
+            const int pj = (int)(rem / s.pz);
+            const int pk = (int)(rem - (int64_t)pj * s.pz);
+            if (pi >= i_begin && pi < i_end && pj >= j0 && pj < j0 + n_own) {
+                const int at = atomicAdd(&n_points, 1);
+                if (at < kStagedPointCap) points[at] = TilePoint{q, pi, pj - j0, pk};
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && n_points > 1 && n_points <= kStagedPointCap) {
+            for (int a = 1; a < n_points; a++) {
+                const TilePoint key = points[a];
+                int b = a - 1;
+                while (b >= 0 && points[b].q > key.q) {
+                    points[b + 1] = points[b];
+                    b--;
+                }
+                points[b + 1] = key;
+            }
+        }
+        __syncthreads();
+    }
+    const int np = any_point ? n_points : 0;
+    const bool overflow = np > kStagedPointCap;   // too many: scan every point, as fused_column
+
     const int c = threadIdx.x;
     const int ry = threadIdx.y;
     const int j = j0 + ry;
     const bool active = c < (s.nz + VW - 1) / VW && j < s.ny;
     const int k0 = c * VW;
     const T cv = s.cv, cp = s.cp;
-    const bool any_point = (s.n_src | s.n_rec) != 0;
     const int64_t step = any_point ? (*f.step_base + f.local_step) : 0;
     const int64_t column = (int64_t)j * s.pz + k0;
     const bool has_above = k0 + VW < s.nz;
+    const bool wall_k = k0 == 0 || k0 + VW >= s.nz;   // the chunk holds k = 0 or k = nz - 1
 
+    // Damping profiles along y and z are fixed for the thread's whole march.
     T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
+    T fkc[VW], fkf[VW + 1];
+#pragma unroll
+    for (int e = 0; e < VW; e++) fkc[e] = T(1);
+#pragma unroll
+    for (int e = 0; e <= VW; e++) fkf[e] = T(1);
     T XL[VW];
     if (active) {
         if (LAYER) {
             fj_cell = __ldg(s.cell[1] + j);
             fj_face = __ldg(s.face[1] + j);
             fj1_face = __ldg(s.face[1] + j + 1);
+#pragma unroll
+            for (int e = 0; e < VW; e++) fkc[e] = __ldg(s.cell[2] + min(k0 + e, s.nz - 1));
+#pragma unroll
+            for (int e = 0; e <= VW; e++) fkf[e] = __ldg(s.face[2] + min(k0 + e, s.nz));
         }
         // The updated vx on face i_begin, as fused_column starts its march.
         const int64_t base = (int64_t)i_begin * s.plane + column;
@@ -873,7 +924,7 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
         for (int e = 0; e < VW; e++) {
             T v = V[e];
             if (i_begin > 0) v = v - cv * (P0[e] - Q[e]);
-            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell, LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1));
+            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell, fkc[e]);
         }
     }
 
@@ -882,8 +933,9 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
     for (; i < i_end; i++) {
         const int u = i - i_begin;
         const int slot = u % S, nslot = (u + 1) % S;
-        const bool ready = mbar_wait(full + slot, (uint32_t)(u / S) & 1u) &&
-                           mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u);
+        // Buffer `slot` (plane i) was already waited for as the next plane, except at the start.
+        bool ready = u > 0 || mbar_wait(full + slot, 0u);
+        ready = ready && mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u);
         if (ready && active) {
             const T *cur = ring + (int64_t)slot * g.stage_elems;
             const T *nxt = ring + (int64_t)nslot * g.stage_elems;
@@ -917,25 +969,25 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
             T XH[VW], YL[VW], YH[VW], ZL[VW];
 #pragma unroll
             for (int e = 0; e < VW; e++) {
-                const T fkc = LAYER ? zcell[min(k0 + e, s.nz - 1)] : T(1);
                 T v = VXo[e];
                 if (x_inner) v = v - cv * (PX[e] - P[e]);
-                XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc);
+                XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc[e]);
                 v = VY[e];
                 if (j > 0) v = v - cv * (P[e] - PYm[e]);
-                YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc);
+                YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc[e]);
                 v = VYp[e];
                 if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
-                YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc);
+                YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc[e]);
                 const int k = k0 + e;
                 v = VZ[e];
                 if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
-                ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, LAYER ? zface[min(k0 + e, s.nz)] : T(1));
+                ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, fkf[e]);
             }
             T ZH3 = vz_above;
             if (has_above) ZH3 = ZH3 - cv * (p_above - P[VW - 1]);
-            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, LAYER ? zface[min(k0 + VW, s.nz)] : T(1));
+            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, fkf[VW]);
 
+            const bool wall_cell = WALLS && (wall_k || j == 0 || j == s.ny - 1 || i == 0 || i == s.nx - 1);
             T Pn[VW];
 #pragma unroll
             for (int e = 0; e < VW; e++) {
@@ -955,25 +1007,60 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
                     }
                     if (NR > 0) pe = pe + d * s.relax_scale;
                     pe = pe - d * cp;
-                    if (WALLS) {
+                    if (WALLS && wall_cell) {
                         T fu, fp;
                         if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
                     }
                     if (LAYER) {
                         pe = pe * fi_cell;
                         pe = pe * fj_cell;
-                        pe = pe * zcell[k];
+                        pe = pe * fkc[e];
                     }
                 }
                 Pn[e] = pe;
             }
-            if (any_point) {
+
+            // Sources after damping, then receivers (scheme.py:293-296,360-363).
+            if (any_point && !overflow) {
+                for (int t = 0; t < np; t++) {
+                    const TilePoint pt = points[t];
+                    const int d = pt.k - k0;
+                    if (pt.i != i || pt.row != ry || d < 0 || d >= VW) continue;
+                    if (pt.q < s.n_src) {
+                        if (pt.k < s.nz && step < s.src_len[pt.q]) {
+                            const T add = s.cs * s.src_sig[pt.q * s.src_stride + step];
+#pragma unroll
+                            for (int e = 0; e < VW; e++)
+                                if (e == d) Pn[e] = Pn[e] + add;
+                        }
+                    } else {
+                        const int r = pt.q - s.n_src;
+                        if (step >= s.rec_start[r]) {
+                            T v = Pn[0];
+#pragma unroll
+                            for (int e = 1; e < VW; e++)
+                                if (e == d) v = Pn[e];
+                            s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
+                        }
+                    }
+                }
+            } else if (any_point) {
                 for (int q = 0; q < s.n_src; q++) {
                     const int64_t d = s.src_off[q] - base;
                     if (d >= 0 && d < VW && k0 + d < s.nz && step < s.src_len[q]) {
 #pragma unroll
                         for (int e = 0; e < VW; e++)
                             if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+                    }
+                }
+                for (int r = 0; r < s.n_rec; r++) {
+                    const int64_t d = s.rec_off[r] - base;
+                    if (d >= 0 && d < VW && step >= s.rec_start[r]) {
+                        T v = Pn[0];
+#pragma unroll
+                        for (int e = 1; e < VW; e++)
+                            if (e == d) v = Pn[e];
+                        s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
                     }
                 }
             }
@@ -990,19 +1077,6 @@ __global__ void __launch_bounds__(256, VW == 2 ? 3 : 2) fused_staged_sweep(const
             if (k0 + VW == s.nz) f.nvz[base + VW] = ZH3;
 #pragma unroll
             for (int r = 0; r < NR; r++) VecW<T, VW>::store(s.psi + r * s.field + base, Sg[r]);
-
-            if (any_point) {
-                for (int r = 0; r < s.n_rec; r++) {
-                    const int64_t d = s.rec_off[r] - base;
-                    if (d >= 0 && d < VW && step >= s.rec_start[r]) {
-                        T v = Pn[0];
-#pragma unroll
-                        for (int e = 1; e < VW; e++)
-                            if (e == d) v = Pn[e];
-                        s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
-                    }
-                }
-            }
 #pragma unroll
             for (int e = 0; e < VW; e++) XL[e] = XH[e];
         }
@@ -2008,9 +2082,7 @@ struct FusedStep {
 // Ring layout and shared memory of the staged sweep for `rows` y rows per CTA.
 struct StagedLayout {
     int64_t stage_elems = 0, off_vx = 0, off_vy = 0, off_vz = 0, off_psi = 0;
-    size_t smem(int stages, bool layer, int64_t pz, size_t es) const {
-        return kStagedBarrierBytes + (size_t)stages * stage_elems * es + (layer ? 2 * (size_t)pz * es : 0);
-    }
+    size_t smem(int stages, size_t es) const { return kStagedBarrierBytes + (size_t)stages * stage_elems * es; }
 };
 
 inline StagedLayout staged_layout(const RoomHost &h, int rows) {
@@ -2032,7 +2104,7 @@ inline int staged_block_x(const RoomHost &h, int vector) {
 inline int staged_stages(const acf_batch *b, int rows, int requested) {
     const RoomHost &h = b->rooms[0];
     const StagedLayout L = staged_layout(h, rows);
-    auto fits = [&](int S) { return L.smem(S, h.has_layer, h.pz, b->elem()) <= (size_t)b->smem_per_block; };
+    auto fits = [&](int S) { return L.smem(S, b->elem()) + 1024 <= (size_t)b->smem_per_block; };
     if (requested) return fits(requested) ? requested : 0;
     for (int S = 3; S >= 2; S--)
         if (fits(S)) return S;
@@ -2042,8 +2114,7 @@ inline int staged_stages(const acf_batch *b, int rows, int requested) {
 template <typename T, bool L, bool W, int NR>
 struct StagedStep {
     static void launch(const StagedParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
-        const size_t smem = kStagedBarrierBytes + (size_t)p.stages * p.stage_elems * sizeof(T) +
-                            (L ? 2 * (size_t)p.f.room.pz * sizeof(T) : 0);
+        const size_t smem = kStagedBarrierBytes + (size_t)p.stages * p.stage_elems * sizeof(T);
         static bool opted_in = false;
         if (!opted_in) {
             int optin = 0, device = 0;

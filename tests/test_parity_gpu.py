@@ -255,3 +255,32 @@ def test_staged_geometries_match_the_oracle(dtype):
             cuda.run(21)
             cuda.check_device()
             assert_same_state(cuda, oracle)
+
+
+@pytest.mark.parametrize("vector", [2, 4])
+def test_staged_points_in_one_tile(vector):
+    """The staged sweep gathers the sources and receivers of each CTA's tile once per launch:
+    several sources in one cell must still add up in the order they were added, receivers must
+    read the finished pressure, and a tile holding more points than the gathered list takes
+    (here 41 in one y row) must fall back to scanning every point -- all bit for bit."""
+    configuration = dict(walls=WallAdmittances.uniform(0.2))
+    oracle = OracleFDTD(GRID, AIR, **configuration)
+    cuda = CudaAcousticFDTD(GRID, steps_per_graph=8, **configuration)
+    cuda.set_staging(1, 0, 5, vector)
+    cuda.set_scheme("staged")
+    rng = np.random.default_rng(3)
+    initial = rng.standard_normal(GRID.shape)
+    signals = [rng.standard_normal(40) for _ in range(3)]
+    row = [(0.315, 0.255, (k + 0.5) * 0.03) for k in range(GRID.shape[2])]
+    for solver in (oracle, cuda):
+        solver.p[:] = initial
+        for signal in signals:                       # three sources, one cell
+            solver.add_volume_source((0.2, 0.2, 0.2), signal)
+        solver.add_volume_source((0.2, 0.2, 0.23), signals[0][::-1])
+        solver.add_pressure_receiver((0.2, 0.2, 0.2))
+        for point in row + row + row[:11]:           # 41 receivers in one row of one tile
+            solver.add_pressure_receiver(point)
+    oracle.run(30)
+    cuda.run(30)
+    cuda.check_device()
+    assert_same_state(cuda, oracle)
