@@ -2115,15 +2115,20 @@ template <typename T, bool L, bool W, int NR>
 struct StagedStep {
     static void launch(const StagedParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
         const size_t smem = kStagedBarrierBytes + (size_t)p.stages * p.stage_elems * sizeof(T);
+        // Opt in to the largest dynamic shared memory the block can hold beside its static part.
         static bool opted_in = false;
         if (!opted_in) {
             int optin = 0, device = 0;
             cudaGetDevice(&device);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 optin);
-            cudaFuncSetAttribute(fused_staged_sweep<T, L, W, NR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 optin);
+            auto opt_in = [optin](const void *kernel) {
+                cudaFuncAttributes attr{};
+                if (cudaFuncGetAttributes(&attr, kernel) == cudaSuccess)
+                    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         optin - (int)attr.sharedSizeBytes);
+            };
+            opt_in((const void *)fused_staged_sweep<T, L, W, NR, 2>);
+            opt_in((const void *)fused_staged_sweep<T, L, W, NR, 4>);
             opted_in = true;
         }
         if (p.vector == 2) fused_staged_sweep<T, L, W, NR, 2><<<g, b, smem, st>>>(p);
