@@ -668,7 +668,24 @@ struct StagedParams {
     int64_t stage_elems;            // elements of one ring buffer
     int64_t off_vx, off_vy, off_vz, off_psi;
     int32_t *error;                 // set to 1 when a wait ran out
+    float2 pairs[16];               // single precision: coefficients duplicated into both lanes
 };
+
+// Slots of StagedParams::pairs.
+enum { kPairCv = 0, kPairCp = 1, kPairRelaxScale = 2, kPairGain = 3, kPairDecay = 7, kPairMean = 11 };
+
+// Packed single precision (sm_100 f32x2): each lane is rounded exactly as the scalar
+// operation, so these reproduce the scalar arithmetic bit for bit.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// a - b as the fused a + (-1) b: the product is exact, so its single rounding is that of a - b.
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 dup2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 damp2(float2 v, float2 fa, float2 fb, float2 fc) {
+    return mul2(mul2(mul2(v, fa), fb), fc);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -966,58 +983,137 @@ fused_staged_sweep(const StagedParams<T> g) {
                 fi1_face = __ldg(s.face[0] + i + 1);
             }
 
-            T XH[VW], YL[VW], YH[VW], ZL[VW];
-#pragma unroll
-            for (int e = 0; e < VW; e++) {
-                T v = VXo[e];
-                if (x_inner) v = v - cv * (PX[e] - P[e]);
-                XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc[e]);
-                v = VY[e];
-                if (j > 0) v = v - cv * (P[e] - PYm[e]);
-                YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc[e]);
-                v = VYp[e];
-                if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
-                YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc[e]);
-                const int k = k0 + e;
-                v = VZ[e];
-                if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
-                ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, fkf[e]);
-            }
-            T ZH3 = vz_above;
-            if (has_above) ZH3 = ZH3 - cv * (p_above - P[VW - 1]);
-            ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, fkf[VW]);
-
+            T XH[VW], YL[VW], YH[VW], ZL[VW], Pn[VW], ZH3;
             const bool wall_cell = WALLS && (wall_k || j == 0 || j == s.ny - 1 || i == 0 || i == s.nx - 1);
-            T Pn[VW];
+            if constexpr (sizeof(T) == 4) {
+                // Packed single precision: two lanes per instruction, each lane rounded exactly
+                // as the scalar operation it replaces, in the same order.
+                constexpr int NP = VW / 2;
+                const float2 cv2 = g.pairs[kPairCv];
+                const float2 fic = dup2(fi_cell), fi1f = dup2(fi1_face);
+                const float2 fjc = dup2(fj_cell), fjf = dup2(fj_face), fj1f = dup2(fj1_face);
+                float2 P2[NP], XH2[NP], YL2[NP], YH2[NP], ZL2[NP];
 #pragma unroll
-            for (int e = 0; e < VW; e++) {
-                const int k = k0 + e;
-                T pe = P[e];
-                if (k < s.nz) {
-                    const T zh = e + 1 < VW ? ZL[e + 1] : ZH3;
-                    T d = XH[e] - XL[e];
-                    d = d + (YH[e] - YL[e]);
-                    d = d + (zh - ZL[e]);
+                for (int q = 0; q < NP; q++) {
+                    const int a = 2 * q;
+                    P2[q] = make_float2(P[a], P[a + 1]);
+                    const float2 fk = make_float2(fkc[a], fkc[a + 1]);
+                    float2 v = make_float2(VXo[a], VXo[a + 1]);
+                    if (x_inner) v = sub2(v, mul2(cv2, sub2(make_float2(PX[a], PX[a + 1]), P2[q])));
+                    XH2[q] = LAYER ? damp2(v, fi1f, fjc, fk) : v;
+                    v = make_float2(VY[a], VY[a + 1]);
+                    if (j > 0) v = sub2(v, mul2(cv2, sub2(P2[q], make_float2(PYm[a], PYm[a + 1]))));
+                    YL2[q] = LAYER ? damp2(v, fic, fjf, fk) : v;
+                    v = make_float2(VYp[a], VYp[a + 1]);
+                    if (j + 1 < s.ny) v = sub2(v, mul2(cv2, sub2(make_float2(PYp[a], PYp[a + 1]), P2[q])));
+                    YH2[q] = LAYER ? damp2(v, fic, fj1f, fk) : v;
+                    // z lower faces: lanes with 0 < k < nz take the gradient update
+                    const float2 vz = make_float2(VZ[a], VZ[a + 1]);
+                    const float2 pm = make_float2(a == 0 ? p_below : P[a - 1], P[a]);
+                    v = sub2(vz, mul2(cv2, sub2(P2[q], pm)));
+                    if (!(k0 > 0 && k0 + VW <= s.nz)) {
+                        if (!(k0 + a > 0 && k0 + a < s.nz)) v.x = vz.x;
+                        if (!(k0 + a + 1 < s.nz)) v.y = vz.y;
+                    }
+                    ZL2[q] = LAYER ? damp2(v, fic, fjc, make_float2(fkf[a], fkf[a + 1])) : v;
+                }
+                ZH3 = vz_above;
+                if (has_above) ZH3 = ZH3 - cv * (p_above - P[VW - 1]);
+                ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, fkf[VW]);
+
+#pragma unroll
+                for (int q = 0; q < NP; q++) {
+                    const int a = 2 * q;
+                    const float2 xl = make_float2(XL[a], XL[a + 1]);
+                    const float2 zh = make_float2(ZL2[q].y, q + 1 < NP ? ZL2[q + 1 < NP ? q + 1 : q].x : ZH3);
+                    float2 d = sub2(XH2[q], xl);
+                    d = add2(d, sub2(YH2[q], YL2[q]));
+                    d = add2(d, sub2(zh, ZL2[q]));
+                    float2 pe = P2[q];
 #pragma unroll
                     for (int r = 0; r < NR; r++) {
-                        const T target = d * s.gain[r];
-                        const T offset = Sg[r][e] - target;
-                        Sg[r][e] = offset * s.decay[r] + target;
-                        pe = pe + offset * s.mean[r];
+                        const float2 old = make_float2(Sg[r][a], Sg[r][a + 1]);
+                        const float2 target = mul2(d, g.pairs[kPairGain + r]);
+                        const float2 offset = sub2(old, target);
+                        float2 next = add2(mul2(offset, g.pairs[kPairDecay + r]), target);
+                        pe = add2(pe, mul2(offset, g.pairs[kPairMean + r]));
+                        if (k0 + a >= s.nz) next.x = old.x;          // padding lanes keep psi
+                        if (k0 + a + 1 >= s.nz) next.y = old.y;
+                        Sg[r][a] = next.x;
+                        Sg[r][a + 1] = next.y;
                     }
-                    if (NR > 0) pe = pe + d * s.relax_scale;
-                    pe = pe - d * cp;
+                    if (NR > 0) pe = add2(pe, mul2(d, g.pairs[kPairRelaxScale]));
+                    pe = sub2(pe, mul2(d, g.pairs[kPairCp]));
                     if (WALLS && wall_cell) {
-                        T fu, fp;
-                        if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
+                        float fu, fp;
+                        if (k0 + a < s.nz && wall_pair(s, i, j, k0 + a, fu, fp)) pe.x = pe.x * fu - P[a] * fp;
+                        if (k0 + a + 1 < s.nz && wall_pair(s, i, j, k0 + a + 1, fu, fp))
+                            pe.y = pe.y * fu - P[a + 1] * fp;
                     }
-                    if (LAYER) {
-                        pe = pe * fi_cell;
-                        pe = pe * fj_cell;
-                        pe = pe * fkc[e];
-                    }
+                    if (LAYER) pe = mul2(mul2(mul2(pe, fic), fjc), make_float2(fkc[a], fkc[a + 1]));
+                    Pn[a] = k0 + a < s.nz ? pe.x : P[a];
+                    Pn[a + 1] = k0 + a + 1 < s.nz ? pe.y : P[a + 1];
+                    XH[a] = XH2[q].x;
+                    XH[a + 1] = XH2[q].y;
+                    YL[a] = YL2[q].x;
+                    YL[a + 1] = YL2[q].y;
+                    YH[a] = YH2[q].x;
+                    YH[a + 1] = YH2[q].y;
+                    ZL[a] = ZL2[q].x;
+                    ZL[a + 1] = ZL2[q].y;
                 }
-                Pn[e] = pe;
+            } else {
+    #pragma unroll
+                for (int e = 0; e < VW; e++) {
+                    T v = VXo[e];
+                    if (x_inner) v = v - cv * (PX[e] - P[e]);
+                    XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc[e]);
+                    v = VY[e];
+                    if (j > 0) v = v - cv * (P[e] - PYm[e]);
+                    YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc[e]);
+                    v = VYp[e];
+                    if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
+                    YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc[e]);
+                    const int k = k0 + e;
+                    v = VZ[e];
+                    if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
+                    ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, fkf[e]);
+                }
+                ZH3 = vz_above;
+                if (has_above) ZH3 = ZH3 - cv * (p_above - P[VW - 1]);
+                ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, fkf[VW]);
+
+    #pragma unroll
+                for (int e = 0; e < VW; e++) {
+                    const int k = k0 + e;
+                    T pe = P[e];
+                    if (k < s.nz) {
+                        const T zh = e + 1 < VW ? ZL[e + 1] : ZH3;
+                        T d = XH[e] - XL[e];
+                        d = d + (YH[e] - YL[e]);
+                        d = d + (zh - ZL[e]);
+    #pragma unroll
+                        for (int r = 0; r < NR; r++) {
+                            const T target = d * s.gain[r];
+                            const T offset = Sg[r][e] - target;
+                            Sg[r][e] = offset * s.decay[r] + target;
+                            pe = pe + offset * s.mean[r];
+                        }
+                        if (NR > 0) pe = pe + d * s.relax_scale;
+                        pe = pe - d * cp;
+                        if (WALLS && wall_cell) {
+                            T fu, fp;
+                            if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
+                        }
+                        if (LAYER) {
+                            pe = pe * fi_cell;
+                            pe = pe * fj_cell;
+                            pe = pe * fkc[e];
+                        }
+                    }
+                    Pn[e] = pe;
+                }
+
             }
 
             // Sources after damping, then receivers (scheme.py:293-296,360-363).
@@ -2165,6 +2261,17 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
             g.off_vz = lay.off_vz;
             g.off_psi = lay.off_psi;
             g.error = b->error_flag();
+            if (sizeof(T) == 4) {
+                auto put = [&](int slot, double v) { g.pairs[slot] = make_float2((float)v, (float)v); };
+                put(kPairCv, h.coef[0]);
+                put(kPairCp, h.coef[1]);
+                put(kPairRelaxScale, h.coef[3]);
+                for (int r = 0; r < h.n_relax; r++) {
+                    put(kPairGain + r, h.gain[r]);
+                    put(kPairDecay + r, h.decay[r]);
+                    put(kPairMean + r, h.mean[r]);
+                }
+            }
             const dim3 block(staged_block_x(h, b->staged_vector), b->staged_rows);
             const dim3 grid((h.ny + b->staged_rows - 1) / b->staged_rows, (h.nx + b->planes - 1) / b->planes);
             dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
