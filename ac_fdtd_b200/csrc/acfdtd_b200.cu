@@ -675,13 +675,22 @@ struct StagedParams {
 enum { kPairCv = 0, kPairCp = 1, kPairRelaxScale = 2, kPairGain = 3, kPairDecay = 7, kPairMean = 11 };
 
 // Packed single precision (sm_100 f32x2): each lane is rounded exactly as the scalar
-// operation, so these reproduce the scalar arithmetic bit for bit.
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-// a - b as the fused a + (-1) b: the product is exact, so its single rounding is that of a - b.
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
-    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
-}
+// operation. The explicit .rn modifier keeps the code generator from fusing a multiply and an
+// add into one rounding, as the PTX rules guarantee for rounding-qualified add, sub and mul --
+// without it a packed multiply feeding a packed add may become a packed fma.
+#define ACF_F32X2(NAME, OP)                                                                 \
+    __device__ __forceinline__ float2 NAME(float2 a, float2 b) {                            \
+        float2 r;                                                                           \
+        asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t" OP \
+            " d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"                                        \
+            : "=f"(r.x), "=f"(r.y)                                                          \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                      \
+        return r;                                                                           \
+    }
+ACF_F32X2(add2, "add.rn.f32x2")
+ACF_F32X2(sub2, "sub.rn.f32x2")
+ACF_F32X2(mul2, "mul.rn.f32x2")
+#undef ACF_F32X2
 __device__ __forceinline__ float2 dup2(float x) { return make_float2(x, x); }
 __device__ __forceinline__ float2 damp2(float2 v, float2 fa, float2 fb, float2 fc) {
     return mul2(mul2(mul2(v, fa), fb), fc);
