@@ -671,26 +671,24 @@ struct StagedParams {
     float2 pairs[16];               // single precision: coefficients duplicated into both lanes
 };
 
-// Slots of StagedParams::pairs.
-enum { kPairCv = 0, kPairCp = 1, kPairRelaxScale = 2, kPairGain = 3, kPairDecay = 7, kPairMean = 11 };
+// Slots of StagedParams::pairs; the Neg slots hold the negated coefficient.
+enum { kPairCv = 0, kPairCp = 1, kPairNegRelaxScale = 2, kPairGain = 3, kPairNegDecay = 7, kPairNegMean = 11 };
 
-// Packed single precision (sm_100 f32x2): each lane is rounded exactly as the scalar
-// operation. The explicit .rn modifier keeps the code generator from fusing a multiply and an
-// add into one rounding, as the PTX rules guarantee for rounding-qualified add, sub and mul --
-// without it a packed multiply feeding a packed add may become a packed fma.
-#define ACF_F32X2(NAME, OP)                                                                 \
-    __device__ __forceinline__ float2 NAME(float2 a, float2 b) {                            \
-        float2 r;                                                                           \
-        asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t" OP \
-            " d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"                                        \
-            : "=f"(r.x), "=f"(r.y)                                                          \
-            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                      \
-        return r;                                                                           \
-    }
-ACF_F32X2(add2, "add.rn.f32x2")
-ACF_F32X2(sub2, "sub.rn.f32x2")
-ACF_F32X2(mul2, "mul.rn.f32x2")
-#undef ACF_F32X2
+// Packed single precision (sm_100 f32x2), each lane rounded exactly as the scalar operation it
+// replaces. a +- b is the fused a + (+-1) b: the product by +-1 is exact, so the one rounding is
+// that of a +- b. The code generator was measured to fuse a packed multiply into a packed add
+// that consumes it -- one rounding where the reference has two -- even with contraction
+// disabled, and even through a + 1 * b; it was not measured to do so through a - b. So every
+// "plus a product" below is written as "minus the product by the negated coefficient", which
+// rounds identically (negation is exact and rounding is symmetric in sign), and add2 only ever
+// adds values that are not products.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(1.0f, 1.0f), a);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 dup2(float x) { return make_float2(x, x); }
 __device__ __forceinline__ float2 damp2(float2 v, float2 fa, float2 fb, float2 fc) {
     return mul2(mul2(mul2(v, fa), fb), fc);
@@ -1044,14 +1042,15 @@ fused_staged_sweep(const StagedParams<T> g) {
                         const float2 old = make_float2(Sg[r][a], Sg[r][a + 1]);
                         const float2 target = mul2(d, g.pairs[kPairGain + r]);
                         const float2 offset = sub2(old, target);
-                        float2 next = add2(mul2(offset, g.pairs[kPairDecay + r]), target);
-                        pe = add2(pe, mul2(offset, g.pairs[kPairMean + r]));
+                        // offset * decay + target, pe + offset * mean
+                        float2 next = sub2(target, mul2(offset, g.pairs[kPairNegDecay + r]));
+                        pe = sub2(pe, mul2(offset, g.pairs[kPairNegMean + r]));
                         if (k0 + a >= s.nz) next.x = old.x;          // padding lanes keep psi
                         if (k0 + a + 1 >= s.nz) next.y = old.y;
                         Sg[r][a] = next.x;
                         Sg[r][a + 1] = next.y;
                     }
-                    if (NR > 0) pe = add2(pe, mul2(d, g.pairs[kPairRelaxScale]));
+                    if (NR > 0) pe = sub2(pe, mul2(d, g.pairs[kPairNegRelaxScale]));   // pe + d * scale
                     pe = sub2(pe, mul2(d, g.pairs[kPairCp]));
                     if (WALLS && wall_cell) {
                         float fu, fp;
@@ -2274,11 +2273,15 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
                 auto put = [&](int slot, double v) { g.pairs[slot] = make_float2((float)v, (float)v); };
                 put(kPairCv, h.coef[0]);
                 put(kPairCp, h.coef[1]);
-                put(kPairRelaxScale, h.coef[3]);
+                // negated after the rounding to float, so each is exactly minus the scalar's value
+                auto put_neg = [&](int slot, double v) {
+                    g.pairs[slot] = make_float2(-(float)v, -(float)v);
+                };
+                put_neg(kPairNegRelaxScale, h.coef[3]);
                 for (int r = 0; r < h.n_relax; r++) {
                     put(kPairGain + r, h.gain[r]);
-                    put(kPairDecay + r, h.decay[r]);
-                    put(kPairMean + r, h.mean[r]);
+                    put_neg(kPairNegDecay + r, h.decay[r]);
+                    put_neg(kPairNegMean + r, h.mean[r]);
                 }
             }
             const dim3 block(staged_block_x(h, b->staged_vector), b->staged_rows);
