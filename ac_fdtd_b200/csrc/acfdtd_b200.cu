@@ -652,12 +652,18 @@ __global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(T, LAYER, NR)) fused
 // to hide the arithmetic's latency. The arithmetic is fused_column's, element for element, so
 // the results are identical to the two-sweep and fused schemes.
 //
-// Every wait is bounded (about two seconds). A CTA whose wait runs out raises the room's error
-// flag, waits (bounded again) for the copies it has issued and returns; the host reports the
-// flag as an error.
+// The copies are issued by a producer warp of their own. Consumer warps release a buffer through
+// an "empty" mbarrier once they are done with it, and the producer refills it with the plane
+// `stages` further on; there is no block-wide barrier in the march, so warps drift apart by up to
+// the ring depth instead of waiting for the slowest at every plane.
+//
+// Every wait is bounded (about two seconds). A warp whose wait runs out raises the room's error
+// flag and stops; the producer, before it returns, waits (bounded again) for the copies it has
+// issued. The host reports the flag as an error.
 
-constexpr int kStagedBarrierBytes = 128;       // room for up to 16 mbarriers
+constexpr int kStagedBarrierBytes = 128;       // full[8] then empty[8] mbarriers
 constexpr int kStagedMaxStages = 8;
+constexpr int kStagedMaxConsumers = 256;      // compute threads per CTA; one producer warp more
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 constexpr int kWaitLimitIterations = 1 << 21;
 
@@ -665,6 +671,7 @@ template <typename T>
 struct StagedParams {
     FusedParams<T> f;
     int32_t rows, stages, vector;   // vector: z elements per thread, 2 or 4
+    int32_t block_x;                // compute threads per row (a multiple of 32)
     int64_t stage_elems;            // elements of one ring buffer
     int64_t off_vx, off_vy, off_vz, off_psi;
     int32_t *error;                 // set to 1 when a wait ran out
@@ -700,6 +707,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
@@ -817,7 +828,7 @@ struct TilePoint {
 };
 
 template <typename T, bool LAYER, bool WALLS, int NR, int VW>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? (VW == 2 ? 2 : 1) : (VW == 2 ? 3 : 2))
+__global__ void __maxnreg__(sizeof(T) == 8 ? (VW == 2 ? 128 : 168) : (VW == 2 ? 80 : 128))
 fused_staged_sweep(const StagedParams<T> g) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ TilePoint points[kStagedPointCap];
@@ -825,11 +836,15 @@ fused_staged_sweep(const StagedParams<T> g) {
     const FusedParams<T> &f = g.f;
     const Room<T> &s = f.room;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + kStagedMaxStages;
     T *ring = reinterpret_cast<T *>(smem + kStagedBarrierBytes);
 
     const int S = g.stages;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int nthreads = blockDim.x * blockDim.y;
+    const int tid = threadIdx.x;
+    const int nthreads = blockDim.x;
+    const int consumers = g.block_x * g.rows;       // the last warp (tid >= consumers) is the producer
+    const bool producer = tid >= consumers;
+    const int lane = tid & 31;
     const int j0 = blockIdx.x * g.rows;
     const int i_begin = blockIdx.y * f.planes;
     const int i_end = min(s.nx, i_begin + f.planes);
@@ -865,13 +880,16 @@ fused_staged_sweep(const StagedParams<T> g) {
     };
 
     if (tid == 0) {
-        for (int q = 0; q < S; q++) mbar_init(full + q, 1);
+        for (int q = 0; q < S; q++) {
+            mbar_init(full + q, 1);
+            mbar_init(empty + q, consumers / 32);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         n_points = 0;
     }
     __syncthreads();
-    int issued = i_begin - 1;   // last plane issued (thread 0)
-    if (tid == 0) {
+    int issued = i_begin - 1;   // last plane issued (producer lane 0)
+    if (tid == consumers) {
         for (int q = 0; q < S && i_begin + q <= i_end; q++) issue(i_begin + q, q);
         issued = min(i_begin + S - 1, i_end);
     }
@@ -908,10 +926,10 @@ fused_staged_sweep(const StagedParams<T> g) {
     const int np = any_point ? n_points : 0;
     const bool overflow = np > kStagedPointCap;   // too many: scan every point, as fused_column
 
-    const int c = threadIdx.x;
-    const int ry = threadIdx.y;
+    const int c = tid % g.block_x;
+    const int ry = tid / g.block_x;
     const int j = j0 + ry;
-    const bool active = c < (s.nz + VW - 1) / VW && j < s.ny;
+    const bool active = !producer && c < (s.nz + VW - 1) / VW && j < s.ny;
     const int k0 = c * VW;
     const T cv = s.cv, cp = s.cp;
     const int64_t step = any_point ? (*f.step_base + f.local_step) : 0;
@@ -952,15 +970,53 @@ fused_staged_sweep(const StagedParams<T> g) {
         }
     }
 
-    int i = i_begin;
-    bool ok = true;
-    for (; i < i_end; i++) {
+    if (producer) {
+        // Refill each buffer once every consumer warp has released it.
+        if (lane == 0) {
+            bool ok = true;
+            for (int q = i_begin + S; q <= i_end; q++) {
+                const int u = q - i_begin;
+                if (!mbar_wait(empty + u % S, (uint32_t)(u / S - 1) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                issue(q, u % S);
+                issued = q;
+            }
+            if (!ok) {
+                atomicExch(g.error, 1);
+                // The latest plane issued into each buffer must land before the CTA exits.
+                for (int q = max(i_begin, issued - S + 1); q <= issued; q++) {
+                    const int u = q - i_begin;
+                    mbar_wait(full + u % S, (uint32_t)(u / S) & 1u);
+                }
+            }
+        }
+        return;
+    }
+
+    // x damping profiles of the current plane, loaded one plane ahead.
+    T fi_cell_next = T(1), fi1_face_next = T(1);
+    if (LAYER && active) {
+        fi_cell_next = __ldg(s.cell[0] + i_begin);
+        fi1_face_next = __ldg(s.face[0] + i_begin + 1);
+    }
+    for (int i = i_begin; i < i_end; i++) {
         const int u = i - i_begin;
         const int slot = u % S, nslot = (u + 1) % S;
         // Buffer `slot` (plane i) was already waited for as the next plane, except at the start.
         bool ready = u > 0 || mbar_wait(full + slot, 0u);
         ready = ready && mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u);
-        if (ready && active) {
+        if (!ready) {
+            atomicExch(g.error, 1);
+            return;
+        }
+        const T fi_cell_here = fi_cell_next, fi1_face_here = fi1_face_next;
+        if (LAYER && active && i + 1 < i_end) {
+            fi_cell_next = __ldg(s.cell[0] + i + 1);
+            fi1_face_next = __ldg(s.face[0] + i + 2);
+        }
+        if (active) {
             const T *cur = ring + (int64_t)slot * g.stage_elems;
             const T *nxt = ring + (int64_t)nslot * g.stage_elems;
             const int64_t base = (int64_t)i * s.plane + column;
@@ -984,11 +1040,7 @@ fused_staged_sweep(const StagedParams<T> g) {
 #pragma unroll
             for (int r = 0; r < NR; r++)
                 VecW<T, VW>::lds(cur + g.off_psi + ((int64_t)r * g.rows + ry) * s.pz + k0, Sg[r]);
-            T fi_cell = T(1), fi1_face = T(1);
-            if (LAYER) {
-                fi_cell = __ldg(s.cell[0] + i);
-                fi1_face = __ldg(s.face[0] + i + 1);
-            }
+            const T fi_cell = fi_cell_here, fi1_face = fi1_face_here;
 
             T XH[VW], YL[VW], YH[VW], ZL[VW], Pn[VW], ZH3;
             const bool wall_cell = WALLS && (wall_k || j == 0 || j == s.ny - 1 || i == 0 || i == s.nx - 1);
@@ -1184,23 +1236,9 @@ fused_staged_sweep(const StagedParams<T> g) {
 #pragma unroll
             for (int e = 0; e < VW; e++) XL[e] = XH[e];
         }
-        // Every thread is done with buffer `slot` (plane i); refill it with plane i + S.
-        if (__syncthreads_or(!ready)) {
-            ok = false;
-            break;
-        }
-        if (tid == 0 && i + S <= i_end) {
-            issue(i + S, slot);
-            issued = i + S;
-        }
-    }
-    if (!ok && tid == 0) {
-        atomicExch(g.error, 1);
-        // Let the copies still in flight land before the CTA's shared memory is released.
-        for (int q = i; q <= issued; q++) {
-            const int u = q - i_begin;
-            mbar_wait(full + u % S, (uint32_t)(u / S) & 1u);
-        }
+        // This warp is done with buffer `slot` (plane i).
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + slot);
     }
 }
 
@@ -2284,7 +2322,8 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
                     put_neg(kPairNegMean + r, h.mean[r]);
                 }
             }
-            const dim3 block(staged_block_x(h, b->staged_vector), b->staged_rows);
+            g.block_x = staged_block_x(h, b->staged_vector);
+            const dim3 block(g.block_x * b->staged_rows + 32);
             const dim3 grid((h.ny + b->staged_rows - 1) / b->staged_rows, (h.nx + b->planes - 1) / b->planes);
             dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
         } else {
@@ -2895,7 +2934,7 @@ int set_scheme(acf_batch *b, int32_t scheme) {
         return fail(ACF_ERR_STATE, "the fused schemes are for single rooms");
     if (scheme == ACF_SCHEME_FUSED_STAGED) {
         const RoomHost &h = b->rooms[0];
-        if (staged_block_x(h, b->staged_vector) * b->staged_rows > 256)
+        if (staged_block_x(h, b->staged_vector) * b->staged_rows > kStagedMaxConsumers)
             return fail(ACF_ERR_ARGUMENT, "staged scheme: %d rows of %d threads exceed 256 threads per CTA",
                         b->staged_rows, staged_block_x(h, b->staged_vector));
         if (!staged_stages(b, b->staged_rows, b->staged_stages))
@@ -3622,7 +3661,7 @@ int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages, int32_t vector)
         return fail(ACF_ERR_ARGUMENT, "stages must be 0 or in [2, %d], got %d", kStagedMaxStages, stages);
     if (vector != 2 && vector != 4) return fail(ACF_ERR_ARGUMENT, "vector must be 2 or 4, got %d", vector);
     const RoomHost &room = h->rooms[0];
-    if (staged_block_x(room, vector) * rows > 256)
+    if (staged_block_x(room, vector) * rows > kStagedMaxConsumers)
         return fail(ACF_ERR_ARGUMENT, "%d rows of %d threads exceed 256 threads per CTA", rows,
                     staged_block_x(room, vector));
     if (!staged_stages(h, rows, stages))
