@@ -30,8 +30,8 @@ _cache: dict[str, tuple[int, int]] = {}
 
 #: (rows per CTA, ring buffers (0: automatic), planes per CTA, z elements per thread) tried
 #: for the staged scheme.
-STAGED_CANDIDATES = ((1, 3, 16, 2), (1, 4, 16, 2), (1, 3, 32, 2), (1, 3, 8, 2), (2, 3, 16, 4),
-                     (1, 2, 16, 2))
+STAGED_CANDIDATES = ((2, 3, 32, 4), (2, 4, 32, 4), (2, 3, 16, 4), (2, 3, 64, 4), (1, 3, 32, 4),
+                     (1, 3, 32, 2))
 
 #: Schemes raced by default; all give bit-identical results.
 SCHEMES = ("staged", "fused", "two_sweeps")

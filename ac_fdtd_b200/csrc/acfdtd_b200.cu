@@ -1978,9 +1978,9 @@ struct acf_batch {
     int block_threads = 256;
     int planes = 4;
     int ctas_per_sm = 4;
-    int staged_rows = 1;             // staged scheme: y rows per CTA
+    int staged_rows = 2;             // staged scheme: y rows per CTA
     int staged_stages = 0;           // staged scheme: ring buffers per CTA (0: automatic)
-    int staged_vector = 2;           // staged scheme: z elements per thread (2 or 4)
+    int staged_vector = 4;           // staged scheme: z elements per thread (2 or 4)
     int smem_per_sm = 233472, smem_per_block = 232448;
 
     // graphs (index: parity of the fused scheme's current buffer at the start of a replay)
@@ -2702,6 +2702,11 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
         b->ctas_per_sm = 0;
     } else {
         b->block_threads = 128;
+        // staged scheme: two rows of 4-element threads where they fit in 256 threads (measured
+        // best at 384^3), with the automatic ring depth
+        const int bx4 = (int)round_up((b->rooms[0].nz + 3) / 4, 32);
+        b->staged_rows = 2 * bx4 <= kStagedMaxConsumers ? 2 : 1;
+        b->staged_vector = 4;
         b->planes = 4;
         while ((b->rooms[0].nx + b->planes - 1) / b->planes > 65535) b->planes *= 2;
     }

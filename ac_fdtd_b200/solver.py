@@ -462,8 +462,8 @@ class CudaAcousticFDTD:
         _native.check(self._lib.acf_set_launch(self._handle, int(block_threads), int(planes)),
                       "acf_set_launch")
 
-    def set_staging(self, rows: int = 1, stages: int = 0, planes: int | None = None,
-                    vector: int = 2) -> None:
+    def set_staging(self, rows: int = 2, stages: int = 0, planes: int | None = None,
+                    vector: int = 4) -> None:
         """Geometry of the staged scheme: y rows per CTA, ring buffers (0: automatic), z
         elements per thread (2 or 4) and, if given, x planes per CTA (which also sets 128
         threads per block for the other schemes)."""

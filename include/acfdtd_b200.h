@@ -144,8 +144,8 @@ int acf_get_scheme(const acf_solver *solver);
  * buffers per CTA (2..8; 0 picks three, or two where three do not fit) and z elements per
  * thread (2 or 4). The x planes per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the
  * CTA would need more than 256 threads or more shared memory than an SM offers; results never
- * depend on it. Default: 1 row, automatic stages, 2 elements. No counterpart in the
- * reference. */
+ * depend on it. Default: 2 rows where 2 rows of 4-element threads fit in 256 threads (else 1),
+ * automatic stages, 4 elements. No counterpart in the reference. */
 int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages, int32_t vector);
 
 /* 0 when no kernel of this solver reported a failed wait; 1 (and the flag cleared) when a
