@@ -21,9 +21,10 @@ __all__ = ["CANDIDATES", "BATCH_CANDIDATES", "STAGED_CANDIDATES", "tune", "apply
 #: (threads per block, planes per block) tried by default.
 CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
 
-#: (threads per tile, planes per tile, CTAs per SM; 0 = one CTA per tile) for batches.
-BATCH_CANDIDATES = ((128, 8, 0), (256, 4, 0), (128, 4, 0), (128, 2, 0), (256, 8, 0), (256, 4, 4),
-                    (128, 4, 8), (256, 2, 0))
+#: (scheme, threads per tile, planes per tile, CTAs per SM; 0 = one CTA per tile) for batches.
+BATCH_CANDIDATES = (("fused", 128, 8, 0), ("fused", 128, 4, 0), ("fused", 64, 8, 0),
+                    ("fused", 256, 4, 0), ("two_sweeps", 128, 8, 0), ("two_sweeps", 256, 4, 0),
+                    ("two_sweeps", 128, 4, 0), ("two_sweeps", 256, 4, 4))
 
 _cache: dict[str, tuple[int, int]] = {}
 
@@ -141,7 +142,8 @@ def tune_batch(batch, candidates=BATCH_CANDIDATES, steps: int = 12, repeats: int
             twin.set_field(r, 0, np.random.default_rng(r).standard_normal(twin.shapes[r]) * 1e-3)
         for candidate in candidates:
             try:
-                twin.set_launch(*candidate)
+                twin.set_scheme(candidate[0])
+                twin.set_launch(*candidate[1:])
             except RuntimeError:
                 continue
             twin.run(2)
@@ -163,5 +165,6 @@ def apply_tuned_batch(batch, candidates=BATCH_CANDIDATES):
     if key not in _cache:
         winner, _ = tune_batch(batch, candidates)
         _cache[key] = winner
-    batch.set_launch(*_cache[key])
+    batch.set_scheme(_cache[key][0])
+    batch.set_launch(*_cache[key][1:])
     return _cache[key]

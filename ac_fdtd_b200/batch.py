@@ -37,7 +37,7 @@ class RoomBatch:
 
     def __init__(self, rooms, dtype=np.float32, *, stream: int = 0,
                  steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
-                 differentiable_walls: bool = False) -> None:
+                 differentiable_walls: bool = False, scheme: str = "two_sweeps") -> None:
         if not rooms:
             raise ValueError("a batch needs at least one room")
         self.dtype = np.dtype(dtype)
@@ -91,6 +91,8 @@ class RoomBatch:
         self._receivers = [[] for _ in rooms]
         self._dirty_sources: set[int] = set()
         self._dirty_receivers: set[int] = set()
+        self.scheme = "two_sweeps"
+        self.set_scheme(scheme)
 
     # ------------------------------------------------------------------ geometry
     def __len__(self) -> int:
@@ -217,6 +219,18 @@ class RoomBatch:
         del keep
         spec.update(walls=walls, absorbing_layer=absorbing_layer, air_absorption=air_absorption)
         self.blocks[room] = block
+
+    SCHEMES = {"two_sweeps": _native.SCHEME_TWO_SWEEPS, "fused": _native.SCHEME_FUSED}
+
+    def set_scheme(self, scheme: str) -> None:
+        """``"two_sweeps"`` (a velocity launch and a pressure launch per step, in place) or
+        ``"fused"`` (one launch per step into a second copy of every room's p and v, (8 + 2R)
+        instead of (12 + 2R) elements moved per cell). Results are bit-identical."""
+        if scheme not in self.SCHEMES:
+            raise ValueError(f"scheme must be one of {sorted(self.SCHEMES)}, got {scheme!r}")
+        _native.check(self._lib.acf_batch_set_scheme(self._handle, self.SCHEMES[scheme]),
+                      "acf_batch_set_scheme")
+        self.scheme = scheme
 
     def reset_state(self) -> None:
         """Every room at rest (all fields zero), on the device."""

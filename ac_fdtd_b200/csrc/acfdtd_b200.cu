@@ -1336,6 +1336,44 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) pressure_batch(
     }
 }
 
+// (a)+(b) over a batch: the fused step (fused_column) on the same tile table, each CTA staging
+// the fused parameters of its tile's room -- the room description with the current p and v and
+// the next copy to write -- for the parity all rooms are at.
+template <typename T>
+struct FusedBatchParams {
+    const FusedParams<T> *rooms;   // one per room, for the current parity
+    const Tile *tiles;
+    int32_t n_tiles;
+    int32_t local_step;
+    const int64_t *step_base;
+};
+
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) fused_batch(const FusedBatchParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(FusedParams<T>)];
+    FusedParams<T> *room = reinterpret_cast<FusedParams<T> *>(raw);
+    static_assert(sizeof(FusedParams<T>) % sizeof(int) == 0, "FusedParams must be a whole number of words");
+    const int64_t step = *b.step_base + b.local_step;
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            const int *from = reinterpret_cast<const int *>(b.rooms + tile.room);
+            int *to = reinterpret_cast<int *>(raw);
+            for (int w = threadIdx.x; w < (int)(sizeof(FusedParams<T>) / sizeof(int)); w += blockDim.x)
+                to[w] = __ldg(from + w);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            fused_column<T, LAYER, WALLS, NR>(*room, tile.i_begin, tile.i_end, pair / room->room.nchunks,
+                                              pair % room->room.nchunks, step);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // Adjoint: the transposed leapfrog, run backward in time (single rooms).
 //
@@ -1964,6 +2002,7 @@ struct acf_batch {
     void *state = nullptr;           // every room's fields, one arena
     size_t state_bytes = 0;
     void *room_table = nullptr;      // device array of Room<T>, one per room
+    void *fused_table = nullptr;     // fused scheme on a batch: 2 x rooms FusedParams<T>, by parity
     bool room_table_dirty = true;
     Tile *tiles = nullptr;
     int32_t n_tiles = 0;
@@ -2044,10 +2083,8 @@ struct acf_batch {
     int n_fields() const { return 4 + n_relax; }
     size_t room_block_bytes(int r) const { return (size_t)n_fields() * rooms[r].field * elem(); }
     int scheme = ACF_SCHEME_TWO_SWEEPS;
-    // one sweep per step into the second copy of p and v (fused or fused-staged)
-    bool fused() const {
-        return rooms.size() == 1 && (scheme == ACF_SCHEME_FUSED || scheme == ACF_SCHEME_FUSED_STAGED);
-    }
+    // one sweep per step into the second copy of p and v (fused, or fused-staged for one room)
+    bool fused() const { return scheme == ACF_SCHEME_FUSED || scheme == ACF_SCHEME_FUSED_STAGED; }
     int32_t *error_flag() const { return reinterpret_cast<int32_t *>(step_base + 1); }
     char *field_ptr(int r, int f) const {
         const RoomHost &h = rooms[r];
@@ -2128,6 +2165,28 @@ int upload_room_table(acf_batch *b) {
     for (size_t r = 0; r < b->rooms.size(); r++) table[r] = make_room<T>(b, (int)r);
     if (!b->room_table) ACF_CUDA(cudaMalloc(&b->room_table, table.size() * sizeof(Room<T>)));
     ACF_CUDA(cudaMemcpy(b->room_table, table.data(), table.size() * sizeof(Room<T>), cudaMemcpyHostToDevice));
+    if (b->scheme == ACF_SCHEME_FUSED) {
+        // Both parities: entry [parity * rooms + r] reads the copy that is current at that parity.
+        const size_t n = b->rooms.size();
+        std::vector<FusedParams<T>> fused(2 * n);
+        for (int parity = 0; parity < 2; parity++)
+            for (size_t r = 0; r < n; r++) {
+                RoomHost &h = b->rooms[r];
+                const int saved = h.cur;
+                h.cur = parity;
+                FusedParams<T> &f = fused[parity * n + r];
+                f = FusedParams<T>{};
+                f.room = make_room<T>(b, (int)r);
+                f.np = (T *)b->other_ptr((int)r, ACF_FIELD_P);
+                f.nvx = (T *)b->other_ptr((int)r, ACF_FIELD_VX);
+                f.nvy = (T *)b->other_ptr((int)r, ACF_FIELD_VY);
+                f.nvz = (T *)b->other_ptr((int)r, ACF_FIELD_VZ);
+                h.cur = saved;
+            }
+        if (!b->fused_table) ACF_CUDA(cudaMalloc(&b->fused_table, fused.size() * sizeof(FusedParams<T>)));
+        ACF_CUDA(cudaMemcpy(b->fused_table, fused.data(), fused.size() * sizeof(FusedParams<T>),
+                            cudaMemcpyHostToDevice));
+    }
     b->room_table_dirty = false;
     return ACF_OK;
 }
@@ -2221,6 +2280,13 @@ struct FusedStep {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct BatchFused {
+    static void launch(const FusedBatchParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        fused_batch<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
 // Ring layout and shared memory of the staged sweep for `rows` y rows per CTA.
 struct StagedLayout {
     int64_t stage_elems = 0, off_vx = 0, off_vy = 0, off_vz = 0, off_psi = 0;
@@ -2283,6 +2349,22 @@ struct StagedStep {
 template <typename T>
 void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
     if (events) cudaEventRecord(events[0], st);
+    if (b->rooms.size() > 1 && b->fused()) {
+        FusedBatchParams<T> p{};
+        p.rooms = (const FusedParams<T> *)b->fused_table + (b->rooms[0].cur ? b->rooms.size() : 0);
+        p.tiles = b->tiles;
+        p.n_tiles = b->n_tiles;
+        p.local_step = local;
+        p.step_base = b->step_base;
+        const dim3 grid(b->batch_ctas), block(b->block_threads);
+        dispatch_pressure<T, BatchFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        for (RoomHost &h : b->rooms) h.cur ^= 1;
+        if (events) {
+            cudaEventRecord(events[1], st);
+            cudaEventRecord(events[2], st);
+        }
+        return;
+    }
     if (b->fused()) {
         RoomHost &h = b->rooms[0];
         FusedParams<T> f{};
@@ -2561,6 +2643,7 @@ void free_batch(acf_batch *b) {
     cudaFree(b->badj_table);
     cudaFree(b->state);
     cudaFree(b->room_table);
+    cudaFree(b->fused_table);
     cudaFree(b->tiles);
     cudaFree(b->step_base);
     cudaFree(b->energy_scratch);
@@ -2927,6 +3010,7 @@ int make_primary(acf_batch *b, cudaStream_t st) {
         ACF_CUDA(cudaMemcpyAsync((char *)b->state + h.state_off, h.second, bytes, cudaMemcpyDeviceToDevice, st));
         h.cur = 0;
         b->graph_dirty = b->adj_graphs_dirty = true;
+        b->room_table_dirty = true;
     }
     return ACF_OK;
 }
@@ -2935,8 +3019,8 @@ int set_scheme(acf_batch *b, int32_t scheme) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
     if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED && scheme != ACF_SCHEME_FUSED_STAGED)
         return fail(ACF_ERR_ARGUMENT, "unknown scheme %d", scheme);
-    if (scheme != ACF_SCHEME_TWO_SWEEPS && b->rooms.size() != 1)
-        return fail(ACF_ERR_STATE, "the fused schemes are for single rooms");
+    if (scheme == ACF_SCHEME_FUSED_STAGED && b->rooms.size() != 1)
+        return fail(ACF_ERR_STATE, "the staged scheme is for single rooms");
     if (scheme == ACF_SCHEME_FUSED_STAGED) {
         const RoomHost &h = b->rooms[0];
         if (staged_block_x(h, b->staged_vector) * b->staged_rows > kStagedMaxConsumers)
@@ -2947,19 +3031,21 @@ int set_scheme(acf_batch *b, int32_t scheme) {
                         b->staged_rows, b->staged_stages);
     }
     DeviceGuard guard(b->device);
-    if (scheme != ACF_SCHEME_TWO_SWEEPS && !b->rooms[0].second) {
-        RoomHost &h = b->rooms[0];
-        const size_t bytes = ((size_t)4 * h.field + (size_t)h.pz) * b->elem();
-        if (cudaMalloc(&h.second, bytes) != cudaSuccess)
-            return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes for the fused scheme failed", bytes);
-        ACF_CUDA(cudaMemset(h.second, 0, bytes));
+    if (scheme != ACF_SCHEME_TWO_SWEEPS) {
+        for (RoomHost &h : b->rooms) {
+            if (h.second) continue;
+            const size_t bytes = ((size_t)4 * h.field + (size_t)h.pz) * b->elem();
+            if (cudaMalloc(&h.second, bytes) != cudaSuccess)
+                return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes for the fused scheme failed", bytes);
+            ACF_CUDA(cudaMemset(h.second, 0, bytes));
+        }
     }
     if (scheme == ACF_SCHEME_TWO_SWEEPS) {
         int rc = make_primary(b, 0);
         if (rc) return rc;
         ACF_CUDA(cudaStreamSynchronize(0));
     }
-    if (scheme != b->scheme) b->graph_dirty = b->adj_graphs_dirty = true;
+    if (scheme != b->scheme) b->graph_dirty = b->adj_graphs_dirty = b->room_table_dirty = true;
     b->scheme = scheme;
     return ACF_OK;
 }
@@ -3880,6 +3966,10 @@ int acf_batch_forward_record(acf_batch *b, int64_t n_steps, int64_t step_offset,
     if (step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step offset");
     DeviceGuard guard(b->device);
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        int rc0 = make_primary(b, st);   // the recorded run is the two sweeps, in place
+        if (rc0) return rc0;
+    }
     // recording capacity, as for a run
     for (RoomHost &r : b->rooms) {
         if (r.n_rec == 0) continue;
@@ -3917,9 +4007,15 @@ int acf_batch_adjoint_run(acf_batch *b, const double *grad_rec, double *grad_src
 int acf_batch_reset_state(acf_batch *b, acf_stream stream) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
     DeviceGuard guard(b->device);
+    for (RoomHost &h : b->rooms) {
+        if (h.cur) b->graph_dirty = b->adj_graphs_dirty = b->room_table_dirty = true;
+        h.cur = 0;
+    }
     ACF_CUDA(cudaMemsetAsync(b->state, 0, b->state_bytes, (cudaStream_t)stream));
     return ACF_OK;
 }
+
+int acf_batch_set_scheme(acf_batch *b, int32_t scheme) { return set_scheme(b, scheme); }
 
 int acf_batch_set_coefficients(acf_batch *b, int32_t room, const acf_config *config) {
     return set_coefficients(b, room, config);

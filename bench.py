@@ -341,6 +341,7 @@ def run_ours(args) -> None:
     batched = None if args.skip_extras else batched_vs_per_room(args)
     adjoint = None if args.skip_extras else adjoint_cost(args)
     inversion = None if args.skip_extras else batched_adjoint_cost(args)
+    precision = None if args.skip_extras else precision_check(args)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -360,6 +361,7 @@ def run_ours(args) -> None:
         "batched": batched,
         "adjoint": adjoint,
         "batched_inversion": inversion,
+        "precision": precision,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -371,6 +373,86 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _errors(single, double) -> dict:
+    """Relative L2 over every receiver and sample, and peak |error| over peak |p|."""
+    a = np.asarray(single, dtype=np.float64)
+    b = np.asarray(double, dtype=np.float64)
+    return {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+            "peak": float(np.max(np.abs(a - b)) / np.max(np.abs(b)))}
+
+
+def precision_check(args) -> dict:
+    """FP32 receiver signals against FP64 on the same rooms, and the FP64 throughput at the
+    headline size. The FP64 path performs the NumPy reference's float64 arithmetic bit for bit
+    (tests/test_parity_gpu.py), so it stands in for the reference at sizes NumPy cannot run."""
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, RoomBatch, WallAdmittances, gaussian_pulse
+    from ac_fdtd_b200.autotune import apply_tuned
+    from ac_fdtd_b200.workloads import differentiable_room, uneven_rooms
+
+    out = {}
+    # the headline room, T steps from rest in each precision
+    grid, objects, points = workload(args.size)
+    T = args.time_steps
+    recordings, times, schemes = {}, {}, {}
+    for dtype in (np.float32, np.float64):
+        solver = CudaAcousticFDTD(grid, dtype=dtype, **objects)
+        schemes[np.dtype(dtype).name] = launch_dict(apply_tuned(solver))
+        solver.add_volume_source(points[0], gaussian_pulse(T, solver.dt, 4000.0))
+        for point in points[1:]:
+            solver.add_pressure_receiver(point)
+        times[np.dtype(dtype).name] = _device_ms(lambda: solver.run(T), torch)
+        recordings[dtype] = solver.recorded_pressure
+        solver.close()
+    f64_gcups = grid.n_cells * T / (times["float64"] * 1e-3) / 1e9
+    peak, _ = measured_peak_hbm()
+    out["room_384"] = {
+        "workload": f"the headline room, {args.size}^3, {T} steps from rest, {len(points) - 1} receivers",
+        "fp32_vs_fp64": _errors(recordings[np.float32], recordings[np.float64]),
+        "fp64_gcups": f64_gcups,
+        "fp64_hbm_frac_of_measured_at_112_B_per_cell": f64_gcups * 112 / peak,
+        "fp64_launch": schemes["float64"],
+        "note": "one run including its CUDA-graph capture, timed with CUDA events",
+    }
+
+    # the differentiable room (128^3, its true walls), adjoint-steps long
+    grid4, true_xi, _, source, receivers = differentiable_room()
+    T4 = args.adjoint_steps
+    rec4 = {}
+    for dtype in (np.float32, np.float64):
+        solver = CudaAcousticFDTD(grid4, dtype=dtype, walls=WallAdmittances(*true_xi))
+        solver.add_volume_source(source, gaussian_pulse(T4, solver.dt, 2000.0))
+        for point in receivers:
+            solver.add_pressure_receiver(point)
+        solver.run(T4)
+        rec4[dtype] = solver.recorded_pressure
+        solver.close()
+    out["differentiable_128"] = {"workload": f"128^3, {T4} steps, 4 receivers",
+                                 "fp32_vs_fp64": _errors(rec4[np.float32], rec4[np.float64])}
+
+    # the 64 uneven rooms, batched, batch-steps long: the worst room
+    rooms = uneven_rooms()
+    T3 = args.batch_steps
+    rec3 = {}
+    for dtype in (np.float32, np.float64):
+        batch = RoomBatch([r[0] for r in rooms], dtype=dtype)
+        for r, (_, src, recs) in enumerate(rooms):
+            batch.add_volume_source(r, src, gaussian_pulse(T3, batch.dt(r), 2000.0))
+            for point in recs:
+                batch.add_pressure_receiver(r, point)
+        batch.run(T3)
+        rec3[dtype] = [batch.recorded_pressure(r) for r in range(len(rooms))]
+        batch.close()
+    per_room = [_errors(a, b) for a, b in zip(rec3[np.float32], rec3[np.float64])]
+    out["uneven_rooms"] = {"workload": f"64 uneven rooms, {T3} steps, 2 receivers each",
+                           "fp32_vs_fp64_worst_room": {
+                               "rel_l2": max(e["rel_l2"] for e in per_room),
+                               "peak": max(e["peak"] for e in per_room)},
+                           "fp32_vs_fp64_median_room_rel_l2": float(np.median([e["rel_l2"] for e in per_room]))}
+    return out
 
 
 def _device_ms(fn, torch) -> float:
@@ -416,8 +498,9 @@ def batched_vs_per_room(args) -> dict:
 
     solvers = []
     for spec, source, receivers in rooms:
+        # each room on its own, in the scheme the batch runs
         solver = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
-                                  air_absorption=spec["air_absorption"])
+                                  air_absorption=spec["air_absorption"], scheme=batch_geometry[0])
         solver.add_volume_source(source, gaussian_pulse(T, solver.dt, 2000.0))
         for point in receivers:
             solver.add_pressure_receiver(point)
@@ -442,10 +525,12 @@ def batched_vs_per_room(args) -> dict:
         "batched_gcups": batched_gcups,
         "per_room_gcups": cells * T / (per_room_ms * 1e-3) / 1e9,
         "speedup": per_room_ms / batch_ms,
-        "batched_hbm_frac_of_measured": batched_gcups * 1e9 * 72 / (peak * 1e9),
+        "batched_hbm_frac_of_measured": batched_gcups * (56 if batch_geometry[0] == "fused" else 72) / peak,
+        "bytes_per_cell": 56 if batch_geometry[0] == "fused" else 72,
         "launches_in_setup_and_runs": launches,
-        "batch_launch": {"block_threads": batch_geometry[0], "planes": batch_geometry[1],
-                         "ctas_per_sm": batch_geometry[2], "chosen_by": "ac_fdtd_b200.autotune"},
+        "batch_launch": {"scheme": batch_geometry[0], "block_threads": batch_geometry[1],
+                         "planes": batch_geometry[2], "ctas_per_sm": batch_geometry[3],
+                         "chosen_by": "ac_fdtd_b200.autotune"},
     }
 
 

@@ -262,6 +262,10 @@ int acf_batch_set_graph(acf_batch *batch, int32_t steps_per_graph);
  * grid striding over the tile table (0: one CTA per tile, scheduled by the hardware). */
 int acf_batch_set_launch(acf_batch *batch, int32_t block_threads, int32_t planes,
                          int32_t ctas_per_sm);
+/* ACF_SCHEME_TWO_SWEEPS or ACF_SCHEME_FUSED (one sweep per step over the tile table, into a
+ * second copy of every room's p and v); bit-identical results. No counterpart in the
+ * reference. */
+int acf_batch_set_scheme(acf_batch *batch, int32_t scheme);
 int acf_batch_energy_terms(acf_batch *batch, int32_t room, double dx, double terms[7],
                            acf_stream stream);
 int acf_batch_profile_enable(acf_batch *batch, int32_t enable);

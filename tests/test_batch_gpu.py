@@ -65,11 +65,12 @@ def populate(solver_like, room_index, spec, seed):
             solver_like.add_pressure_receiver(point)
 
 
+@pytest.mark.parametrize("scheme", ["two_sweeps", "fused"])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("with_air", [True, False])
-def test_every_room_matches_its_oracle(dtype, with_air):
+def test_every_room_matches_its_oracle(dtype, with_air, scheme):
     rooms = mixed_rooms(with_air)
-    batch = RoomBatch(rooms, dtype=dtype, steps_per_graph=16)
+    batch = RoomBatch(rooms, dtype=dtype, steps_per_graph=16, scheme=scheme)
     oracles = []
     for r, spec in enumerate(rooms):
         populate(batch, r, spec, seed=r)
@@ -91,8 +92,9 @@ def test_every_room_matches_its_oracle(dtype, with_air):
 def test_launch_geometry_does_not_change_results():
     rooms = mixed_rooms(True)
     results = []
-    for geometry in ((256, 4, 4), (64, 1, 2), (128, 16, 8), (32, 3, 1)):
-        batch = RoomBatch(rooms, dtype=np.float32, steps_per_graph=8)
+    for scheme, *geometry in (("two_sweeps", 256, 4, 4), ("two_sweeps", 64, 1, 2),
+                              ("fused", 128, 16, 8), ("fused", 32, 3, 1), ("fused", 128, 8, 0)):
+        batch = RoomBatch(rooms, dtype=np.float32, steps_per_graph=8, scheme=scheme)
         batch.set_launch(*geometry)
         for r, spec in enumerate(rooms):
             populate(batch, r, spec, seed=10 + r)
@@ -137,3 +139,34 @@ def test_profiled_and_graphed_batch_runs_agree():
     for r in range(len(rooms)):
         np.testing.assert_array_equal(a.p(r), b.p(r))
         np.testing.assert_array_equal(a.recorded_pressure(r), b.recorded_pressure(r))
+
+
+def test_fused_batch_switches_schemes_and_resets():
+    """The fused batch alternates every room between two copies of p and v: odd step counts,
+    state written between runs, a switch back to the two sweeps, a reset and a fresh run must
+    all see the current copy."""
+    rooms = mixed_rooms(True)
+    batch = RoomBatch(rooms, dtype=np.float64, steps_per_graph=8, scheme="fused")
+    oracles = []
+    for r, spec in enumerate(rooms):
+        populate(batch, r, spec, seed=60 + r)
+        oracle = OracleFDTD(spec["grid"], AIR, **{k: v for k, v in spec.items() if k != "grid"})
+        populate(oracle, r, spec, seed=60 + r)
+        oracles.append(oracle)
+    for scheme, n in (("fused", 9), ("fused", 16), ("two_sweeps", 5), ("fused", 3)):
+        batch.set_scheme(scheme)
+        batch.run(n)
+        for oracle in oracles:
+            oracle.run(n)
+    p1 = np.random.default_rng(1).standard_normal(rooms[1]["grid"].shape)
+    batch.set_field(1, 0, p1)
+    oracles[1].p[:] = p1
+    batch.run(7)
+    for oracle in oracles:
+        oracle.run(7)
+    for r, oracle in enumerate(oracles):
+        np.testing.assert_array_equal(batch.p(r), oracle.p, err_msg=f"room {r}")
+        np.testing.assert_array_equal(batch.recorded_pressure(r), oracle.recorded_pressure)
+    batch.reset_state()
+    for r in range(len(rooms)):
+        assert not np.any(batch.p(r)) and not any(np.any(v) for v in batch.velocity(r))
