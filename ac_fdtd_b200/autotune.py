@@ -22,8 +22,8 @@ __all__ = ["CANDIDATES", "BATCH_CANDIDATES", "STAGED_CANDIDATES", "tune", "apply
 CANDIDATES = ((64, 4), (64, 8), (128, 2), (128, 4), (128, 8), (256, 4), (256, 8))
 
 #: (scheme, threads per tile, planes per tile, CTAs per SM; 0 = one CTA per tile) for batches.
-BATCH_CANDIDATES = (("fused", 128, 8, 0), ("fused", 128, 4, 0), ("fused", 64, 8, 0),
-                    ("fused", 256, 4, 0), ("two_sweeps", 128, 8, 0), ("two_sweeps", 256, 4, 0),
+BATCH_CANDIDATES = (("fused", 128, 16, 0), ("fused", 128, 8, 0), ("fused", 64, 8, 0),
+                    ("fused", 128, 32, 0), ("two_sweeps", 128, 8, 0), ("two_sweeps", 256, 4, 0),
                     ("two_sweeps", 128, 4, 0), ("two_sweeps", 256, 4, 4))
 
 _cache: dict[str, tuple[int, int]] = {}

@@ -598,6 +598,9 @@ def batched_adjoint_cost(args) -> dict:
     cells = int(sum(spec["grid"].n_cells for spec in specs))
     inversion = DifferentiableBatch(specs, dtype=np.float32, max_steps=T)
     forward = RoomBatch([dict(spec, walls=start) for spec, start, _, _ in rooms], dtype=np.float32)
+    from ac_fdtd_b200.autotune import apply_tuned_batch
+
+    forward_geometry = apply_tuned_batch(forward)      # the fastest plain forward
     for r, (spec, start, source, receivers) in enumerate(rooms):
         for batch in (inversion.batch, forward):
             batch.add_volume_source(r, source, gaussian_pulse(T, batch.dt(r), 2000.0))
@@ -628,6 +631,8 @@ def batched_adjoint_cost(args) -> dict:
         "forward_ms": forward_ms, "gradient_ms": gradient_ms, "ratio": gradient_ms / forward_ms,
         "gradient_steps_per_s": 1000.0 / gradient_ms,
         "forward_gcups": cells * T / (forward_ms * 1e-3) / 1e9,
+        "forward_launch": {"scheme": forward_geometry[0], "block_threads": forward_geometry[1],
+                           "planes": forward_geometry[2], "ctas_per_sm": forward_geometry[3]},
     }
 
 
