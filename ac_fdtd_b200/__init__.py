@@ -17,6 +17,7 @@ from .boundaries import (
     reflection_coefficient,
 )
 from .grid import Grid, max_stable_time_step
+from .io import resample, write_wav
 from .medium import AIR, Medium
 from .room import ImpulseResponse, Room, simulate_impulse_response
 from .solver import CudaAcousticFDTD, pinned_array
@@ -46,5 +47,7 @@ __all__ = [
     "max_stable_time_step",
     "pinned_array",
     "reflection_coefficient",
+    "resample",
     "simulate_impulse_response",
+    "write_wav",
 ]

@@ -496,26 +496,29 @@ def batched_vs_per_room(args) -> dict:
     launches = batch.launch_count()
     batch.close()
 
-    solvers = []
-    for spec, source, receivers in rooms:
-        # each room on its own, in the scheme the batch runs
-        solver = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
-                                  air_absorption=spec["air_absorption"], scheme=batch_geometry[0])
-        solver.add_volume_source(source, gaussian_pulse(T, solver.dt, 2000.0))
-        for point in receivers:
-            solver.add_pressure_receiver(point)
-        solvers.append(solver)
+    # each room on its own, one after another, in each scheme; the faster one is the per-room arm
+    per_room = {}
+    for scheme in ("two_sweeps", "fused"):
+        solvers = []
+        for spec, source, receivers in rooms:
+            solver = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
+                                      air_absorption=spec["air_absorption"], scheme=scheme)
+            solver.add_volume_source(source, gaussian_pulse(T, solver.dt, 2000.0))
+            for point in receivers:
+                solver.add_pressure_receiver(point)
+            solvers.append(solver)
 
-    def run_rooms():
+        def run_rooms():
+            for solver in solvers:
+                solver.step_index = 0
+                solver.run(T)
+
+        for _ in range(max(1, args.warmup - 1)):
+            run_rooms()
+        per_room[scheme] = min(_device_ms(run_rooms, torch) for _ in range(2))
         for solver in solvers:
-            solver.step_index = 0
-            solver.run(T)
-
-    for _ in range(max(1, args.warmup - 1)):
-        run_rooms()
-    per_room_ms = min(_device_ms(run_rooms, torch) for _ in range(2))
-    for solver in solvers:
-        solver.close()
+            solver.close()
+    per_room_ms = min(per_room.values())
     peak, _ = measured_peak_hbm()
     batched_gcups = cells * T / (batch_ms * 1e-3) / 1e9
     return {
@@ -524,6 +527,7 @@ def batched_vs_per_room(args) -> dict:
                     f"receivers per room, {T} steps (CUDA graphs in both arms)",
         "batched_gcups": batched_gcups,
         "per_room_gcups": cells * T / (per_room_ms * 1e-3) / 1e9,
+        "per_room_gcups_by_scheme": {k: cells * T / (v * 1e-3) / 1e9 for k, v in per_room.items()},
         "speedup": per_room_ms / batch_ms,
         "batched_hbm_frac_of_measured": batched_gcups * (56 if batch_geometry[0] == "fused" else 72) / peak,
         "bytes_per_cell": 56 if batch_geometry[0] == "fused" else 72,

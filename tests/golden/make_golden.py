@@ -231,12 +231,49 @@ def make_impulse(ref_pkg) -> tuple[dict, dict]:
     return data, meta
 
 
-def main(reference: str = "/root/reference") -> None:
+def make_io(ref_pkg, scratch: Path) -> tuple[dict, dict]:
+    """The reference's export path: rational-ratio resampling from grid rates to audio rates,
+    and a WAV file written and read back."""
+    from scipy.io import wavfile
+
+    from ac_fdtd import io as ref_io
+
+    rng = np.random.default_rng(11)
+    signal = rng.standard_normal((3, 1200)) * np.exp(-np.arange(1200) / 300.0)
+    data = {"signal": signal}
+    cases = [(29716.4, 48000.0), (59432.7, 44100.0), (17150.0, 48000.0), (48000.0, 48000.0)]
+    for n, (source_rate, target_rate) in enumerate(cases):
+        data[f"resampled_{n}"] = ref_io.resample(signal, source_rate, target_rate)
+    path = ref_io.write_wav(scratch / "ir.wav", signal, 29716.4)
+    rate, written = wavfile.read(path)
+    data["wav"] = written
+    path = ref_io.write_wav(scratch / "raw.wav", signal[0], 29716.4, target_rate=None, normalise=False)
+    rate_raw, written_raw = wavfile.read(path)
+    data["wav_raw"] = written_raw
+    meta = {"cases": cases, "wav_rate": int(rate), "wav_raw_rate": int(rate_raw)}
+    return data, meta
+
+
+def main(reference: str = "/root/reference", *parts: str) -> None:
+    """Regenerate every fixture, or only the named parts (setup, trajectories, rooms, impulse,
+    io); golden.json keeps the entries of the parts not regenerated."""
     scratch = Path(tempfile.mkdtemp(prefix="acfdtd_ref_"))
     shutil.copytree(Path(reference) / "src", scratch / "src")
     sys.path.insert(0, str(scratch / "src"))
     import ac_fdtd as ref_pkg
     from ac_fdtd import c_backend
+
+    if parts:
+        meta = json.loads((HERE / "golden.json").read_text())
+        if "io" in parts:
+            io_data, meta["io"] = make_io(ref_pkg, scratch)
+            np.savez_compressed(HERE / "io.npz", **io_data)
+        unknown = set(parts) - {"io"}
+        if unknown:
+            raise SystemExit(f"only 'io' can be regenerated on its own, not {sorted(unknown)}")
+        (HERE / "golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
+        shutil.rmtree(scratch)
+        return
 
     setup, setup_meta = make_setup(ref_pkg)
     np.savez_compressed(HERE / "setup.npz", **setup)
@@ -246,8 +283,10 @@ def main(reference: str = "/root/reference") -> None:
     np.savez_compressed(HERE / "rooms.npz", **rooms)
     impulse, impulse_meta = make_impulse(ref_pkg)
     np.savez_compressed(HERE / "impulse.npz", **impulse)
+    io_data, io_meta = make_io(ref_pkg, scratch)
+    np.savez_compressed(HERE / "io.npz", **io_data)
     meta = {"setup": setup_meta, "trajectories": traj_meta, "rooms": rooms_meta,
-            "impulse": impulse_meta,
+            "impulse": impulse_meta, "io": io_meta,
             "generator": "tests/golden/make_golden.py", "numpy": np.__version__}
     (HERE / "golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     shutil.rmtree(scratch)
