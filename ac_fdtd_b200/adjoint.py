@@ -12,7 +12,8 @@ respect to
 
 Walls and sources need only the pressure history on the boundary cells, kept for every step of
 the forward run. The air needs the divergence and relaxation states of every cell at every
-step; those are recomputed segment by segment from full-state checkpoints taken every
+step. When that history fits in device memory the recorded run keeps it for every step;
+otherwise it is recomputed segment by segment from full-state checkpoints taken every
 ``checkpoint_every`` steps (default ceil(sqrt(T))), because the lossy scheme cannot be run
 backward stably. ``room_response`` exposes the same computation as a
 ``torch.autograd.Function``. The reference's solvers are not differentiable.
@@ -145,10 +146,12 @@ class DifferentiableRoom:
             if self.solver.n_relax == 0:
                 raise ValueError("air gradients need air absorption")
             flags |= _native.GRAD_AIR
-        self.checkpoint_every = int(checkpoint_every or math.ceil(math.sqrt(self.max_steps)))
         lib = self.solver._lib
+        # None: the library keeps the whole D/psi history when it fits in device memory (no
+        # recompute), else checkpoints every ceil(sqrt(max_steps)) steps.
         _native.check(lib.acf_adjoint_prepare(self.solver._handle, flags, self.max_steps,
-                                              self.checkpoint_every), "acf_adjoint_prepare")
+                                              int(checkpoint_every or 0)), "acf_adjoint_prepare")
+        self.checkpoint_every = int(lib.acf_adjoint_checkpoint_interval(self.solver._handle))
         self._shell_size = int(lib.acf_adjoint_shell_size(self.solver._handle))
         self.n_steps = 0
 

@@ -2056,6 +2056,8 @@ struct acf_batch {
         int64_t capacity = 0;        // steps a forward record may hold
         int32_t every = 0;           // checkpoint interval
         int64_t recorded = 0, step0 = 0;
+        bool fields_recorded = false;   // the recorded run wrote D and psi of every step itself
+        int direct_mode = -1;        // fields_recorded of the last recorded run (graph validity)
         int64_t shell_total = 0;
         int64_t face_off[6] = {};
         void *hist_shell = nullptr;  // capacity x shell_total pairs
@@ -3171,15 +3173,29 @@ int record_steps(acf_batch *b, acf_batch::Graph &g, const void *state, const His
 
 template <typename T>
 int forward_record_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
-    if (b->adj.step0 != step_offset) b->adj_graphs_dirty = true;
-    b->adj.recorded = n_steps;
-    b->adj.step0 = step_offset;
+    auto &A = b->adj;
+    if (A.step0 != step_offset) b->adj_graphs_dirty = true;
+    A.recorded = n_steps;
+    A.step0 = step_offset;
     History<T> hist = make_history<T>(b);
-    hist.shell = (T *)b->adj.hist_shell;
+    hist.shell = (T *)A.hist_shell;
     hist.shell_step0 = step_offset;
-    hist.shell_steps = b->adj.hist_shell ? b->adj.capacity : 0;
+    hist.shell_steps = A.hist_shell ? A.capacity : 0;
+    // One segment covers the whole run: the run itself keeps D and psi of every step, and the
+    // adjoint recomputes nothing (and needs no checkpoint).
+    const bool air = (A.flags & ACF_GRAD_AIR) && A.segment;
+    A.fields_recorded = air && n_steps <= A.every;
+    if (A.fields_recorded) {
+        hist.fields = (T *)A.segment;
+        hist.fields_step0 = step_offset;
+        hist.fields_slots = A.every;
+    }
+    if ((int)A.fields_recorded != A.direct_mode) {
+        b->adj_graphs_dirty = true;           // the record graph holds the history pointers
+        A.direct_mode = (int)A.fields_recorded;
+    }
     int rc = record_steps<T>(b, b->g_record, b->field_ptr(0, ACF_FIELD_P), hist, step_offset, n_steps,
-                             true, st, (b->adj.flags & ACF_GRAD_AIR) != 0);
+                             true, st, air && !A.fields_recorded);
     if (rc) return rc;
     ACF_CUDA(cudaGetLastError());
     return ACF_OK;
@@ -3299,7 +3315,7 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     for (int64_t seg = n_seg - 1; seg >= 0; seg--) {
         const int64_t s0 = A.step0 + seg * K;
         const int64_t s1 = std::min(s0 + K, A.step0 + n);
-        if (air) {
+        if (air && !A.fields_recorded) {
             // Recompute the segment from its checkpoint, keeping D and psi of every step.
             ACF_CUDA(cudaMemcpyAsync(A.scratch, (char *)A.checkpoints + seg * b->room_block_bytes(0),
                                      b->room_block_bytes(0), cudaMemcpyDeviceToDevice, st));
@@ -3343,10 +3359,21 @@ int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t ever
     if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
     if (b->rooms.size() != 1) return fail(ACF_ERR_STATE, "the adjoint is for single rooms");
     if (max_steps < 1) return fail(ACF_ERR_ARGUMENT, "max_steps must be >= 1");
-    if ((flags & ACF_GRAD_AIR) && (every < 1 || every > max_steps))
+    if ((flags & ACF_GRAD_AIR) && (every < 0 || every > max_steps))
         return fail(ACF_ERR_ARGUMENT, "checkpoint interval %d out of range", every);
     DeviceGuard guard(b->device);
     ACF_CUDA(cudaDeviceSynchronize());
+    if ((flags & ACF_GRAD_AIR) && every == 0) {
+        // Automatic: keep D and psi of every step when that history takes at most 60 % of the
+        // free device memory (the recorded run then writes it and nothing is recomputed), else
+        // checkpoints every ceil(sqrt(max_steps)) steps.
+        const RoomHost &h = b->rooms[0];
+        const double whole = (double)max_steps * (1 + h.n_relax) * h.field * b->elem();
+        size_t free_bytes = 0, total_bytes = 0;
+        ACF_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
+        every = whole <= 0.6 * (double)free_bytes ? (int32_t)std::min<int64_t>(max_steps, INT32_MAX)
+                                                   : (int32_t)std::ceil(std::sqrt((double)max_steps));
+    }
     auto &A = b->adj;
     b->adj_graphs_dirty = true;
     void **buffers[] = {&A.hist_shell, &A.checkpoints, &A.scratch, &A.segment, &A.fields};
@@ -3362,6 +3389,8 @@ int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t ever
     A.capacity = max_steps;
     A.every = (flags & ACF_GRAD_AIR) ? every : (int32_t)std::min<int64_t>(max_steps, INT32_MAX);
     A.recorded = 0;
+    A.fields_recorded = false;
+    A.direct_mode = -1;
     const int64_t sizes[6] = {(int64_t)h.ny * h.nz, (int64_t)h.ny * h.nz, (int64_t)h.nx * h.nz,
                               (int64_t)h.nx * h.nz, (int64_t)h.nx * h.ny, (int64_t)h.nx * h.ny};
     A.shell_total = 0;
@@ -3795,6 +3824,8 @@ int acf_adjoint_prepare(acf_solver *h, int32_t flags, int64_t max_steps, int32_t
 }
 
 int64_t acf_adjoint_shell_size(const acf_solver *h) { return h ? h->adj.shell_total : -1; }
+
+int32_t acf_adjoint_checkpoint_interval(const acf_solver *h) { return h ? h->adj.every : -1; }
 
 int acf_forward_record(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_stream stream) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");

@@ -545,6 +545,7 @@ def adjoint_cost(args) -> dict:
 
     from ac_fdtd_b200 import AirAbsorption, CudaAcousticFDTD, WallAdmittances, gaussian_pulse
     from ac_fdtd_b200.adjoint import DifferentiableRoom
+    from ac_fdtd_b200.autotune import apply_tuned
     from ac_fdtd_b200.workloads import differentiable_room
 
     T = args.adjoint_steps
@@ -556,6 +557,7 @@ def adjoint_cost(args) -> dict:
         wrt = ("signal", "walls") if air is None else ("signal", "walls", "air")
         forward = CudaAcousticFDTD(grid, dtype=np.float32, walls=WallAdmittances(*start_xi),
                                    air_absorption=air)
+        forward_launch = launch_dict(apply_tuned(forward))     # against the fastest forward
         room = DifferentiableRoom(grid, dtype=np.float32, walls=WallAdmittances(*true_xi),
                                   air_absorption=air, max_steps=T, wrt=wrt)
         signal = gaussian_pulse(T, room.dt, 2000.0)
@@ -580,7 +582,8 @@ def adjoint_cost(args) -> dict:
         gradient_ms = min(_device_ms(gradient, torch) for _ in range(3))
         out[label] = {"forward_ms": forward_ms, "gradient_ms": gradient_ms,
                       "ratio": gradient_ms / forward_ms,
-                      "checkpoint_every": room.checkpoint_every if air is not None else None}
+                      "checkpoint_every": room.checkpoint_every if air is not None else None,
+                      "forward_launch": forward_launch}
         forward.close()
         room.solver.close()
     return out

@@ -172,7 +172,9 @@ int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream 
  * linear in the state, so the backward recursion needs no forward state; parameter gradients
  * read a forward history: the pressure before the step and before the wall closed form on
  * every boundary cell (walls), and D and psi of every cell (air), recomputed segment by segment
- * from full-state checkpoints taken every `checkpoint_every` steps.
+ * from full-state checkpoints taken every `checkpoint_every` steps. checkpoint_every = 0 picks
+ * it: the whole run when D and psi of every step take at most 60 % of the free device memory
+ * -- the recorded run then keeps them and nothing is recomputed -- else ceil(sqrt(max_steps)).
  *
  * acf_adjoint_prepare  allocates the history for runs of up to max_steps steps.
  * acf_forward_record   is acf_run that also writes that history (and the checkpoints).
@@ -192,6 +194,8 @@ int acf_set_coefficients(acf_solver *solver, const acf_config *config);
 int acf_adjoint_prepare(acf_solver *solver, int32_t flags, int64_t max_steps,
                         int32_t checkpoint_every);
 int64_t acf_adjoint_shell_size(const acf_solver *solver);
+/* The checkpoint interval in use (after an automatic choice); -1 for a null solver. */
+int32_t acf_adjoint_checkpoint_interval(const acf_solver *solver);
 int acf_forward_record(acf_solver *solver, int64_t n_steps, int64_t step_offset,
                        acf_stream stream);
 int acf_adjoint_run(acf_solver *solver, const double *grad_rec, double *grad_src,

@@ -127,7 +127,7 @@ def test_patch_gradients_match_central_differences():
     assert np.max(np.abs(got - np.array(fds))) <= 1e-6 * np.max(np.abs(grads.walls)), (got, fds)
 
 
-@pytest.mark.parametrize("every", [7, 90])
+@pytest.mark.parametrize("every", [7, 90, None])
 def test_air_strength_gradients_match_central_differences(every):
     air = AirAbsorption(temperature=22.0, relative_humidity=35.0)
     room = make_room(air=air, wrt=("signal", "walls", "air"), every=every)
@@ -225,3 +225,21 @@ def test_differentiable_room_full_size_matches_central_differences():
     fds = np.array(fds)
     assert value > 0
     assert np.max(np.abs(grads.walls - fds)) <= 1e-6 * np.max(np.abs(fds)), (grads.walls, fds)
+
+
+def test_air_gradients_agree_with_and_without_recompute():
+    """Whole-run history (the recorded run keeps D and psi) and checkpoint recompute give the
+    same gradients bit for bit, also for a run shorter than the prepared capacity."""
+    air = AirAbsorption(temperature=19.0, relative_humidity=55.0)
+    results = []
+    for every in (STEPS, 9):
+        room = make_room(air=air, wrt=("signal", "walls", "air"), every=every)
+        assert room.checkpoint_every == every
+        w = weights(8, steps=STEPS - 13)
+        g = room.backward(w * room.forward(STEPS - 13))
+        results.append((g.strength, g.relaxation_time, g.walls, g.signal))
+        room.solver.close()
+    for a, b in zip(*results, strict=True):
+        np.testing.assert_array_equal(a, b)
+    auto = make_room(air=air, wrt=("signal", "walls", "air"))
+    assert auto.checkpoint_every == STEPS          # a small room's history always fits
