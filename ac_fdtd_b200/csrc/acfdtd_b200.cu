@@ -124,6 +124,8 @@ struct Room {
     int64_t src_stride;
     const int64_t *rec_off;        // padded offsets
     const int64_t *rec_start;      // first absolute step recorded
+    const int64_t *src_col;        // in-plane offsets (padded offset mod plane): j * pz + k
+    const int64_t *rec_col;
     T *rec;
     int64_t rec_stride, rec_origin;
 };
@@ -301,6 +303,73 @@ __device__ __forceinline__ bool wall_pair(const Room<T> &s, int i, int j, int k,
     return fp != T(0) || fu != T(1);
 }
 
+// Sources (bit q) and receivers (bit n_src + r) that lie in one (row j, chunk at k0) column,
+// found once per column so that the march visits them only at their own plane instead of
+// scanning every point at every plane. Beyond 32 points `all` is set and every point is
+// scanned, as before.
+template <typename T>
+__device__ __forceinline__ uint32_t column_points(const Room<T> &s, int j, int k0, bool &all) {
+    const int total = s.n_src + s.n_rec;
+    all = total > 32;
+    uint32_t mask = 0;
+    if (all) return 0;
+    const int64_t first = (int64_t)j * s.pz + k0;
+    for (int q = 0; q < total; q++) {
+        const int64_t col = q < s.n_src ? s.src_col[q] : s.rec_col[q - s.n_src];
+        if (col >= first && col < first + kVec) mask |= 1u << q;
+    }
+    return mask;
+}
+
+__device__ __forceinline__ uint32_t source_bits(uint32_t mask, int n_src) {
+    return n_src >= 32 ? mask : mask & ((1u << n_src) - 1u);
+}
+
+__device__ __forceinline__ uint32_t receiver_bits(uint32_t mask, int n_src) {
+    return n_src >= 32 ? 0u : mask >> n_src;
+}
+
+// Sources of the column's cell at `base`, after damping, in the order they were added
+// (scheme.py:293,360-363).
+template <typename T>
+__device__ __forceinline__ void add_sources(const Room<T> &s, uint32_t mask, bool all, int64_t base,
+                                            int k0, int64_t step, T Pn[kVec]) {
+    uint32_t m = all ? 0u : source_bits(mask, s.n_src);
+    for (int q = all ? 0 : -1; all ? q < s.n_src : m != 0; q++) {
+        if (!all) {
+            q = __ffs(m) - 1;
+            m &= m - 1;
+        }
+        const int64_t d = s.src_off[q] - base;
+        if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
+#pragma unroll
+            for (int e = 0; e < kVec; e++)
+                if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+        }
+    }
+}
+
+// Receivers of the column read the finished pressure (scheme.py:294-296).
+template <typename T>
+__device__ __forceinline__ void record_receivers(const Room<T> &s, uint32_t mask, bool all,
+                                                 int64_t base, int64_t step, const T Pn[kVec]) {
+    uint32_t m = all ? 0u : receiver_bits(mask, s.n_src);
+    for (int r = all ? 0 : -1; all ? r < s.n_rec : m != 0; r++) {
+        if (!all) {
+            r = __ffs(m) - 1;
+            m &= m - 1;
+        }
+        const int64_t d = s.rec_off[r] - base;
+        if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+            T v = Pn[0];
+#pragma unroll
+            for (int e = 1; e < kVec; e++)
+                if (e == d) v = Pn[e];
+            s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
+        }
+    }
+}
+
 template <typename T, bool LAYER, bool WALLS, int NR, bool REC = false>
 __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, int i_end, int j,
                                                 int c, int64_t step,
@@ -308,6 +377,12 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
     const int k0 = c * kVec;
     const bool any_point = (s.n_src | s.n_rec) != 0;
     const bool has_above = k0 + kVec <= s.nz;
+    bool all_points = false;
+    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    // The column touches a wall where its row or its chunk is on the boundary; planes 0 and
+    // nx - 1 are boundary planes for every column.
+    const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
 
     T fk[kVec];
     T fj = T(1);
@@ -355,6 +430,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
             }
         }
 
+        const bool boundary = wall_column || i == 0 || i == s.nx - 1;
         T Pn[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
@@ -371,7 +447,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
                 }
                 if (NR > 0) pe = pe + D[e] * s.relax_scale;
                 pe = pe - D[e] * cp;
-                if (REC && hist->shell) {
+                if (REC && hist->shell && boundary) {
                     int64_t idx;
                     const int f = shell_face(s, i, j, k, idx);
                     const int64_t slot = step - hist->shell_step0;
@@ -381,7 +457,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
                         h[1] = pe;
                     }
                 }
-                if (WALLS) {
+                if (WALLS && boundary) {
                     T fu, fp;
                     if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
                 }
@@ -394,36 +470,13 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
             Pn[e] = pe;
         }
 
-        // Sources after damping, in the order they were added (scheme.py:293,360-363).
-        if (any_point) {
-            for (int q = 0; q < s.n_src; q++) {
-                const int64_t d = s.src_off[q] - base;
-                if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
-#pragma unroll
-                    for (int e = 0; e < kVec; e++)
-                        if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
-                }
-            }
-        }
+        if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
 
         // ---- stores
         Vec4<T>::store(s.p + base, Pn);
 #pragma unroll
         for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, S[r]);
-
-        // Receivers read the finished p (scheme.py:294-296).
-        if (any_point) {
-            for (int r = 0; r < s.n_rec; r++) {
-                const int64_t d = s.rec_off[r] - base;
-                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
-                    T v = Pn[0];
-#pragma unroll
-                    for (int e = 1; e < kVec; e++)
-                        if (e == d) v = Pn[e];
-                    s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
-                }
-            }
-        }
+        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
 #pragma unroll
         for (int e = 0; e < kVec; e++) XL[e] = XH[e];
     }
@@ -464,6 +517,10 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
     const bool any_point = (s.n_src | s.n_rec) != 0;
     const int64_t column = (int64_t)j * s.pz + k0;
     const bool has_above = k0 + kVec < s.nz;   // p and vz at k0 + 4 are interior
+    bool all_points = false;
+    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
 
     // Layer profiles are read where used (L1-resident): holding the z profiles of the chunk
     // across the march would cost registers the load phase needs.
@@ -542,6 +599,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
                               LAYER ? __ldg(s.face[2] + min(k0 + kVec, s.nz)) : T(1));
 
         // ---- pressure, as the pressure sweep computes it
+        const bool boundary = wall_column || i == 0 || i == s.nx - 1;
         T Pn[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
@@ -561,7 +619,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
                 }
                 if (NR > 0) pe = pe + d * s.relax_scale;
                 pe = pe - d * cp;
-                if (WALLS) {
+                if (WALLS && boundary) {
                     T fu, fp;
                     if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
                 }
@@ -573,16 +631,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
             }
             Pn[e] = pe;
         }
-        if (any_point) {
-            for (int q = 0; q < s.n_src; q++) {
-                const int64_t d = s.src_off[q] - base;
-                if (d >= 0 && d < kVec && k0 + d < s.nz && step < s.src_len[q]) {
-#pragma unroll
-                    for (int e = 0; e < kVec; e++)
-                        if (e == d) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
-                }
-            }
-        }
+        if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
 
         // ---- stores: p, the three lower faces, the far boundary faces, psi in place. A z
         // element k == nz inside this chunk is the top face, already updated in ZL (no
@@ -599,19 +648,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
         if (k0 + kVec == s.nz) f.nvz[base + kVec] = ZH3;
 #pragma unroll
         for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, S[r]);
-
-        if (any_point) {
-            for (int r = 0; r < s.n_rec; r++) {
-                const int64_t d = s.rec_off[r] - base;
-                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
-                    T v = Pn[0];
-#pragma unroll
-                    for (int e = 1; e < kVec; e++)
-                        if (e == d) v = Pn[e];
-                    s.rec[r * s.rec_stride + (step - s.rec_origin)] = v;
-                }
-            }
-        }
+        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
             XL[e] = XH[e];
@@ -1420,6 +1457,10 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
     const int64_t column = (int64_t)j * s.pz + k0;
     const bool has_above = k0 + kVec <= s.nz;
     const T scp = s.relax_scale - s.cp;
+    bool all_points = false;
+    const uint32_t points = (s.n_src | s.n_rec) != 0 ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
     T XL[kVec];
     Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
     for (int i = i_begin; i < i_end; i++) {
@@ -1458,25 +1499,38 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
             dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
             LPn[e] = L[e] + s.cv * dmu;
         }
-        for (int r = 0; r < s.n_rec; r++) {
-            const int64_t d = s.rec_off[r] - base;
-            if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
-                const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
+        if (any_mine) {
+            uint32_t m = all_points ? 0u : receiver_bits(points, s.n_src);
+            for (int r = all_points ? 0 : -1; all_points ? r < s.n_rec : m != 0; r++) {
+                if (!all_points) {
+                    r = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.rec_off[r] - base;
+                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                    const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
 #pragma unroll
-                for (int e = 0; e < kVec; e++)
-                    if (e == d) LPn[e] = LPn[e] + g;
+                    for (int e = 0; e < kVec; e++)
+                        if (e == d) LPn[e] = LPn[e] + g;
+                }
+            }
+            m = all_points ? 0u : source_bits(points, s.n_src);
+            for (int q = all_points ? 0 : -1; all_points ? q < s.n_src : m != 0; q++) {
+                if (!all_points) {
+                    q = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.src_off[q] - base;
+                if (d >= 0 && d < kVec && step < s.src_len[q]) {
+                    T v = LPn[0];
+#pragma unroll
+                    for (int e = 1; e < kVec; e++)
+                        if (e == d) v = LPn[e];
+                    a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
+                }
             }
         }
-        for (int q = 0; q < s.n_src; q++) {
-            const int64_t d = s.src_off[q] - base;
-            if (d >= 0 && d < kVec && step < s.src_len[q]) {
-                T v = LPn[0];
-#pragma unroll
-                for (int e = 1; e < kVec; e++)
-                    if (e == d) v = LPn[e];
-                a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
-            }
-        }
+        const bool boundary = wall_column || i == 0 || i == s.nx - 1;
         T LD[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
@@ -1491,7 +1545,7 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
                 lph = lph * __ldg(s.cell[2] + k);
             }
             T lpt = lph, lpart = lph;
-            if (WALLS) {
+            if (WALLS && boundary) {
                 int64_t idx;
                 const int f = shell_face(s, i, j, k, idx);
                 if (f >= 0) {
@@ -2150,11 +2204,13 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     for (int f = 0; f < 6; f++) s.shell[f] = h.shell ? (const T *)h.shell + h.shell_off[f] : nullptr;
     s.n_src = (int32_t)h.n_src;
     s.src_off = h.src_off;
+    s.src_col = h.src_off ? h.src_off + h.n_src : nullptr;
     s.src_len = h.src_len;
     s.src_sig = (const T *)h.src_sig;
     s.src_stride = h.src_stride;
     s.n_rec = (int32_t)h.n_rec;
     s.rec_off = h.rec_off;
+    s.rec_col = h.rec_off ? h.rec_off + h.n_rec : nullptr;
     s.rec_start = h.rec_start;
     s.rec = (T *)h.rec;
     s.rec_stride = h.rec_capacity;
@@ -2829,9 +2885,11 @@ int set_sources(acf_batch *b, int room, int64_t n, const int64_t *cell, const in
     b->room_table_dirty = true;
     if (n == 0) return ACF_OK;
     const size_t es = b->elem();
-    ACF_CUDA(cudaMalloc(&h.src_off, n * sizeof(int64_t)));
+    // padded offsets, then their in-plane offsets
+    for (int64_t q = 0; q < n; q++) off.push_back(off[q] % h.plane);
+    ACF_CUDA(cudaMalloc(&h.src_off, 2 * n * sizeof(int64_t)));
     ACF_CUDA(cudaMalloc(&h.src_len, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMemcpy(h.src_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    ACF_CUDA(cudaMemcpy(h.src_off, off.data(), 2 * n * sizeof(int64_t), cudaMemcpyHostToDevice));
     ACF_CUDA(cudaMemcpy(h.src_len, len.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
     std::vector<double> host((size_t)n * (size_t)std::max<int64_t>(stride, 1), 0.0);
     if (stride > 0) std::copy(signal, signal + (size_t)n * stride, host.begin());
@@ -2886,9 +2944,10 @@ int set_receivers(acf_batch *b, int room, int64_t n, const int64_t *cell, const 
     b->room_table_dirty = true;
     h.host_rec_start.assign(start_step, start_step + n);
     if (n == 0) return ACF_OK;
-    ACF_CUDA(cudaMalloc(&h.rec_off, n * sizeof(int64_t)));
+    for (int64_t r = 0; r < n; r++) off.push_back(off[r] % h.plane);   // then in-plane offsets
+    ACF_CUDA(cudaMalloc(&h.rec_off, 2 * n * sizeof(int64_t)));
     ACF_CUDA(cudaMalloc(&h.rec_start, n * sizeof(int64_t)));
-    ACF_CUDA(cudaMemcpy(h.rec_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    ACF_CUDA(cudaMemcpy(h.rec_off, off.data(), 2 * n * sizeof(int64_t), cudaMemcpyHostToDevice));
     ACF_CUDA(cudaMemcpy(h.rec_start, start_step, n * sizeof(int64_t), cudaMemcpyHostToDevice));
     h.n_rec = n;
     return ACF_OK;
