@@ -3350,12 +3350,14 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     };
     // Steps [e - G, e) in reverse: graph locals are captured in launch order t = 0..G-1 and
     // reverse step base + (G - 1 - t).
+    // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter).
+    const int64_t chunk = air ? std::min<int64_t>(A.every, kAdjointChunk) : kAdjointChunk;
     auto reverse_range = [&](int64_t s0, int64_t e) -> int {
         int64_t end = e;
         while (end > s0) {
-            const int64_t G = std::min<int64_t>(air ? A.every : kAdjointChunk, end - s0);
+            const int64_t G = std::min<int64_t>(chunk, end - s0);
             set_step_base<<<1, 1, 0, st>>>(b->step_base, end - G);
-            if (G == (air ? A.every : kAdjointChunk)) {
+            if (G == chunk) {
                 int rc = replay(b, b->g_adjoint, G, 0, 1, st,
                                 [&](int32_t t, cudaStream_t s) { adjoint_step((int32_t)(G - 1 - t), s); });
                 if (rc) return rc;
@@ -3872,8 +3874,9 @@ int acf_set_coefficients(acf_solver *h, const acf_config *config) {
 int acf_reset_state(acf_solver *h, acf_stream stream) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
     DeviceGuard guard(h->device);
+    // The primary copy becomes current. No captured graph goes stale: the run graphs are kept
+    // per starting copy, and the adjoint's graphs always work on the primary copy.
     h->rooms[0].cur = 0;
-    h->graph_dirty = h->adj_graphs_dirty = true;
     ACF_CUDA(cudaMemsetAsync(h->field_ptr(0, ACF_FIELD_P), 0, h->room_block_bytes(0), (cudaStream_t)stream));
     return ACF_OK;
 }
