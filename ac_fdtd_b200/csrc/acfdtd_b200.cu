@@ -130,14 +130,15 @@ struct Room {
     int64_t rec_stride, rec_origin;
 };
 
-// Forward history kept for the adjoint (single rooms): per step, the pair (p^n, p-tilde^n) --
-// pressure before the step and before the wall closed form -- on every boundary cell, and, for a
+// Forward history kept for the adjoint: per step, p^n and p-tilde^n -- pressure before the step
+// and before the wall closed form -- on every boundary cell (two blocks of shell_total values,
+// first every p^n, then every p-tilde^n), and, for a
 // segment of steps, the divergence D^n and the relaxation states psi^n before their update.
 // Boundary cells are indexed as in the wall shells: the first face of FACES order a cell lies
 // on, then row-major over that face's two other axes; face f starts at face_off[f].
 template <typename T>
 struct History {
-    T *shell;                      // steps x shell_total pairs, or null
+    T *shell;                      // steps x 2 x shell_total values, or null
     int64_t shell_total, shell_step0, shell_steps;
     int64_t face_off[6];
     T *fields;                     // slots x (1 + n_relax) fields (padded geometry), or null;
@@ -370,6 +371,47 @@ __device__ __forceinline__ void record_receivers(const Room<T> &s, uint32_t mask
     }
 }
 
+// Boundary history of one step for the wall gradients: p^n and p before the wall closed form,
+// on every boundary cell, in two blocks of shell_total values per step (first p, then the other)
+// indexed as the wall shells are -- each cell on the first face of FACES order it lies on, then
+// row-major over that face's two other axes. A column on an x-face plane or a y-face row owns
+// contiguous entries for its whole chunk; elsewhere only its k = 0 and k = nz - 1 cells are on a
+// (z) face.
+template <typename T>
+__device__ __forceinline__ void record_shell(const Room<T> &s, const History<T> &hist, int i, int j,
+                                             int k0, int64_t step, const T P[kVec], const T PT[kVec]) {
+    const int64_t slot = step - hist.shell_step0;
+    if (slot < 0 || slot >= hist.shell_steps) return;
+    T *hp = hist.shell + slot * 2 * hist.shell_total;
+    T *ht = hp + hist.shell_total;
+    if (i == 0 || i == s.nx - 1 || j == 0 || j == s.ny - 1) {
+        const bool x_face = i == 0 || i == s.nx - 1;
+        const int f = x_face ? (i == 0 ? 0 : 1) : (j == 0 ? 2 : 3);
+        const int64_t at = hist.face_off[f] + (x_face ? (int64_t)j : (int64_t)i) * s.nz + k0;
+#pragma unroll
+        for (int e = 0; e < kVec; e++)
+            if (k0 + e < s.nz) {
+                hp[at + e] = P[e];
+                ht[at + e] = PT[e];
+            }
+        return;
+    }
+    const int64_t at = (int64_t)i * s.ny + j;
+    if (k0 == 0) {
+        hp[hist.face_off[4] + at] = P[0];
+        ht[hist.face_off[4] + at] = PT[0];
+    }
+    const int top = s.nz - 1 - k0;   // element of k = nz - 1, unless that cell is also k = 0
+    if (s.nz > 1 && top >= 0 && top < kVec) {
+#pragma unroll
+        for (int e = 0; e < kVec; e++)
+            if (e == top) {
+                hp[hist.face_off[5] + at] = P[e];
+                ht[hist.face_off[5] + at] = PT[e];
+            }
+    }
+}
+
 template <typename T, bool LAYER, bool WALLS, int NR, bool REC = false>
 __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, int i_end, int j,
                                                 int c, int64_t step,
@@ -431,11 +473,12 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
         }
 
         const bool boundary = wall_column || i == 0 || i == s.nx - 1;
-        T Pn[kVec];
+        T Pn[kVec], PT[kVec];   // PT: p before the wall closed form (recorded runs)
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
             const int k = k0 + e;
             T pe = P[e];
+            PT[e] = T(0);
             if (k < s.nz) {
                 // relaxation states (scheme.py:337-358), then p -= c_p div (scheme.py:325-326)
 #pragma unroll
@@ -447,16 +490,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
                 }
                 if (NR > 0) pe = pe + D[e] * s.relax_scale;
                 pe = pe - D[e] * cp;
-                if (REC && hist->shell && boundary) {
-                    int64_t idx;
-                    const int f = shell_face(s, i, j, k, idx);
-                    const int64_t slot = step - hist->shell_step0;
-                    if (f >= 0 && slot >= 0 && slot < hist->shell_steps) {
-                        T *h = hist->shell + 2 * (slot * hist->shell_total + hist->face_off[f] + idx);
-                        h[0] = P[e];
-                        h[1] = pe;
-                    }
-                }
+                if (REC) PT[e] = pe;
                 if (WALLS && boundary) {
                     T fu, fp;
                     if (wall_pair(s, i, j, k, fu, fp)) pe = pe * fu - P[e] * fp;
@@ -470,6 +504,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
             Pn[e] = pe;
         }
 
+        if (REC && hist->shell && boundary) record_shell(s, *hist, i, j, k0, step, P, PT);
         if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
 
         // ---- stores
@@ -1554,11 +1589,11 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
                     lpt = u * lph;
                     lpart = lpt - q * lph;
                     if (a.grad_shell) {
-                        const T *h = a.hist.shell + 2 * ((step - a.hist.shell_step0) * a.hist.shell_total +
-                                                         a.hist.face_off[f] + idx);
+                        const T *h = a.hist.shell + (step - a.hist.shell_step0) * 2 * a.hist.shell_total +
+                                     a.hist.face_off[f] + idx;
                         const double uu = (double)u;
                         a.grad_shell[a.hist.face_off[f] + idx] +=
-                            -(double)lph * uu * uu * ((double)h[1] + (double)h[0]);
+                            -(double)lph * uu * uu * ((double)h[a.hist.shell_total] + (double)h[0]);
                     }
                 }
             }
@@ -2114,7 +2149,7 @@ struct acf_batch {
         int direct_mode = -1;        // fields_recorded of the last recorded run (graph validity)
         int64_t shell_total = 0;
         int64_t face_off[6] = {};
-        void *hist_shell = nullptr;  // capacity x shell_total pairs
+        void *hist_shell = nullptr;  // capacity x 2 x shell_total values
         void *checkpoints = nullptr; // ceil(capacity / every) room states
         void *scratch = nullptr;     // recompute state
         void *segment = nullptr;     // every x (1 + n_relax) fields
