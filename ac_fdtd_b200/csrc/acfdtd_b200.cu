@@ -1479,11 +1479,30 @@ struct AdjointParams {
     int32_t local_step;
     int32_t planes;
     int32_t air;                   // accumulate air gradients (needs hist.fields)
+    // Fused adjoint step only: mu^{n+1} and lambda_D^n go to these (the other copies); lvx..lvz
+    // hold mu^{n+2} and ld holds lambda_D^{n+1}.
+    T *out_vx, *out_vy, *out_vz, *out_d;
 };
+
+// mu on a face: (LV + (lambda_D[lower cell] - lambda_D[upper cell])) g_a g_b g_c, the face
+// sweep's arithmetic, with lambda_D = 0 outside the room (x - 0 == x exactly, so the far faces'
+// LV + lambda_D[lower] is reproduced bit for bit).
+template <typename T, bool LAYER>
+__device__ __forceinline__ T adjoint_face(T lv, T d_lower, T d_upper, T ga, T gb, T gc) {
+    T m = lv + (d_lower - d_upper);
+    if (LAYER) m = ((m * ga) * gb) * gc;
+    return m;
+}
 
 // One (row j, chunk c) column of the adjoint pressure sweep over planes [i_begin, i_end),
 // reversing forward step `step`; air-gradient terms are added to `air_acc`.
-template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
+//
+// FUSED also performs the face sweep of the step after (forward step + 1) first: mu^{n+1} on the
+// cell's six faces from mu^{n+2} (lvx..lvz) and lambda_D^{n+1} (ld) -- its own three lower faces
+// (stored, with the far boundary faces) and its three upper faces (recomputed exactly as their
+// owners compute them) -- and writes lambda_D^n to out_d. Per cell and step this moves (10 + 2R)
+// elements instead of the two sweeps' (13 + 2R), with the same results.
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR, bool FUSED = false>
 __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &a, int i_begin,
                                                         int i_end, int j, int c, int64_t step,
                                                         T *air_acc) {
@@ -1497,15 +1516,93 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
     const bool any_mine = points != 0 || all_points;
     const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
     T XL[kVec];
-    Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
+    // FUSED: lambda_D^{n+1} of the current cell and of the cell below in x, carried along x
+    T Dc[kVec], Dm[kVec];
+    T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
+    if (FUSED) {
+        const int64_t b0 = (int64_t)i_begin * s.plane + column;
+        Vec4<T>::ldg(a.ld + b0, Dc);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Dm[e] = T(0);
+        if (i_begin > 0) Vec4<T>::ldg(a.ld + b0 - s.plane, Dm);
+        if (LAYER) {
+            fj_cell = __ldg(s.cell[1] + j);
+            fj_face = __ldg(s.face[1] + j);
+            fj1_face = __ldg(s.face[1] + j + 1);
+        }
+        T V[kVec];
+        Vec4<T>::ldg(a.lvx + b0, V);
+        const T fi_face = LAYER ? __ldg(s.face[0] + i_begin) : T(1);
+#pragma unroll
+        for (int e = 0; e < kVec; e++)
+            XL[e] = k0 + e < s.nz ? adjoint_face<T, LAYER>(V[e], Dm[e], Dc[e], fi_face, fj_cell,
+                                                           LAYER ? __ldg(s.cell[2] + k0 + e) : T(1))
+                                  : V[e];
+    } else {
+        Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
+    }
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
         T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
-        Vec4<T>::ldg(a.lvx + base + s.plane, XH);
-        Vec4<T>::ldg(a.lvy + base, YL);
-        Vec4<T>::ldg(a.lvy + base + s.pz, YH);
-        Vec4<T>::ldg(a.lvz + base, Z);
-        const T above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+        T above;
+        T Dxp[kVec];   // FUSED: lambda_D^{n+1} of the next plane
+        if (FUSED) {
+            T Dy[kVec], Dyp[kVec], VXp[kVec], VY[kVec], VYp[kVec], VZ[kVec];
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                Dxp[e] = T(0);
+                Dy[e] = T(0);
+                Dyp[e] = T(0);
+            }
+            if (i + 1 < s.nx) Vec4<T>::ldg(a.ld + base + s.plane, Dxp);
+            if (j > 0) Vec4<T>::ldg(a.ld + base - s.pz, Dy);
+            if (j + 1 < s.ny) Vec4<T>::ldg(a.ld + base + s.pz, Dyp);
+            const T d_below = k0 > 0 ? __ldg(a.ld + base - 1) : T(0);
+            const T d_above = k0 + kVec < s.nz ? __ldg(a.ld + base + kVec) : T(0);
+            Vec4<T>::ldg(a.lvx + base + s.plane, VXp);
+            Vec4<T>::ldg(a.lvy + base, VY);
+            Vec4<T>::ldg(a.lvy + base + s.pz, VYp);
+            Vec4<T>::ldg(a.lvz + base, VZ);
+            const T vz_above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+            T fi_cell = T(1), fi1_face = T(1);
+            if (LAYER) {
+                fi_cell = __ldg(s.cell[0] + i);
+                fi1_face = __ldg(s.face[0] + i + 1);
+            }
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                const int k = k0 + e;
+                const T gk_cell = LAYER ? __ldg(s.cell[2] + min(k, s.nz - 1)) : T(1);
+                if (k < s.nz) {
+                    XH[e] = adjoint_face<T, LAYER>(VXp[e], Dc[e], Dxp[e], fi1_face, fj_cell, gk_cell);
+                    YL[e] = adjoint_face<T, LAYER>(VY[e], Dy[e], Dc[e], fi_cell, fj_face, gk_cell);
+                    YH[e] = adjoint_face<T, LAYER>(VYp[e], Dc[e], Dyp[e], fi_cell, fj1_face, gk_cell);
+                } else {
+                    XH[e] = VXp[e];
+                    YL[e] = VY[e];
+                    YH[e] = VYp[e];
+                }
+                // z face k: between cells k - 1 and k; the top face k = nz has only the lower one
+                if (k <= s.nz) {
+                    const T lower = k > 0 ? (e == 0 ? d_below : Dc[e - 1]) : T(0);
+                    const T upper = k < s.nz ? Dc[e] : T(0);
+                    Z[e] = adjoint_face<T, LAYER>(VZ[e], lower, upper, fi_cell, fj_cell,
+                                                  LAYER ? __ldg(s.face[2] + k) : T(1));
+                } else {
+                    Z[e] = VZ[e];
+                }
+            }
+            above = T(0);
+            if (has_above)
+                above = adjoint_face<T, LAYER>(vz_above, Dc[kVec - 1], d_above, fi_cell, fj_cell,
+                                               LAYER ? __ldg(s.face[2] + k0 + kVec) : T(1));
+        } else {
+            Vec4<T>::ldg(a.lvx + base + s.plane, XH);
+            Vec4<T>::ldg(a.lvy + base, YL);
+            Vec4<T>::ldg(a.lvy + base + s.pz, YH);
+            Vec4<T>::ldg(a.lvz + base, Z);
+            above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+        }
         Vec4<T>::load(a.lp + base, L);
 #pragma unroll
         for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
@@ -1616,9 +1713,24 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
             LD[e] = ld;
         }
         Vec4<T>::store(a.lp + base, L);
-        Vec4<T>::store(a.ld + base, LD);
 #pragma unroll
         for (int r = 0; r < NR; r++) Vec4<T>::store(a.lpsi + r * s.field + base, LS[r]);
+        if (FUSED) {
+            Vec4<T>::store(a.out_d + base, LD);
+            Vec4<T>::store(a.out_vx + base, XL);
+            Vec4<T>::store(a.out_vy + base, YL);
+            Vec4<T>::store(a.out_vz + base, Z);
+            if (i == s.nx - 1) Vec4<T>::store(a.out_vx + base + s.plane, XH);
+            if (j == s.ny - 1) Vec4<T>::store(a.out_vy + base + s.pz, YH);
+            if (k0 + kVec == s.nz) a.out_vz[base + kVec] = above;
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                Dm[e] = Dc[e];
+                Dc[e] = Dxp[e];
+            }
+        } else {
+            Vec4<T>::store(a.ld + base, LD);
+        }
 #pragma unroll
         for (int e = 0; e < kVec; e++) XL[e] = XH[e];
     }
@@ -1638,6 +1750,44 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 
     if (c < a.room.nchunks && j < a.room.ny) {
         const int i_begin = blockIdx.z * a.planes;
         adjoint_pressure_column<T, LAYER, WALLS, NR, AIR>(a, i_begin, min(a.room.nx, i_begin + a.planes),
+                                                          j, c, *a.step_base + a.local_step, air_acc);
+    }
+    if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
+        __shared__ double red[NA][8];
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+        const int lane = tid & 31, warp = tid >> 5;
+        const int n_warps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+        for (int t = 0; t < NA; t++) {
+            double v = (double)air_acc[t];
+            for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+            if (lane == 0) red[t][warp] = v;
+        }
+        __syncthreads();
+        if (tid < NA) {
+            double v = 0.0;
+            for (int w = 0; w < n_warps; w++) v += red[tid][w];
+            const int64_t block = ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            a.air_partials[block * NA + tid] += v;
+        }
+    }
+}
+
+// The face sweep of forward step n + 1 and the cell sweep of step n in one launch (FUSED above).
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 2 : 3)))
+    adjoint_fused_sweep(const AdjointParams<T> a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    constexpr int NA = 3 * NR + 1;
+    // Per-thread sums over this launch's few cells in the working precision; the block sums
+    // and the sums across blocks and steps are FP64.
+    T air_acc[NA];
+#pragma unroll
+    for (int t = 0; t < NA; t++) air_acc[t] = T(0);
+    if (c < a.room.nchunks && j < a.room.ny) {
+        const int i_begin = blockIdx.z * a.planes;
+        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR, true>(a, i_begin, min(a.room.nx, i_begin + a.planes),
                                                           j, c, *a.step_base + a.local_step, air_acc);
     }
     if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
@@ -2136,7 +2286,7 @@ struct acf_batch {
             exec = nullptr;
         }
     };
-    Graph g_record, g_recompute, g_adjoint;
+    Graph g_record, g_recompute, g_adjoint, g_adjoint_odd;   // adjoint: per starting copy
     bool adj_graphs_dirty = true;
 
     // adjoint (single rooms)
@@ -2154,6 +2304,7 @@ struct acf_batch {
         void *scratch = nullptr;     // recompute state
         void *segment = nullptr;     // every x (1 + n_relax) fields
         void *fields = nullptr;      // (5 + n_relax) adjoint fields
+        void *fields2 = nullptr;     // the fused adjoint's second copy of mu (3 fields), lambda_D
         double *grad_shell = nullptr;
         double *air_partials = nullptr;
         int64_t air_blocks = 0;
@@ -2714,6 +2865,7 @@ void free_batch(acf_batch *b) {
     b->g_record.release();
     b->g_recompute.release();
     b->g_adjoint.release();
+    b->g_adjoint_odd.release();
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     for (auto &e : b->ring)
         if (e) cudaEventDestroy(e);
@@ -2723,6 +2875,7 @@ void free_batch(acf_batch *b) {
     cudaFree(b->adj.scratch);
     cudaFree(b->adj.segment);
     cudaFree(b->adj.fields);
+    cudaFree(b->adj.fields2);
     cudaFree(b->adj.grad_shell);
     cudaFree(b->adj.air_partials);
     cudaFree(b->adj.grad_rec);
@@ -3176,6 +3329,21 @@ struct AdjPressureAir {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct AdjFused {
+    static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        adjoint_fused_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct AdjFusedAir {
+    static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        if (NR > 0) adjoint_fused_sweep<T, L, W, NR, NR != 0><<<g, b, 0, st>>>(p);
+        else adjoint_fused_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
+    }
+};
+
 template <typename T>
 History<T> make_history(const acf_batch *b) {
     History<T> h{};
@@ -3194,6 +3362,7 @@ int replay(acf_batch *b, acf_batch::Graph &g, int64_t chunk, int64_t bump, int64
         b->g_record.release();
         b->g_recompute.release();
         b->g_adjoint.release();
+        b->g_adjoint_odd.release();
         b->adj_graphs_dirty = false;
     }
     if (!g.exec || g.steps != chunk) {
@@ -3374,33 +3543,67 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     a.planes = b->planes;
     a.air = air ? 1 : 0;
 
-    // One adjoint step per call: reverse forward step *step_base + local.
-    auto adjoint_step = [&](int32_t local, cudaStream_t s) {
-        AdjointParams<T> q = a;
+    // The reversed steps, last first. The last recorded step is a cell sweep alone (mu^{n+1} = 0);
+    // every earlier step n is one fused launch -- the face sweep of step n + 1, then the cell sweep
+    // of step n -- reading mu and lambda_D from one copy and writing them to the other; the face
+    // sweep of the first step closes the run. a0 reads copy 0 (the adjoint fields) and writes
+    // copy 1 (fields2); a1 the reverse.
+    AdjointParams<T> a0 = a, a1 = a;
+    {
+        T *g2 = (T *)A.fields2;
+        a0.out_vx = g2;
+        a0.out_vy = g2 + h.field;
+        a0.out_vz = g2 + 2 * h.field;
+        a0.out_d = g2 + 3 * h.field;
+        a1.lvx = a0.out_vx;
+        a1.lvy = a0.out_vy;
+        a1.lvz = a0.out_vz;
+        a1.ld = a0.out_d;
+        a1.out_vx = a.lvx;
+        a1.out_vy = a.lvy;
+        a1.out_vz = a.lvz;
+        a1.out_d = a.ld;
+    }
+    int parity = 0;       // the copy holding the latest mu and lambda_D
+    bool first = true;
+    auto fused_unit = [&](int32_t local, cudaStream_t s, int par) {
+        AdjointParams<T> q = par ? a1 : a0;
         q.local_step = local;
-        if (air) dispatch_pressure<T, AdjPressureAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
-        else dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
-        if (h.has_layer) adjoint_velocity_sweep<T, true><<<L.grid, L.block, 0, s>>>(q);
-        else adjoint_velocity_sweep<T, false><<<L.grid, L.block, 0, s>>>(q);
+        if (air) dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        else dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
     };
-    // Steps [e - G, e) in reverse: graph locals are captured in launch order t = 0..G-1 and
-    // reverse step base + (G - 1 - t).
-    // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter).
+    // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter),
+    // one graph per starting copy. Steps [e - G, e) in reverse: graph locals are captured in
+    // launch order t = 0..G-1 and reverse step base + (G - 1 - t).
     const int64_t chunk = air ? std::min<int64_t>(A.every, kAdjointChunk) : kAdjointChunk;
     auto reverse_range = [&](int64_t s0, int64_t e) -> int {
         int64_t end = e;
+        if (first && end > s0) {
+            set_step_base<<<1, 1, 0, st>>>(b->step_base, end - 1);
+            AdjointParams<T> q = a0;
+            q.local_step = 0;
+            if (air) dispatch_pressure<T, AdjPressureAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, st);
+            else dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, st);
+            b->launches += 2;
+            end -= 1;
+            first = false;
+        }
         while (end > s0) {
             const int64_t G = std::min<int64_t>(chunk, end - s0);
             set_step_base<<<1, 1, 0, st>>>(b->step_base, end - G);
+            const int p0 = parity;
             if (G == chunk) {
-                int rc = replay(b, b->g_adjoint, G, 0, 1, st,
-                                [&](int32_t t, cudaStream_t s) { adjoint_step((int32_t)(G - 1 - t), s); });
+                int rc = replay(b, p0 ? b->g_adjoint_odd : b->g_adjoint, G, 0, 1, st,
+                                [&](int32_t t, cudaStream_t s) {
+                                    fused_unit((int32_t)(G - 1 - t), s, p0 ^ (int)(t & 1));
+                                });
                 if (rc) return rc;
-                b->launches += 2 * G + 2;
+                b->launches += G + 2;
             } else {
-                for (int64_t t = 0; t < G; t++) adjoint_step((int32_t)(G - 1 - t), st);
-                b->launches += 2 * G + 1;
+                for (int64_t t = 0; t < G; t++) fused_unit((int32_t)(G - 1 - t), st, p0 ^ (int)(t & 1));
+                b->launches += G + 1;
             }
+            parity ^= (int)(G & 1);
             end -= G;
         }
         return ACF_OK;
@@ -3424,6 +3627,19 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
         }
         int rc = reverse_range(s0, s1);
         if (rc) return rc;
+    }
+    // The face sweep of the first recorded step, in place, then mu and lambda_D back in the
+    // adjoint fields if they ended in the second copy.
+    {
+        AdjointParams<T> q = parity ? a1 : a0;
+        q.local_step = 0;
+        if (h.has_layer) adjoint_velocity_sweep<T, true><<<L.grid, L.block, 0, st>>>(q);
+        else adjoint_velocity_sweep<T, false><<<L.grid, L.block, 0, st>>>(q);
+        b->launches += 1;
+        if (parity) {
+            ACF_CUDA(cudaMemcpyAsync(a.lvx, a0.out_vx, (size_t)3 * h.field * es, cudaMemcpyDeviceToDevice, st));
+            ACF_CUDA(cudaMemcpyAsync(a.ld, a0.out_d, (size_t)h.field * es, cudaMemcpyDeviceToDevice, st));
+        }
     }
     a.local_step = 0;
     adjoint_finish<T><<<L.grid, L.block, 0, st>>>(a);
@@ -3472,7 +3688,7 @@ int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t ever
     }
     auto &A = b->adj;
     b->adj_graphs_dirty = true;
-    void **buffers[] = {&A.hist_shell, &A.checkpoints, &A.scratch, &A.segment, &A.fields};
+    void **buffers[] = {&A.hist_shell, &A.checkpoints, &A.scratch, &A.segment, &A.fields, &A.fields2};
     for (void **p : buffers) {
         cudaFree(*p);
         *p = nullptr;
@@ -3496,6 +3712,9 @@ int adjoint_prepare(acf_batch *b, int32_t flags, int64_t max_steps, int32_t ever
     }
     const size_t adj_bytes = ((size_t)(5 + h.n_relax) * h.field + h.pz) * es;
     ACF_CUDA(cudaMalloc(&A.fields, adj_bytes));
+    const size_t second = ((size_t)4 * h.field + h.pz) * es;
+    ACF_CUDA(cudaMalloc(&A.fields2, second));
+    ACF_CUDA(cudaMemset(A.fields2, 0, second));
     if ((flags & ACF_GRAD_WALLS) && h.has_walls) {
         const size_t bytes = (size_t)max_steps * A.shell_total * 2 * es;
         if (cudaMalloc(&A.hist_shell, bytes) != cudaSuccess)
