@@ -557,34 +557,14 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
     const bool any_mine = points != 0 || all_points;
     const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
 
-    // Layer profiles along y and z are fixed for the whole march. In single precision the z
-    // profiles are held in registers (measured 2-3 % faster at 384^3); in double precision that
-    // would spill, so they are read where used (L1-resident).
-    constexpr bool hold_z = sizeof(T) == 4;
+    // Layer profiles are read where used (L1-resident): holding the z profiles of the chunk
+    // across the march would cost registers the load phase needs.
     T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
-    T fkc[kVec], fkf[kVec + 1];
-#pragma unroll
-    for (int e = 0; e < kVec; e++) fkc[e] = T(1);
-#pragma unroll
-    for (int e = 0; e <= kVec; e++) fkf[e] = T(1);
     if (LAYER) {
         fj_cell = __ldg(s.cell[1] + j);
         fj_face = __ldg(s.face[1] + j);
         fj1_face = __ldg(s.face[1] + j + 1);
-        if (hold_z) {
-#pragma unroll
-            for (int e = 0; e < kVec; e++) fkc[e] = __ldg(s.cell[2] + min(k0 + e, s.nz - 1));
-#pragma unroll
-            for (int e = 0; e <= kVec; e++) fkf[e] = __ldg(s.face[2] + min(k0 + e, s.nz));
-        }
     }
-    // z profile of element e's cell and of its lower z face (e = kVec: the face above the chunk)
-    auto zc = [&](int e) -> T {
-        return !LAYER ? T(1) : hold_z ? fkc[e] : __ldg(s.cell[2] + min(k0 + e, s.nz - 1));
-    };
-    auto zf = [&](int e) -> T {
-        return !LAYER ? T(1) : hold_z ? fkf[e] : __ldg(s.face[2] + min(k0 + e, s.nz));
-    };
 
     // Carried from plane to plane: p(i) and the updated vx on face i.
     T P[kVec], XL[kVec];
@@ -599,7 +579,8 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
         for (int e = 0; e < kVec; e++) {
             T v = V[e];
             if (i_begin > 0) v = v - cv * (P[e] - Q[e]);
-            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell, zc(e));
+            XL[e] = damp3<T, LAYER>(v, fi_face, fj_cell,
+                                    LAYER ? __ldg(s.cell[2] + min(k0 + e, s.nz - 1)) : T(1));
         }
     }
 
@@ -630,25 +611,27 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
         T XH[kVec], YL[kVec], YH[kVec], ZL[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
-            const T fkc_e = zc(e);
+            const T fkc = LAYER ? __ldg(s.cell[2] + min(k0 + e, s.nz - 1)) : T(1);
             T v = VXo[e];
             if (x_inner) v = v - cv * (PX[e] - P[e]);
-            XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc_e);
+            XH[e] = damp3<T, LAYER>(v, fi1_face, fj_cell, fkc);
             v = VY[e];
             if (j > 0) v = v - cv * (P[e] - PYm[e]);
-            YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc_e);
+            YL[e] = damp3<T, LAYER>(v, fi_cell, fj_face, fkc);
             v = VYp[e];
             if (j + 1 < s.ny) v = v - cv * (PYp[e] - P[e]);
-            YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc_e);
+            YH[e] = damp3<T, LAYER>(v, fi_cell, fj1_face, fkc);
             const int k = k0 + e;
             v = VZ[e];
             if (k > 0 && k < s.nz) v = v - cv * (P[e] - (e == 0 ? p_below : P[e - 1]));
-            ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell, zf(e));
+            ZL[e] = damp3<T, LAYER>(v, fi_cell, fj_cell,
+                                    LAYER ? __ldg(s.face[2] + min(k0 + e, s.nz)) : T(1));
         }
         // z face k0 + 4: the next chunk's first lower face, or the top face z = nz.
         T ZH3 = vz_above;
         if (has_above) ZH3 = ZH3 - cv * (p_above - P[kVec - 1]);
-        ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell, zf(kVec));
+        ZH3 = damp3<T, LAYER>(ZH3, fi_cell, fj_cell,
+                              LAYER ? __ldg(s.face[2] + min(k0 + kVec, s.nz)) : T(1));
 
         // ---- pressure, as the pressure sweep computes it
         const bool boundary = wall_column || i == 0 || i == s.nx - 1;
@@ -678,7 +661,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
                 if (LAYER) {
                     pe = pe * fi_cell;
                     pe = pe * fj_cell;
-                    pe = pe * zc(e);
+                    pe = pe * __ldg(s.cell[2] + k);
                 }
             }
             Pn[e] = pe;
