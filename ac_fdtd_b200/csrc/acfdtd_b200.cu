@@ -1972,6 +1972,32 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 3)) adjoint_pressur
     }
 }
 
+// The fused adjoint step (face sweep of forward step n + 1, cell sweep of step n) over a batch:
+// each room's parameters name the copy of mu and lambda_D it reads and the one it writes.
+template <typename T, bool LAYER, bool WALLS, int NR>
+__global__ void __maxnreg__(sizeof(T) == 8 ? 168 : 96) adjoint_fused_batch(const BatchAdjointParams<T> b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(AdjointParams<T>)];
+    AdjointParams<T> *room = reinterpret_cast<AdjointParams<T> *>(raw);
+    const int64_t step = *b.step_base + b.local_step;
+    T unused[1];
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            stage_adjoint(b.rooms + tile.room, room);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            adjoint_pressure_column<T, LAYER, WALLS, NR, false, true>(*room, tile.i_begin, tile.i_end,
+                                                                      pair / room->room.nchunks,
+                                                                      pair % room->room.nchunks, step, unused);
+        }
+    }
+}
+
 template <typename T, bool LAYER>
 __global__ void __launch_bounds__(256, 3) adjoint_velocity_batch(const BatchAdjointParams<T> b) {
     __shared__ __align__(16) unsigned char raw[sizeof(AdjointParams<T>)];
@@ -2315,12 +2341,13 @@ struct acf_batch {
     // adjoint of a batch of rooms (walls and sources): per-room history and adjoint fields
     struct RoomAdjoint {
         void *hist_shell = nullptr, *fields = nullptr;
+        void *fields2 = nullptr;     // second copy of mu (3 fields) and lambda_D for the fused step
         double *grad_shell = nullptr, *grad_rec = nullptr, *grad_src = nullptr;
         int64_t shell_total = 0, face_off[6] = {}, rows_rec = 0, rows_src = 0;
     };
     std::vector<RoomAdjoint> badj;
     int64_t badj_capacity = 0, badj_recorded = 0, badj_step0 = 0;
-    void *badj_table = nullptr;      // device array of AdjointParams<T>, one per room
+    void *badj_table = nullptr;      // device array of AdjointParams<T>: 2 per room (the two copies of mu)
 
     size_t elem() const { return (size_t)precision; }
     int n_fields() const { return 4 + n_relax; }
@@ -2883,6 +2910,7 @@ void free_batch(acf_batch *b) {
     for (auto &ra : b->badj) {
         cudaFree(ra.hist_shell);
         cudaFree(ra.fields);
+        cudaFree(ra.fields2);
         cudaFree(ra.grad_shell);
         cudaFree(ra.grad_rec);
         cudaFree(ra.grad_src);
@@ -3810,6 +3838,13 @@ struct BatchAdjPressure {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct BatchAdjFused {
+    static void launch(const BatchAdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
+        adjoint_fused_batch<T, L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
 int batch_adjoint_prepare(acf_batch *b, int64_t max_steps) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null batch");
     if (max_steps < 1) return fail(ACF_ERR_ARGUMENT, "max_steps must be >= 1");
@@ -3819,6 +3854,7 @@ int batch_adjoint_prepare(acf_batch *b, int64_t max_steps) {
     for (auto &ra : b->badj) {
         cudaFree(ra.hist_shell);
         cudaFree(ra.fields);
+        cudaFree(ra.fields2);
         cudaFree(ra.grad_shell);
         cudaFree(ra.grad_rec);
         cudaFree(ra.grad_src);
@@ -3838,6 +3874,8 @@ int batch_adjoint_prepare(acf_batch *b, int64_t max_steps) {
         if (cudaMalloc(&ra.hist_shell, hist) != cudaSuccess)
             return fail(ACF_ERR_MEMORY, "room %zu: cudaMalloc of %zu bytes of wall history failed", r, hist);
         ACF_CUDA(cudaMalloc(&ra.fields, ((size_t)(5 + h.n_relax) * h.field + h.pz) * es));
+        ACF_CUDA(cudaMalloc(&ra.fields2, ((size_t)4 * h.field + h.pz) * es));
+        ACF_CUDA(cudaMemset(ra.fields2, 0, ((size_t)4 * h.field + h.pz) * es));
         ACF_CUDA(cudaMalloc(&ra.grad_shell, ra.shell_total * sizeof(double)));
     }
     b->badj_capacity = max_steps;
@@ -3848,7 +3886,10 @@ int batch_adjoint_prepare(acf_batch *b, int64_t max_steps) {
 // Fill the device table of per-room adjoint descriptions for the current run.
 template <typename T>
 int upload_adjoint_table(acf_batch *b, int64_t n) {
-    std::vector<AdjointParams<T>> table(b->rooms.size());
+    // Entries [0, rooms): mu and lambda_D read from the adjoint fields, written to fields2 (by
+    // the fused step); entries [rooms, 2 rooms): the reverse.
+    const size_t nr = b->rooms.size();
+    std::vector<AdjointParams<T>> table(2 * nr);
     for (size_t r = 0; r < b->rooms.size(); r++) {
         const RoomHost &h = b->rooms[r];
         auto &ra = b->badj[r];
@@ -3874,6 +3915,21 @@ int upload_adjoint_table(acf_batch *b, int64_t n) {
         a.hist.fields_slots = 1;
         a.grad_shell = h.has_walls ? ra.grad_shell : nullptr;
         a.planes = b->planes;
+        T *g2 = (T *)ra.fields2;
+        a.out_vx = g2;
+        a.out_vy = g2 + h.field;
+        a.out_vz = g2 + 2 * h.field;
+        a.out_d = g2 + 3 * h.field;
+        AdjointParams<T> &o = table[nr + r];
+        o = a;
+        o.lvx = a.out_vx;
+        o.lvy = a.out_vy;
+        o.lvz = a.out_vz;
+        o.ld = a.out_d;
+        o.out_vx = a.lvx;
+        o.out_vy = a.lvy;
+        o.out_vz = a.lvz;
+        o.out_d = a.ld;
         (void)n;
     }
     if (!b->badj_table) ACF_CUDA(cudaMalloc(&b->badj_table, table.size() * sizeof(AdjointParams<T>)));
@@ -3953,13 +4009,26 @@ int batch_adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, d
     p.step_base = b->step_base;
     const dim3 grid(b->batch_ctas), block(b->block_threads);
     set_step_base<<<1, 1, 0, st>>>(b->step_base, b->badj_step0);
-    for (int64_t t = n - 1; t >= 0; t--) {
+    // The last recorded step as a cell sweep alone; every earlier step as one fused launch (the
+    // face sweep of step t + 1, then the cell sweep of step t), alternating between the two
+    // copies of mu and lambda_D; the face sweep of step 0 closes the run.
+    const AdjointParams<T> *tables[2] = {(const AdjointParams<T> *)b->badj_table,
+                                         (const AdjointParams<T> *)b->badj_table + b->rooms.size()};
+    int parity = 0;
+    p.rooms = tables[0];
+    p.local_step = (int32_t)(n - 1);
+    dispatch_pressure<T, BatchAdjPressure>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+    for (int64_t t = n - 2; t >= 0; t--) {
+        p.rooms = tables[parity];
         p.local_step = (int32_t)t;
-        dispatch_pressure<T, BatchAdjPressure>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
-        if (b->any_layer) adjoint_velocity_batch<T, true><<<grid, block, 0, st>>>(p);
-        else adjoint_velocity_batch<T, false><<<grid, block, 0, st>>>(p);
+        dispatch_pressure<T, BatchAdjFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        parity ^= 1;
     }
-    b->launches += 2 * n + 1;
+    p.rooms = tables[parity];
+    p.local_step = 0;
+    if (b->any_layer) adjoint_velocity_batch<T, true><<<grid, block, 0, st>>>(p);
+    else adjoint_velocity_batch<T, false><<<grid, block, 0, st>>>(p);
+    b->launches += n + 2;
     ACF_CUDA(cudaGetLastError());
     int64_t src_row = 0, shell_at = 0;
     for (size_t r = 0; r < b->rooms.size(); r++) {
