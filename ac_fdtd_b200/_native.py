@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "acf_batch_energy_terms", "acf_batch_profile_enable", "acf_batch_profile_read",
     "acf_batch_launch_count", "acf_set_coefficients", "acf_adjoint_prepare",
     "acf_adjoint_shell_size", "acf_forward_record", "acf_adjoint_run", "acf_adjoint_download",
-    "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status", "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval",
+    "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status", "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval", "acf_set_device",
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
 )
@@ -130,6 +130,7 @@ _SIGNATURES = {
     "acf_set_staging": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "acf_batch_set_scheme": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_adjoint_checkpoint_interval": (ctypes.c_int32, [_P]),
+    "acf_set_device": (ctypes.c_int, [ctypes.c_int32]),
     "acf_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "acf_batch_adjoint_prepare": (ctypes.c_int, [_P, _I64]),
     "acf_batch_adjoint_shell_size": (ctypes.c_int64, [_P, ctypes.c_int32]),

@@ -37,7 +37,8 @@ class RoomBatch:
 
     def __init__(self, rooms, dtype=np.float32, *, stream: int = 0,
                  steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
-                 differentiable_walls: bool = False, scheme: str = "two_sweeps") -> None:
+                 differentiable_walls: bool = False, scheme: str = "two_sweeps",
+                 device: int | None = None) -> None:
         if not rooms:
             raise ValueError("a batch needs at least one room")
         self.dtype = np.dtype(dtype)
@@ -46,6 +47,8 @@ class RoomBatch:
         _native.check(self._lib.acf_device_count(ctypes.byref(count)), "acf_device_count")
         if count.value < 1:
             raise RuntimeError("no CUDA device is visible; the cuda backend has no CPU path")
+        if device is not None:      # else the library's current device (0 unless set)
+            _native.check(self._lib.acf_set_device(int(device)), "acf_set_device")
         self.specs = [dict(room) for room in rooms]
         self.blocks = []
         self._force_walls = differentiable_walls

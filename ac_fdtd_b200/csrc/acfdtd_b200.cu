@@ -4067,6 +4067,15 @@ int acf_device_count(int *count) {
     return ACF_OK;
 }
 
+int acf_set_device(int32_t device) {
+    int count = 0;
+    ACF_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count)
+        return fail(ACF_ERR_ARGUMENT, "device %d out of range (%d visible)", device, count);
+    ACF_CUDA(cudaSetDevice(device));
+    return ACF_OK;
+}
+
 // ---- one room ---------------------------------------------------------------------------
 
 int acf_create(const acf_config *cfg, acf_solver **out) {

@@ -34,8 +34,9 @@ def partition_rooms(cell_counts, world_size: int) -> list[list[int]]:
 class ShardedRooms:
     """This rank's part of a room list, run as one batch, with a gather of the recordings.
 
-    ``make_batch(specs)`` builds the local batch (a ``RoomBatch`` in production; tests pass a
-    stand-in); ``rank``/``world_size`` default to the current process group.
+    ``make_batch(specs)`` builds the local batch (in production a ``RoomBatch`` on this rank's
+    GPU, e.g. ``functools.partial(RoomBatch, device=local_rank)``; tests pass a stand-in);
+    ``rank``/``world_size`` default to the current process group.
     """
 
     def __init__(self, specs, make_batch, rank: int | None = None, world_size: int | None = None):

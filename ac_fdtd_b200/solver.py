@@ -101,7 +101,8 @@ class CudaAcousticFDTD:
     def __init__(self, grid, medium=AIR, courant: float = 1.0, dtype=np.float64, walls=None,
                  absorbing_layer=None, air_absorption=None, *, stream: int = 0,
                  steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
-                 differentiable_walls: bool = False, scheme: str = "two_sweeps") -> None:
+                 differentiable_walls: bool = False, scheme: str = "two_sweeps",
+                 device: int | None = None) -> None:
         block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
                                   air_absorption, force_walls=differentiable_walls)
         self._force_walls = differentiable_walls
@@ -123,6 +124,8 @@ class CudaAcousticFDTD:
         _native.check(self._lib.acf_device_count(ctypes.byref(count)), "acf_device_count")
         if count.value < 1:
             raise RuntimeError("no CUDA device is visible; the cuda backend has no CPU path")
+        if device is not None:      # else the library's current device (0 unless set)
+            _native.check(self._lib.acf_set_device(int(device)), "acf_set_device")
 
         config, keep = config_from_block(block)
         handle = ctypes.c_void_p()

@@ -65,7 +65,7 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: str):
         self.device = device
         self.rows: list[list[str]] = []
         self._stop = threading.Event()
@@ -201,13 +201,23 @@ def run_reference(args) -> None:
 
 
 # --------------------------------------------------------------------------- our arm
-def run_ours(args) -> None:
-    import torch
+def physical_gpu(local: int) -> str:
+    """The GPU (index or UUID, as CUDA_VISIBLE_DEVICES names it) that local rank `local` runs on."""
+    visible = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return visible[local] if local < len(visible) else str(local)
 
+
+def run_ours(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    gpu = physical_gpu(local)
+    # One visible GPU per process, before CUDA starts: device 0 is then the same GPU for torch
+    # (NCCL, events) and for the CUDA library's own runtime, whatever device either would pick.
+    os.environ["CUDA_VISIBLE_DEVICES"] = gpu
+    import torch
+
+    torch.cuda.set_device(0)
     dist = None
     if world > 1:
         import datetime
@@ -215,7 +225,7 @@ def run_ours(args) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+                                device_id=torch.device("cuda", 0))
 
     from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse, pinned_array
 
@@ -257,7 +267,7 @@ def run_ours(args) -> None:
     solver.profile(True)
     launches0 = solver.launch_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    with ClockSampler(gpu) as clocks:
         barrier()
         start.record()
         for _ in range(args.steps):

@@ -95,6 +95,12 @@ int acf_abi_version(void);
 size_t acf_struct_size(void);          /* sizeof(acf_config), for FFI mirror checks */
 const char *acf_last_error(void);      /* message of the last failure on this thread */
 int acf_device_count(int *count);
+/* Make `device` the calling thread's current device in this library's CUDA runtime, so the
+ * next acf_create / acf_batch_create place their handle there (a handle keeps its device;
+ * every call on it switches to that device and back). Needed by callers with several GPUs in
+ * one process: the library links its own runtime, whose current device another runtime's
+ * selection need not change. No counterpart in the reference (one CPU pool per process). */
+int acf_set_device(int32_t device);
 
 /* Handle lifetime. acf_create allocates zeroed device state on the current device. */
 int acf_create(const acf_config *config, acf_solver **out);

@@ -153,3 +153,20 @@ def test_batch_sends_one_config_per_room(stub):
     batch.add_volume_source(1, (0.1, 0.1, 0.1), np.ones(3))
     batch.run(4)
     assert ("acf_batch_set_sources" in stub.names()) and ("acf_batch_run" in stub.names())
+
+
+def test_a_device_is_selected_before_the_handle_is_created(stub):
+    """With device=, the library's runtime is switched to that GPU before the handle that will
+    live there is created; without it, no device call is made."""
+    grid = Grid(dx=0.05, nx=6, ny=5, nz=4)
+    CudaAcousticFDTD(grid, device=3)
+    names = stub.names()
+    assert names.index("acf_set_device") < names.index("acf_create")
+    assert [args for name, args in stub.calls if name == "acf_set_device"] == [(3,)]
+    stub.calls.clear()
+    RoomBatch([dict(grid=grid), dict(grid=grid)], device=1)
+    names = stub.names()
+    assert names.index("acf_set_device") < names.index("acf_batch_create")
+    stub.calls.clear()
+    CudaAcousticFDTD(grid)
+    assert "acf_set_device" not in stub.names()
