@@ -284,3 +284,19 @@ def test_staged_points_in_one_tile(vector):
     cuda.run(30)
     cuda.check_device()
     assert_same_state(cuda, oracle)
+
+
+def test_an_explicit_device_gives_the_same_results():
+    """device= selects the GPU in the library's own runtime; on device 0 the results equal the
+    default construction bit for bit, for a single room and a batch."""
+    from ac_fdtd_b200 import RoomBatch
+
+    oracle, default = paired(walls=WallAdmittances.uniform(0.2))
+    explicit = prepare(CudaAcousticFDTD(GRID, device=0, walls=WallAdmittances.uniform(0.2)))
+    for solver in (oracle, default, explicit):
+        solver.run(40)
+    assert_same_state(explicit, oracle)
+    batch = RoomBatch([dict(grid=GRID)], dtype=np.float64, device=0)
+    batch.set_field(0, 0, np.random.default_rng(0).standard_normal(GRID.shape))
+    batch.run(5)
+    assert np.all(np.isfinite(batch.p(0)))
