@@ -254,6 +254,107 @@ def make_io(ref_pkg, scratch: Path) -> tuple[dict, dict]:
     return data, meta
 
 
+def make_autograd(ref_pkg) -> tuple[dict, dict]:
+    """Gradients of a linear receiver loss by PyTorch autograd through the reference's Torch
+    backend (CPU, float64): with respect to the source signal, the initial pressure, the six wall
+    admittances and the air's relaxation strengths and times. Autograd needs every coefficient as
+    a tensor of those parameters, so the wall coefficient and the relaxation coefficients are
+    rebuilt here with the reference's formulas (boundaries.py wall_update_coefficients,
+    torch_backend.py __init__), and the backend's two updates that write through out= (which
+    autograd cannot follow) are replaced by the same operations in the same order without it."""
+    import math
+
+    import torch
+
+    from ac_fdtd import AbsorbingLayer, AirAbsorption, Grid, WallAdmittances
+    from ac_fdtd.boundaries import FACES
+    from ac_fdtd.sources import gaussian_pulse
+    from ac_fdtd.torch_backend import TorchAcousticFDTD
+
+    torch.set_default_dtype(torch.float64)
+    grid = Grid(dx=0.05, nx=14, ny=12, nz=10)
+    xi = np.array([0.31, 0.12, 0.45, 0.2, 0.08, 0.27])
+    air = AirAbsorption(temperature=20.0, relative_humidity=50.0)
+    source, receivers = (0.22, 0.31, 0.19), [(0.55, 0.4, 0.35), (0.1, 0.5, 0.42), (0.63, 0.12, 0.08)]
+    steps = 90
+    solver = TorchAcousticFDTD(grid, dtype=torch.float64, walls=WallAdmittances(*xi),
+                               absorbing_layer=AbsorbingLayer(thickness=3), air_absorption=air)
+    rng = np.random.default_rng(21)
+    p0 = rng.standard_normal(grid.shape)
+    w = rng.standard_normal((len(receivers), steps))
+    signal = gaussian_pulse(steps, solver.dt, 2500.0)
+
+    p0_t = torch.tensor(p0, requires_grad=True)
+    signal_t = torch.tensor(signal, requires_grad=True)
+    xi_t = torch.tensor(xi, requires_grad=True)
+    processes = air.processes(solver.medium.sound_speed, solver.dt)
+    strength_t = torch.tensor([q.strength for q in processes], requires_grad=True)
+    tau_t = torch.tensor([q.relaxation_time for q in processes], requires_grad=True)
+
+    # walls: a = sum over the faces touching a cell of c dt xi_f / (2 dx), at the reference's cells
+    scale = solver.medium.sound_speed * solver.dt / (2.0 * grid.dx)
+    a_field = torch.zeros(grid.shape)
+    for f, (axis, side) in enumerate(FACES):
+        mask = torch.zeros(grid.shape)
+        index = [slice(None)] * 3
+        index[axis] = 0 if side == 0 else grid.shape[axis] - 1
+        mask[tuple(index)] = 1.0
+        a_field = a_field + mask * (scale * xi_t[f])
+    a = a_field.reshape(-1)[solver._wall_indices]
+    solver._wall_from_updated = 1.0 / (1.0 + a)
+    solver._wall_from_previous = a / (1.0 + a)
+
+    # air: the backend's relaxation coefficients as functions of the strengths and times
+    c, rho, dt, dx = solver.medium.sound_speed, solver.medium.density, solver.dt, grid.dx
+    relaxed = c**2 / (1.0 + strength_t.sum())
+    relaxation = []
+    for r in range(len(processes)):
+        decay = torch.exp(-dt / tau_t[r])
+        mean_weight = (tau_t[r] / dt) * (1.0 - decay)
+        relaxation.append((torch.zeros(grid.shape), decay, dt * mean_weight,
+                           rho * relaxed * strength_t[r] / dx))
+    target_scale = dt * sum(gain for _, _, _, gain in relaxation)
+
+    from ac_fdtd.torch_backend import _lower, _upper
+
+    def update_pressure():
+        flat = solver.p.view(-1)
+        previous = flat[solver._wall_indices].clone()
+        divergence = solver.velocity[0][_upper(0)] - solver.velocity[0][_lower(0)]
+        for axis in (1, 2):
+            divergence = divergence + (solver.velocity[axis][_upper(axis)] - solver.velocity[axis][_lower(axis)])
+        for k, (state, decay, mean_weight, gain) in enumerate(relaxation):
+            target = divergence * gain
+            offset = state - target
+            relaxation[k] = (offset * decay + target, decay, mean_weight, gain)
+            solver.p = solver.p + offset * mean_weight
+        solver.p = solver.p + divergence * target_scale
+        solver.p = solver.p - divergence * solver._pressure_coefficient
+        flat = solver.p.reshape(-1)
+        updated = flat[solver._wall_indices] * solver._wall_from_updated - previous * solver._wall_from_previous
+        solver.p = flat.index_put((solver._wall_indices,), updated).reshape(grid.shape)
+
+    solver._update_pressure = update_pressure
+    solver._relaxation = []
+    solver.p = p0_t * 1.0
+    solver.velocity = [v.clone() for v in solver.velocity]
+    solver._sources = [(int(np.ravel_multi_index(grid.cell_index(source), grid.shape)), signal_t)]
+    for point in receivers:
+        solver.add_pressure_receiver(point)
+    solver.run(steps)
+    loss = (torch.tensor(w) * solver._recording).sum()
+    loss.backward()
+    data = {"p0": p0, "w": w, "signal": signal, "recording": solver._recording.detach().numpy(),
+            "grad_signal": signal_t.grad.numpy(), "grad_p0": p0_t.grad.numpy(),
+            "grad_xi": xi_t.grad.numpy(), "grad_strength": strength_t.grad.numpy(),
+            "grad_relaxation_time": tau_t.grad.numpy()}
+    meta = {"shape": list(grid.shape), "dx": grid.dx, "xi": xi.tolist(), "layer_thickness": 3,
+            "air": {"temperature": 20.0, "relative_humidity": 50.0}, "source": source,
+            "receivers": receivers, "steps": steps, "max_frequency": 2500.0,
+            "torch": torch.__version__, "loss": float(loss.detach())}
+    return data, meta
+
+
 def main(reference: str = "/root/reference", *parts: str) -> None:
     """Regenerate every fixture, or only the named parts (setup, trajectories, rooms, impulse,
     io); golden.json keeps the entries of the parts not regenerated."""
@@ -268,9 +369,12 @@ def main(reference: str = "/root/reference", *parts: str) -> None:
         if "io" in parts:
             io_data, meta["io"] = make_io(ref_pkg, scratch)
             np.savez_compressed(HERE / "io.npz", **io_data)
-        unknown = set(parts) - {"io"}
+        if "autograd" in parts:
+            ag_data, meta["autograd"] = make_autograd(ref_pkg)
+            np.savez_compressed(HERE / "autograd.npz", **ag_data)
+        unknown = set(parts) - {"io", "autograd"}
         if unknown:
-            raise SystemExit(f"only 'io' can be regenerated on its own, not {sorted(unknown)}")
+            raise SystemExit(f"only 'io' and 'autograd' can be regenerated on their own, not {sorted(unknown)}")
         (HERE / "golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
         shutil.rmtree(scratch)
         return
@@ -285,8 +389,10 @@ def main(reference: str = "/root/reference", *parts: str) -> None:
     np.savez_compressed(HERE / "impulse.npz", **impulse)
     io_data, io_meta = make_io(ref_pkg, scratch)
     np.savez_compressed(HERE / "io.npz", **io_data)
+    ag_data, ag_meta = make_autograd(ref_pkg)
+    np.savez_compressed(HERE / "autograd.npz", **ag_data)
     meta = {"setup": setup_meta, "trajectories": traj_meta, "rooms": rooms_meta,
-            "impulse": impulse_meta, "io": io_meta,
+            "impulse": impulse_meta, "io": io_meta, "autograd": ag_meta,
             "generator": "tests/golden/make_golden.py", "numpy": np.__version__}
     (HERE / "golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True) + "\n")
     shutil.rmtree(scratch)
