@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>
@@ -2595,11 +2596,14 @@ template <typename T, bool L, bool W, int NR>
 struct StagedStep {
     static void launch(const StagedParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
         const size_t smem = kStagedBarrierBytes + (size_t)p.stages * p.stage_elems * sizeof(T);
-        // Opt in to the largest dynamic shared memory the block can hold beside its static part.
-        static bool opted_in = false;
-        if (!opted_in) {
-            int optin = 0, device = 0;
-            cudaGetDevice(&device);
+        // Opt in to the largest dynamic shared memory the block can hold beside its static part:
+        // a per-device attribute of the kernel, so once on each device (first 64 devices).
+        static std::atomic<uint64_t> opted_in{0};
+        int device = 0;
+        cudaGetDevice(&device);
+        const uint64_t bit = device < 64 ? (uint64_t)1 << device : 0;
+        if (!bit || !(opted_in.load() & bit)) {
+            int optin = 0;
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
             auto opt_in = [optin](const void *kernel) {
                 cudaFuncAttributes attr{};
@@ -2609,7 +2613,7 @@ struct StagedStep {
             };
             opt_in((const void *)fused_staged_sweep<T, L, W, NR, 2>);
             opt_in((const void *)fused_staged_sweep<T, L, W, NR, 4>);
-            opted_in = true;
+            opted_in.fetch_or(bit);
         }
         if (p.vector == 2) fused_staged_sweep<T, L, W, NR, 2><<<g, b, smem, st>>>(p);
         else fused_staged_sweep<T, L, W, NR, 4><<<g, b, smem, st>>>(p);
