@@ -2,10 +2,13 @@
 
 Each room is described by the arguments of ``CudaAcousticFDTD`` (grid, medium, courant, walls,
 absorbing_layer, air_absorption); all rooms share the precision and the number of ISO
-relaxation processes and step in lockstep. Both sweeps of a step are single launches over a
-flat tile table that covers every room (one CTA per tile, or a persistent grid striding over
-the table), and long runs replay CUDA graphs of those launches. Per room, the arithmetic is exactly that of the single-room solver, so every room's
-fields and recordings equal a ``CudaAcousticFDTD`` run of that room alone, bit for bit.
+relaxation processes and step in lockstep. Each sweep is a single launch over a flat tile
+table that covers every room (one CTA per tile, or a persistent grid striding over the table):
+two launches a step with ``scheme="two_sweeps"``, one with ``scheme="fused"`` (the velocity and
+pressure updates of a step in one sweep, ping-ponging the fields as ``CudaAcousticFDTD`` does
+with the same scheme). Long runs replay CUDA graphs of those launches. Per room, the arithmetic
+is exactly that of the single-room solver, so every room's fields and recordings equal a
+``CudaAcousticFDTD`` run of that room alone, bit for bit, under either scheme.
 
 The reference solves one room per solver object (``src/ac_fdtd/scheme.py:82``); batching is
 this backend's addition for workloads of many rooms or many source positions.

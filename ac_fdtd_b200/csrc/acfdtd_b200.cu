@@ -1,6 +1,6 @@
 // acfdtd_b200.cu -- the staggered pressure-velocity leapfrog on sm_100a, behind a C ABI.
 //
-// One time step is two HBM-bound sweeps over the grid (ac-fdtd: src/ac_fdtd/scheme.py:285-296,
+// One time step is two HBM-bound updates of the grid (ac-fdtd: src/ac_fdtd/scheme.py:285-296,
 // src/ac_fdtd/c/acfdtd.c:110-190,342-376):
 //
 //   (a) velocity: v_a -= c_v (p_hi - p_lo) on interior faces, then the absorbing-layer damping
@@ -19,11 +19,22 @@
 // a neighbour on any axis is a constant stride away. Rows start on 32-byte boundaries, which
 // keeps every 4-element group of a thread a single aligned vector access.
 //
+// Three step schemes give the same bits:
+//   * two_sweeps: (a) and (b) as two launches, fields updated in place;
+//   * fused: one launch per step; each cell computes the updated velocities of its six faces
+//     and then its pressure, writing the next p and v into a second copy of the fields
+//     (ping-pong), so a cell costs one read and one write of each field;
+//   * staged: the fused step with the planes of its inputs brought into a shared-memory ring
+//     by the bulk-copy engine (one producer warp, mbarrier waits with a time limit).
+//
 // Two launch forms share the per-column code:
 //   * one room: a 2D grid of (z chunk, y row) threads, each block marching `planes` x planes;
 //   * a batch of rooms of different sizes packed in one arena: a persistent grid walks a flat
 //     tile table (room, first (row, chunk) pair, plane range); each CTA stages its room's
 //     description in shared memory. One launch per sweep covers every room.
+//
+// The adjoint (transposed) leapfrog for gradients reuses the same layout, launch forms and
+// fusion, backward in time.
 
 #include <cuda_runtime.h>
 

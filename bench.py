@@ -418,12 +418,12 @@ def precision_check(args) -> dict:
         recordings[dtype] = solver.recorded_pressure
         solver.close()
     f64_gcups = grid.n_cells * T / (times["float64"] * 1e-3) / 1e9
-    peak, _ = measured_peak_hbm()
+    peak, peak_kind = measured_peak_hbm()
     out["room_384"] = {
         "workload": f"the headline room, {args.size}^3, {T} steps from rest, {len(points) - 1} receivers",
         "fp32_vs_fp64": _errors(recordings[np.float32], recordings[np.float64]),
         "fp64_gcups": f64_gcups,
-        "fp64_hbm_frac_of_measured_at_112_B_per_cell": f64_gcups * 112 / peak,
+        f"fp64_hbm_frac_of_{peak_kind}_at_112_B_per_cell": f64_gcups * 112 / peak,
         "fp64_launch": schemes["float64"],
         "note": "one run including its CUDA-graph capture, timed with CUDA events",
     }
@@ -529,7 +529,7 @@ def batched_vs_per_room(args) -> dict:
         for solver in solvers:
             solver.close()
     per_room_ms = min(per_room.values())
-    peak, _ = measured_peak_hbm()
+    peak, peak_kind = measured_peak_hbm()
     batched_gcups = cells * T / (batch_ms * 1e-3) / 1e9
     return {
         "workload": f"64 rooms 3-10 m per axis at dx 5 cm ({cells} cells, 60-200 per axis), fp32, "
@@ -539,7 +539,7 @@ def batched_vs_per_room(args) -> dict:
         "per_room_gcups": cells * T / (per_room_ms * 1e-3) / 1e9,
         "per_room_gcups_by_scheme": {k: cells * T / (v * 1e-3) / 1e9 for k, v in per_room.items()},
         "speedup": per_room_ms / batch_ms,
-        "batched_hbm_frac_of_measured": batched_gcups * (56 if batch_geometry[0] == "fused" else 72) / peak,
+        f"batched_hbm_frac_of_{peak_kind}": batched_gcups * (56 if batch_geometry[0] == "fused" else 72) / peak,
         "bytes_per_cell": 56 if batch_geometry[0] == "fused" else 72,
         "launches_in_setup_and_runs": launches,
         "batch_launch": {"scheme": batch_geometry[0], "block_threads": batch_geometry[1],
