@@ -36,6 +36,7 @@ EXPORTED_SYMBOLS = (
     "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status", "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval", "acf_set_device",
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
+    "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED = 0, 1, 2
@@ -138,6 +139,9 @@ _SIGNATURES = {
     "acf_batch_adjoint_run": (ctypes.c_int, [_P, _DP, _DP, _DP, _P]),
     "acf_batch_reset_state": (ctypes.c_int, [_P, _P]),
     "acf_batch_set_coefficients": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(AcfConfig)]),
+    "acf_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_get_prefetch": (ctypes.c_int, [_P]),
+    "acf_batch_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
 }
 
 

@@ -238,6 +238,14 @@ class RoomBatch:
                       "acf_batch_set_scheme")
         self.scheme = scheme
 
+    def set_prefetch(self, enabled: bool | None = None) -> None:
+        """L2 prefetch of each next x plane: ``None`` (default) turns it on when every room's
+        fields together exceed the GPU's L2, ``True``/``False`` force it. Results never depend
+        on it."""
+        mode = -1 if enabled is None else int(bool(enabled))
+        _native.check(self._lib.acf_batch_set_prefetch(self._handle, mode),
+                      "acf_batch_set_prefetch")
+
     def reset_state(self) -> None:
         """Every room at rest (all fields zero), on the device."""
         _native.check(self._lib.acf_batch_reset_state(self._handle, self._stream),

@@ -115,12 +115,22 @@ struct Vec4<double> {
     }
 };
 
+// Ask L2 for the line holding `a` ahead of its load: the request holds no register and no
+// shared memory, so a marching thread can have its next plane on the way from DRAM while it
+// computes the current one. Only addresses the thread will load later are passed.
+template <typename T>
+__device__ __forceinline__ void prefetch_l2(const T *a) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
 // ------------------------------------------------------------------------------------------
 // What the sweeps read about one room. Plain data, identical on host and device.
 
 template <typename T>
 struct Room {
     int32_t nx, ny, nz, nchunks;
+    int32_t prefetch;              // 1: marching threads ask L2 for their next plane ahead
+    int32_t reserved;
     int64_t pz, plane, field;      // row pitch, plane pitch, elements per field
     T *p, *vx, *vy, *vz, *psi;     // psi: n_relax fields back to back
     T cv, cp, cs, relax_scale;
@@ -202,6 +212,13 @@ __device__ __forceinline__ void velocity_column(const Room<T> &s, int i_begin, i
 
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
+        if (s.prefetch && i + 1 < i_end) {  // the next plane's own-row inputs into L2
+            const int64_t next = base + s.plane;
+            prefetch_l2(s.p + next);
+            prefetch_l2(s.vx + next);
+            prefetch_l2(s.vy + next);
+            prefetch_l2(s.vz + next);
+        }
         // ---- loads
         T P[kVec], Py[kVec], VX[kVec], VY[kVec], VZ[kVec];
         Vec4<T>::ldg(s.p + base, P);
@@ -452,6 +469,15 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
 
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
+        if (s.prefetch && i + 1 < i_end) {  // the next plane's own-row inputs into L2
+            const int64_t next = base + s.plane;
+            prefetch_l2(s.vx + next + s.plane);
+            prefetch_l2(s.vy + next);
+            prefetch_l2(s.vz + next);
+            prefetch_l2(s.p + next);
+#pragma unroll
+            for (int r = 0; r < NR; r++) prefetch_l2(s.psi + r * s.field + next);
+        }
         // ---- loads
         T XH[kVec], YL[kVec], YH[kVec], Z[kVec], P[kVec], S[NR > 0 ? NR : 1][kVec];
         Vec4<T>::ldg(s.vx + base + s.plane, XH);
@@ -599,6 +625,17 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
         const bool x_inner = i + 1 < s.nx;
+        // ---- the next plane's own-row inputs into L2 (its y-neighbour rows are other
+        // threads' own rows): the loads of the next iteration then wait on L2, not DRAM.
+        if (s.prefetch && i + 1 < i_end) {
+            const int64_t next = base + s.plane;
+            if (i + 2 < s.nx) prefetch_l2(s.p + next + s.plane);
+            prefetch_l2(s.vx + next + s.plane);
+            prefetch_l2(s.vy + next);
+            prefetch_l2(s.vz + next);
+#pragma unroll
+            for (int r = 0; r < NR; r++) prefetch_l2(s.psi + r * s.field + next);
+        }
         // ---- loads (all read-only: the next state goes to the other buffer)
         T PX[kVec], VXo[kVec], PYm[kVec], PYp[kVec], VY[kVec], VYp[kVec], VZ[kVec], S[NR > 0 ? NR : 1][kVec];
         if (x_inner) Vec4<T>::ldg(s.p + base + s.plane, PX);
@@ -1555,6 +1592,22 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
     }
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
+        if (s.prefetch && i + 1 < i_end) {  // the next plane's own-row inputs into L2
+            const int64_t next = base + s.plane;
+            if (FUSED && i + 2 < s.nx) prefetch_l2(a.ld + next + s.plane);
+            prefetch_l2(a.lvx + next + s.plane);
+            prefetch_l2(a.lvy + next);
+            prefetch_l2(a.lvz + next);
+            prefetch_l2(a.lp + next);
+#pragma unroll
+            for (int r = 0; r < NR; r++) prefetch_l2(a.lpsi + r * s.field + next);
+            if (AIR && NR > 0) {
+                const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
+                const T *h = a.hist.fields + slot * (1 + NR) * s.field + next;
+#pragma unroll
+                for (int r = 0; r <= NR; r++) prefetch_l2(h + r * s.field);
+            }
+        }
         T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
         T above;
         T Dxp[kVec];   // FUSED: lambda_D^{n+1} of the next plane
@@ -1833,6 +1886,13 @@ __device__ __forceinline__ void adjoint_velocity_column(const AdjointParams<T> &
     if (i_begin > 0) Vec4<T>::ldg(a.ld + (int64_t)(i_begin - 1) * s.plane + column, Dm);
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
+        if (s.prefetch && i + 1 < i_end) {  // the next plane's own-row inputs into L2
+            const int64_t next = base + s.plane;
+            prefetch_l2(a.ld + next);
+            prefetch_l2(a.lvx + next);
+            prefetch_l2(a.lvy + next);
+            prefetch_l2(a.lvz + next);
+        }
         T Dc[kVec], Dy[kVec], VX[kVec], VY[kVec], VZ[kVec];
         Vec4<T>::ldg(a.ld + base, Dc);
         if (j > 0) Vec4<T>::ldg(a.ld + base - s.pz, Dy);
@@ -2299,6 +2359,8 @@ struct acf_batch {
     int staged_stages = 0;           // staged scheme: ring buffers per CTA (0: automatic)
     int staged_vector = 4;           // staged scheme: z elements per thread (2 or 4)
     int smem_per_sm = 233472, smem_per_block = 232448;
+    int prefetch_mode = -1;          // L2 prefetch of the next plane: -1 by size, 0 off, 1 on
+    int64_t l2_bytes = 0;            // the device's L2 size
 
     // graphs (index: parity of the fused scheme's current buffer at the start of a replay)
     int32_t graph_steps = 0;
@@ -2388,6 +2450,18 @@ namespace {
 
 // `state` (optional) points at another copy of the room's fields in the same geometry, such as
 // the adjoint's recompute buffer.
+// Whether the marching kernels ask L2 for each next plane ahead of its loads. Automatically
+// when the fields one step streams (every room of the handle; the fused schemes' second copy
+// of p and v included) exceed L2: the prefetches then keep more DRAM reads in flight than the
+// threads' registers hold, while a room that stays in L2 would only pay for the extra requests.
+bool prefetch_planes(const acf_batch *b) {
+    if (b->prefetch_mode >= 0) return b->prefetch_mode != 0;
+    const double fields = (double)b->n_fields() + (b->scheme != ACF_SCHEME_TWO_SWEEPS ? 4.0 : 0.0);
+    double bytes = 0;
+    for (const RoomHost &h : b->rooms) bytes += fields * (double)h.field * (double)b->elem();
+    return bytes > (double)b->l2_bytes;
+}
+
 template <typename T>
 Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     const RoomHost &h = b->rooms[r];
@@ -2396,6 +2470,7 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     s.ny = h.ny;
     s.nz = h.nz;
     s.nchunks = (int32_t)((h.nz + kVec - 1) / kVec);
+    s.prefetch = prefetch_planes(b) ? 1 : 0;
     s.pz = h.pz;
     s.plane = h.plane;
     s.field = h.field;
@@ -2976,6 +3051,9 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
     }
     ACF_CUDA(cudaGetDevice(&b->device));
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, b->device);
+    b->l2_bytes = l2;
     b->precision = configs[0].precision;
     b->n_relax = configs[0].n_relax;
     b->rooms.resize((size_t)n_rooms);
@@ -3340,6 +3418,15 @@ int set_scheme(acf_batch *b, int32_t scheme) {
     }
     if (scheme != b->scheme) b->graph_dirty = b->adj_graphs_dirty = b->room_table_dirty = true;
     b->scheme = scheme;
+    return ACF_OK;
+}
+
+int set_prefetch(acf_batch *b, int32_t mode) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (mode < -1 || mode > 1) return fail(ACF_ERR_ARGUMENT, "prefetch mode must be -1, 0 or 1, got %d", mode);
+    // The flag travels in the room descriptions that graphs and room tables hold.
+    if (mode != b->prefetch_mode) b->graph_dirty = b->adj_graphs_dirty = b->room_table_dirty = true;
+    b->prefetch_mode = mode;
     return ACF_OK;
 }
 
@@ -4183,6 +4270,10 @@ int acf_set_scheme(acf_solver *h, int32_t scheme) { return set_scheme(h, scheme)
 
 int acf_get_scheme(const acf_solver *h) { return h ? h->scheme : -1; }
 
+int acf_set_prefetch(acf_solver *h, int32_t mode) { return set_prefetch(h, mode); }
+
+int acf_get_prefetch(const acf_solver *h) { return h ? (prefetch_planes(h) ? 1 : 0) : -1; }
+
 int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages, int32_t vector) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
     if (rows < 1 || rows > 16) return fail(ACF_ERR_ARGUMENT, "rows must be in [1, 16], got %d", rows);
@@ -4457,6 +4548,8 @@ int acf_batch_reset_state(acf_batch *b, acf_stream stream) {
 }
 
 int acf_batch_set_scheme(acf_batch *b, int32_t scheme) { return set_scheme(b, scheme); }
+
+int acf_batch_set_prefetch(acf_batch *b, int32_t mode) { return set_prefetch(b, mode); }
 
 int acf_batch_set_coefficients(acf_batch *b, int32_t room, const acf_config *config) {
     return set_coefficients(b, room, config);

@@ -460,6 +460,18 @@ class CudaAcousticFDTD:
         self.scheme = scheme
         self._mirror_current.clear()
 
+    def set_prefetch(self, enabled: bool | None = None) -> None:
+        """L2 prefetch of each next x plane in the marching kernels: ``None`` (default) turns
+        it on when the fields a step streams exceed the GPU's L2, ``True``/``False`` force it.
+        Results never depend on it."""
+        mode = -1 if enabled is None else int(bool(enabled))
+        _native.check(self._lib.acf_set_prefetch(self._handle, mode), "acf_set_prefetch")
+
+    @property
+    def prefetch(self) -> bool:
+        """Whether the L2 prefetch is in effect for this room."""
+        return self._lib.acf_get_prefetch(self._handle) == 1
+
     def set_launch(self, block_threads: int = 256, planes: int = 4) -> None:
         """Launch geometry of the sweeps (threads per block, x planes per block)."""
         _native.check(self._lib.acf_set_launch(self._handle, int(block_threads), int(planes)),

@@ -146,6 +146,14 @@ enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1, ACF_SCHEME_FUSED_STAGED 
 int acf_set_scheme(acf_solver *solver, int32_t scheme);
 int acf_get_scheme(const acf_solver *solver);
 
+/* L2 prefetch in the marching kernels: each thread asks L2 for its next x plane's inputs
+ * while it computes the current one, so more DRAM reads are in flight than its registers
+ * hold. mode -1 (default) enables it when the fields one step streams exceed the device's L2,
+ * 0 disables it, 1 enables it. Results never depend on it. acf_get_prefetch returns whether it
+ * is in effect (1 or 0; -1 for a null solver). No counterpart in the reference. */
+int acf_set_prefetch(acf_solver *solver, int32_t mode);
+int acf_get_prefetch(const acf_solver *solver);
+
 /* Geometry of the staged scheme: y rows per CTA (1..16, each a whole padded z row), ring
  * buffers per CTA (2..8; 0 picks three, or two where three do not fit) and z elements per
  * thread (2 or 4). The x planes per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the
@@ -276,6 +284,8 @@ int acf_batch_set_launch(acf_batch *batch, int32_t block_threads, int32_t planes
  * second copy of every room's p and v); bit-identical results. No counterpart in the
  * reference. */
 int acf_batch_set_scheme(acf_batch *batch, int32_t scheme);
+/* acf_set_prefetch for a batch; the default compares every room's fields together with L2. */
+int acf_batch_set_prefetch(acf_batch *batch, int32_t mode);
 int acf_batch_energy_terms(acf_batch *batch, int32_t room, double dx, double terms[7],
                            acf_stream stream);
 int acf_batch_profile_enable(acf_batch *batch, int32_t enable);

@@ -243,3 +243,23 @@ def test_air_gradients_agree_with_and_without_recompute():
         np.testing.assert_array_equal(a, b)
     auto = make_room(air=air, wrt=("signal", "walls", "air"))
     assert auto.checkpoint_every == STEPS          # a small room's history always fits
+
+
+@pytest.mark.parametrize("every", [STEPS, 9])
+def test_l2_prefetch_leaves_gradients_unchanged(every):
+    """The plane prefetch (off by default at this size, forced on here) touches no arithmetic:
+    forward recordings and every gradient are bit-identical, with and without recompute."""
+    air = AirAbsorption(temperature=21.0, relative_humidity=45.0)
+    results = []
+    for prefetch in (False, True):
+        room = make_room(air=air, layer=AbsorbingLayer(thickness=3),
+                         wrt=("signal", "walls", "air"), every=every)
+        room.solver.set_prefetch(prefetch)
+        assert room.solver.prefetch == prefetch
+        w = weights(3)
+        rec = room.forward(STEPS)
+        g = room.backward(w * rec)
+        results.append((rec, g.strength, g.relaxation_time, g.walls, g.signal, g.initial_p))
+        room.solver.close()
+    for a, b in zip(*results, strict=True):
+        np.testing.assert_array_equal(a, b)

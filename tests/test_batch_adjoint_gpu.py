@@ -49,6 +49,7 @@ def setup_batch(specs):
 def test_batched_gradients_equal_single_room_gradients():
     specs = rooms()
     batch = setup_batch(specs)
+    batch.batch.set_prefetch(True)     # forced on for the batch; the single rooms run without
     recs = batch.forward(STEPS)
     weights = [np.random.default_rng(20 + r).standard_normal(rec.shape) for r, rec in enumerate(recs)]
     grads = batch.backward([w * rec for w, rec in zip(weights, recs, strict=True)])

@@ -92,10 +92,14 @@ def test_every_room_matches_its_oracle(dtype, with_air, scheme):
 def test_launch_geometry_does_not_change_results():
     rooms = mixed_rooms(True)
     results = []
-    for scheme, *geometry in (("two_sweeps", 256, 4, 4), ("two_sweeps", 64, 1, 2),
-                              ("fused", 128, 16, 8), ("fused", 32, 3, 1), ("fused", 128, 8, 0)):
+    # (scheme, block threads, planes, CTAs per SM, L2 prefetch of the next plane)
+    for scheme, *geometry, prefetch in (
+            ("two_sweeps", 256, 4, 4, None), ("two_sweeps", 64, 1, 2, None),
+            ("two_sweeps", 128, 8, 0, True), ("fused", 128, 16, 8, None),
+            ("fused", 32, 3, 1, True), ("fused", 128, 8, 0, None), ("fused", 64, 5, 0, True)):
         batch = RoomBatch(rooms, dtype=np.float32, steps_per_graph=8, scheme=scheme)
         batch.set_launch(*geometry)
+        batch.set_prefetch(prefetch)
         for r, spec in enumerate(rooms):
             populate(batch, r, spec, seed=10 + r)
         batch.run(30)

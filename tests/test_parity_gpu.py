@@ -194,16 +194,20 @@ def test_odd_and_degenerate_grids(scheme):
                              air_absorption=AirAbsorption())
         oracle = OracleFDTD(grid, AIR, **configuration)
         cuda = CudaAcousticFDTD(grid, scheme=scheme, **configuration)
+        prefetching = CudaAcousticFDTD(grid, scheme=scheme, **configuration)
+        prefetching.set_prefetch(True)
         rng = np.random.default_rng(sum(shape))
         initial = rng.standard_normal(shape)
         point = tuple((n - 0.5) * 0.02 for n in shape)
-        for solver in (oracle, cuda):
+        for solver in (oracle, cuda, prefetching):
             solver.p[:] = initial
             solver.add_volume_source((0.0, 0.0, 0.0), np.hanning(12))
             solver.add_pressure_receiver(point)
         oracle.run(40)
         cuda.run(40)
+        prefetching.run(40)
         assert_same_state(cuda, oracle)
+        assert_same_state(prefetching, oracle)
 
 
 def test_switching_schemes_mid_run_and_odd_step_counts():
@@ -223,6 +227,24 @@ def test_switching_schemes_mid_run_and_odd_step_counts():
         np.testing.assert_array_equal(cuda.p, oracle.p)
     assert_same_state(cuda, oracle)
     assert cuda.step_index == total
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_l2_prefetch_forced_on_matches_the_oracle(dtype, scheme):
+    """Rooms this small stay in L2, so the plane prefetch is off by default; forced on (and
+    toggled mid-run, with graphs captured either way) the results stay bit-identical."""
+    configuration = CONFIGURATIONS["everything at once"]
+    oracle, cuda = paired(dtype=dtype, steps_per_graph=8, scheme=scheme, **configuration)
+    assert not cuda.prefetch
+    cuda.set_prefetch(True)
+    assert cuda.prefetch
+    for enabled, n in ((True, 37), (False, 9), (True, 16), (None, 5)):
+        cuda.set_prefetch(enabled)
+        cuda.run(n)
+        oracle.run(n)
+    assert not cuda.prefetch
+    assert_same_state(cuda, oracle)
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
