@@ -170,3 +170,15 @@ def test_a_device_is_selected_before_the_handle_is_created(stub):
     stub.calls.clear()
     CudaAcousticFDTD(grid)
     assert "acf_set_device" not in stub.names()
+
+
+def test_prefetch_modes_cross_the_boundary_as_minus_one_zero_one(stub):
+    solver = CudaAcousticFDTD(GRID, dtype=np.float32)
+    batch = RoomBatch([dict(grid=GRID), dict(grid=Grid(dx=0.03, nx=9, ny=8, nz=7))],
+                      dtype=np.float32)
+    for enabled in (True, False, None):
+        solver.set_prefetch(enabled)
+        batch.set_prefetch(enabled)
+    sent = [args[1] for name, args in stub.calls if name == "acf_set_prefetch"]
+    sent_batch = [args[1] for name, args in stub.calls if name == "acf_batch_set_prefetch"]
+    assert sent == sent_batch == [1, 0, -1]
