@@ -742,6 +742,8 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
 }
 
 // Resident blocks of 256 threads the compiler must fit (register budget 65536 / (256 x this)).
+// For the fp32 room with a layer: 80 registers, no spills. Timed at 384^3 with the plane
+// prefetch, 72 registers (56 bytes of spills) ran 2 % slower and 64 (140 bytes) 19 % slower.
 #ifndef ACF_FUSED_MIN_BLOCKS
 #define ACF_FUSED_MIN_BLOCKS(T, LAYER, NR) (sizeof(T) == 8 ? 2 : (LAYER || NR >= 4 ? 3 : 4))
 #endif
