@@ -36,7 +36,8 @@ EXPORTED_SYMBOLS = (
     "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status", "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval", "acf_set_device",
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
-    "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch",
+    "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch", "acf_copy_plane",
+    "acf_solver_device",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED = 0, 1, 2
@@ -142,6 +143,8 @@ _SIGNATURES = {
     "acf_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_get_prefetch": (ctypes.c_int, [_P]),
     "acf_batch_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_copy_plane": (ctypes.c_int, [_P, _I64, _P, _I64, ctypes.c_int, _P]),
+    "acf_solver_device": (ctypes.c_int, [_P]),
 }
 
 

@@ -4260,6 +4260,32 @@ int acf_field_pointer(acf_solver *h, int field, void **ptr, int64_t strides[3]) 
     return ACF_OK;
 }
 
+int acf_copy_plane(acf_solver *dst, int64_t dst_plane, const acf_solver *src, int64_t src_plane,
+                   int field, acf_stream stream) {
+    if (!dst || !src) return fail(ACF_ERR_ARGUMENT, "null solver");
+    int rc = check_field(dst, 0, field);
+    if (rc) return rc;
+    rc = check_field(src, 0, field);
+    if (rc) return rc;
+    const RoomHost &hd = dst->rooms[0], &hs = src->rooms[0];
+    if (dst->precision != src->precision || hd.ny != hs.ny || hd.nz != hs.nz)
+        return fail(ACF_ERR_ARGUMENT, "the two rooms' planes differ in precision or shape");
+    if (dst_plane < 0 || dst_plane > hd.nx || src_plane < 0 || src_plane > hs.nx)
+        return fail(ACF_ERR_ARGUMENT, "plane %lld or %lld out of range", (long long)dst_plane,
+                    (long long)src_plane);
+    const size_t bytes = (size_t)hd.plane * dst->elem();   // one padded plane: (ny+1) x pz
+    char *d = dst->field_ptr(0, field) + (size_t)dst_plane * bytes;
+    const char *sp = src->field_ptr(0, field) + (size_t)src_plane * bytes;
+    DeviceGuard guard(dst->device);
+    if (dst->device == src->device)
+        ACF_CUDA(cudaMemcpyAsync(d, sp, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    else
+        ACF_CUDA(cudaMemcpyPeerAsync(d, dst->device, sp, src->device, bytes, (cudaStream_t)stream));
+    return ACF_OK;
+}
+
+int acf_solver_device(const acf_solver *h) { return h ? h->device : -1; }
+
 int acf_profile_enable(acf_solver *h, int32_t enable) { return profile_enable(h, enable); }
 
 int acf_profile_read(acf_solver *h, double *velocity_ms, double *pressure_ms, int64_t *launches) {

@@ -102,9 +102,17 @@ class CudaAcousticFDTD:
                  absorbing_layer=None, air_absorption=None, *, stream: int = 0,
                  steps_per_graph: int = DEFAULT_STEPS_PER_GRAPH,
                  differentiable_walls: bool = False, scheme: str = "two_sweeps",
-                 device: int | None = None) -> None:
-        block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
-                                  air_absorption, force_walls=differentiable_walls)
+                 device: int | None = None, coefficients=None) -> None:
+        # ``coefficients``: a prepared block for ``grid`` (a slab of a larger room cuts its own
+        # from the whole room's); otherwise built from the arguments as the reference does.
+        if coefficients is None:
+            block = room_coefficients(grid, medium, courant, dtype, walls, absorbing_layer,
+                                      air_absorption, force_walls=differentiable_walls)
+        else:
+            block = coefficients
+            if tuple(block.shape) != (int(grid.nx), int(grid.ny), int(grid.nz)):
+                raise ValueError(f"coefficient block of shape {block.shape} for a grid of "
+                                 f"{(grid.nx, grid.ny, grid.nz)}")
         self._force_walls = differentiable_walls
         self.grid = grid
         self.medium = medium
@@ -308,6 +316,20 @@ class CudaAcousticFDTD:
         self._receivers_dirty = True
         return len(self._receivers) - 1
 
+    def add_volume_source_at(self, cell, signal) -> None:
+        """``add_volume_source`` for the cell with index ``(i, j, k)``."""
+        values = np.asarray(signal, dtype=self.dtype).reshape(-1)
+        self._sources.append((int(np.ravel_multi_index(tuple(int(c) for c in cell), self._shape)),
+                              values))
+        self._sources_dirty = True
+
+    def add_pressure_receiver_at(self, cell) -> int:
+        """``add_pressure_receiver`` for the cell with index ``(i, j, k)``."""
+        flat = int(np.ravel_multi_index(tuple(int(c) for c in cell), self._shape))
+        self._receivers.append((flat, self.step_index))
+        self._receivers_dirty = True
+        return len(self._receivers) - 1
+
     def _push_points(self) -> None:
         if self._sources_dirty:
             n = len(self._sources)
@@ -388,6 +410,24 @@ class CudaAcousticFDTD:
 
     def step(self) -> None:
         self.run(1)
+
+    def flush(self) -> None:
+        """Upload what was written into the host snapshots now (``run`` does it by itself)."""
+        self._flush()
+
+    @property
+    def device(self) -> int:
+        """The GPU this solver's state lives on."""
+        return int(self._lib.acf_solver_device(self._handle))
+
+    def field_pointer(self, field: int) -> tuple[int, tuple[int, int, int]]:
+        """Device address of a field in the padded layout and its (x, y, z) element strides;
+        valid until the next ``run`` (the fused schemes alternate between two copies)."""
+        pointer = ctypes.c_void_p()
+        strides = (ctypes.c_int64 * 3)()
+        _native.check(self._lib.acf_field_pointer(self._handle, int(field), ctypes.byref(pointer),
+                                                  strides), "acf_field_pointer")
+        return int(pointer.value or 0), (int(strides[0]), int(strides[1]), int(strides[2]))
 
     def synchronize(self) -> None:
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")

@@ -244,6 +244,18 @@ int acf_energy_terms_noalloc(const void *p, const void *vx, const void *vy, cons
  * of one field in the internal padded layout. */
 int acf_field_pointer(acf_solver *solver, int field, void **ptr, int64_t strides[3]);
 
+/* Copy x plane `src_plane` of one field of `src` into x plane `dst_plane` of the same field of
+ * `dst` (every field has nx + 1 planes of (ny + 1) padded rows), device to device -- a peer
+ * copy when the two solvers live on different GPUs. The rooms must share precision, ny and nz.
+ * Asynchronous on `stream`; order it after both solvers' work (the same stream, or a
+ * synchronization). The ghost-plane exchange of a room split into x slabs. No counterpart in
+ * the reference (its solver is one shared-memory process). */
+int acf_copy_plane(acf_solver *dst, int64_t dst_plane, const acf_solver *src, int64_t src_plane,
+                   int field, acf_stream stream);
+
+/* The GPU a solver's state lives on (-1 for a null solver). No counterpart in the reference. */
+int acf_solver_device(const acf_solver *solver);
+
 /* Instrumentation: when enabled, acf_run launches step by step with CUDA events around each
  * sweep and accumulates their device time. */
 int acf_profile_enable(acf_solver *solver, int32_t enable);
