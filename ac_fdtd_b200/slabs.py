@@ -10,7 +10,7 @@ the single-room arithmetic, and the owned planes equal a one-GPU run of the room
 After every step each part sends its first owned p plane to the left neighbour's right ghost
 and its last owned p plane to the right neighbour's left ghost. The next velocity sweep then
 computes every owned face, including the two faces shared with ghosts, from current pressures,
-so only pressure planes travel: ((ny + 1) x pz elements each way per cut and step (590 KB at
+so only pressure planes travel: (ny + 1) x pz elements each way per cut and step (604 KB at
 384^2 fp32 in the padded layout). Ghost cells are themselves updated by the sweeps and then
 overwritten by the exchange; nothing owned reads them in between.
 
