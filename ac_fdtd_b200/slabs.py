@@ -224,7 +224,8 @@ class SlabGroup(_SlabSet):
 
     def add_volume_source(self, point, signal) -> None:
         owners = [s.add_volume_source(point, signal) for s in self.slabs]
-        assert sum(owners) == 1
+        if sum(owners) != 1:
+            raise RuntimeError(f"point {point} is owned by {sum(owners)} parts, not one")
 
     def add_pressure_receiver(self, point) -> int:
         for q, s in enumerate(self.slabs):
@@ -232,7 +233,7 @@ class SlabGroup(_SlabSet):
             if local is not None:
                 self._receivers.append((q, local))
                 return len(self._receivers) - 1
-        raise AssertionError("every point belongs to one part")
+        raise RuntimeError(f"point {point} is owned by no part")
 
     def _copy(self, dst: SlabRoom, dst_plane: int, src: SlabRoom, src_plane: int) -> None:
         _native.check(self._lib.acf_copy_plane(dst.solver._handle, dst_plane, src.solver._handle,
@@ -317,14 +318,16 @@ def exchange_ghosts(first_owned, last_owned, left_ghost, right_ghost, rank: int,
 class DistributedSlabRoom(_SlabSet):
     """This rank's part of a room cut into one slab per rank (one process per GPU).
 
-    The process group must be initialised; ``device`` is this rank's GPU (default: the local
-    rank). Recordings stay with the rank that owns each receiver; ``gather_recordings`` brings
-    them to one rank.
+    The process group must be initialised; ``device`` is this rank's GPU (default: the
+    library's current device -- pass the local rank unless CUDA_VISIBLE_DEVICES already narrows
+    the process to one GPU). Recordings stay with the rank that owns each receiver;
+    ``gather_recordings`` brings them to one rank.
     """
 
     def __init__(self, grid, medium=AIR, courant: float = 1.0, dtype=np.float64, walls=None,
                  absorbing_layer=None, air_absorption=None, *, device: int | None = None,
                  group=None, scheme: str = "two_sweeps") -> None:
+        import torch
         import torch.distributed as dist
 
         self.group = group
@@ -332,6 +335,8 @@ class DistributedSlabRoom(_SlabSet):
         self.world = dist.get_world_size(group)
         self.slab = SlabRoom(grid, medium, courant, dtype, walls, absorbing_layer, air_absorption,
                              part=self.rank, parts=self.world, device=device, scheme=scheme)
+        # NCCL's point-to-point calls run on torch's current device: make it this part's GPU.
+        torch.cuda.set_device(self.slab.solver.device)
         self.slabs = [self.slab]
         self.dt = self.slab.dt
         self._receivers: list[int | None] = []
