@@ -2123,24 +2123,28 @@ __global__ void bump_step_base(int64_t *base, int64_t by) { *base += by; }
 // ------------------------------------------------------------------------------------------
 // Energy terms of one room, FP64 accumulation (scheme.py:365-389). Two passes, fixed order:
 // block partial sums into a scratch array, then one block sums the partials.
-
+//
+// Over the x planes [i0, i1): the cells of those planes with their y and z faces, and the x
+// faces i0 .. i_faces - 1 (i_faces = i1, or i1 + 1 to take the far face nx too). The whole
+// room is i0 = 0, i1 = nx, i_faces = nx + 1; a slab of a larger room takes its owned planes.
 template <typename T>
 __global__ void __launch_bounds__(256) energy_partials(const Room<T> s, double inv_dx,
-                                                       double *partials) {
+                                                       double *partials, int i0, int i1,
+                                                       int i_faces) {
     double acc[kEnergyTerms];
 #pragma unroll
     for (int t = 0; t < kEnergyTerms; t++) acc[t] = 0.0;
 
-    const int64_t rows = (int64_t)(s.nx + 1) * (s.ny + 1);
+    const int64_t rows = (int64_t)(i_faces - i0) * (s.ny + 1);
     const int64_t total = rows * (s.nz + 1);
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < total;
          n += (int64_t)gridDim.x * blockDim.x) {
         const int k = (int)(n % (s.nz + 1));
         const int64_t row = n / (s.nz + 1);
         const int j = (int)(row % (s.ny + 1));
-        const int i = (int)(row / (s.ny + 1));
+        const int i = i0 + (int)(row / (s.ny + 1));
         const int64_t o = (int64_t)i * s.plane + (int64_t)j * s.pz + k;
-        const bool in_x = i < s.nx, in_y = j < s.ny, in_z = k < s.nz;
+        const bool in_x = i < i1, in_y = j < s.ny, in_z = k < s.nz;
         if (in_x && in_y && in_z) {
             const double p = (double)s.p[o];
             acc[0] += p * p;
@@ -2895,9 +2899,11 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
 }
 
 template <typename T>
-int energy_impl(acf_batch *b, int room, double dx, double *terms, cudaStream_t st) {
+int energy_impl(acf_batch *b, int room, double dx, double *terms, cudaStream_t st, int i0, int i1,
+                int i_faces) {
     const Room<T> s = make_room<T>(b, room);
-    energy_partials<T><<<b->energy_blocks, 256, 0, st>>>(s, 1.0 / dx, b->energy_scratch);
+    energy_partials<T><<<b->energy_blocks, 256, 0, st>>>(s, 1.0 / dx, b->energy_scratch, i0, i1,
+                                                         i_faces);
     energy_finish<<<1, 32, 0, st>>>(b->energy_scratch, b->energy_blocks,
                                     b->energy_scratch + (size_t)b->energy_blocks * kEnergyTerms);
     b->launches += 2;
@@ -3355,15 +3361,23 @@ int profile_enable(acf_batch *b, int32_t enable) {
     return ACF_OK;
 }
 
-int energy_terms(acf_batch *b, int room, double dx, double terms[7], acf_stream stream) {
+int energy_terms(acf_batch *b, int room, double dx, double terms[7], acf_stream stream,
+                 int64_t x_begin = 0, int64_t x_end = -1, int32_t far_face = 1) {
     int rc = check_room(b, room);
     if (rc) return rc;
     if (!terms) return fail(ACF_ERR_ARGUMENT, "null argument");
     if (!(dx > 0)) return fail(ACF_ERR_ARGUMENT, "dx must be positive");
+    const int nx = b->rooms[room].nx;
+    if (x_end < 0) x_end = nx;
+    if (x_begin < 0 || x_begin > x_end || x_end > nx)
+        return fail(ACF_ERR_ARGUMENT, "x planes [%lld, %lld) outside 0..%d", (long long)x_begin,
+                    (long long)x_end, nx);
+    const int i_faces = (int)x_end + (far_face && x_end == nx ? 1 : 0);
     DeviceGuard guard(b->device);
     cudaStream_t st = (cudaStream_t)stream;
-    return b->precision == 8 ? energy_impl<double>(b, room, dx, terms, st)
-                             : energy_impl<float>(b, room, dx, terms, st);
+    return b->precision == 8
+               ? energy_impl<double>(b, room, dx, terms, st, (int)x_begin, (int)x_end, i_faces)
+               : energy_impl<float>(b, room, dx, terms, st, (int)x_begin, (int)x_end, i_faces);
 }
 
 }  // namespace
@@ -4247,6 +4261,11 @@ int acf_set_launch(acf_solver *h, int32_t block_threads, int32_t planes) {
 
 int acf_energy_terms(acf_solver *h, double dx, double terms[7], acf_stream stream) {
     return energy_terms(h, 0, dx, terms, stream);
+}
+
+int acf_energy_terms_planes(acf_solver *h, double dx, int64_t x_begin, int64_t x_end,
+                            int32_t far_face, double terms[7], acf_stream stream) {
+    return energy_terms(h, 0, dx, terms, stream, x_begin, x_end, far_face);
 }
 
 int acf_field_pointer(acf_solver *h, int field, void **ptr, int64_t strides[3]) {

@@ -22,8 +22,8 @@ Two ways to run the parts:
   ``exchange_ghosts`` over ``torch.distributed`` (NCCL between GPUs; gloo in the CPU tests).
 
 The reference runs one room in one shared-memory process; the slab decomposition is this
-backend's addition. Energy is not offered on slabs (the sums would need the ghost cells and the
-cut faces taken out).
+backend's addition. Energy sums each part's owned cells and faces on its GPU
+(``acf_energy_terms_planes``) and adds the seven sums over the parts.
 """
 
 from __future__ import annotations
@@ -37,7 +37,7 @@ from .boundaries import FACES
 from .coefficients import room_coefficients
 from .grid import Grid, cell_index
 from .medium import AIR
-from .solver import CudaAcousticFDTD
+from .solver import CudaAcousticFDTD, energy_from_terms
 
 __all__ = ["slab_ranges", "slab_coefficients", "SlabRoom", "SlabGroup", "DistributedSlabRoom",
            "exchange_ghosts"]
@@ -160,6 +160,12 @@ class SlabRoom:
         cell = self.owned_cell(point)
         return None if cell is None else self.solver.add_pressure_receiver_at(cell)
 
+    def energy_terms(self) -> np.ndarray:
+        """The seven energy sums over this part's owned cells and faces (the room's far x face
+        on the last part); the parts' sums add up to the whole room's."""
+        return self.solver.energy_terms(planes=(self.first_owned, self.last_owned + 1),
+                                        far_face=not self.has_right)
+
     def plane_view(self, plane: int):
         """A torch tensor over local p plane ``plane`` in device memory (no copy)."""
         import torch
@@ -266,6 +272,12 @@ class SlabGroup(_SlabSet):
     def synchronize(self) -> None:
         for s in self.slabs:
             s.solver.synchronize()
+
+    def energy(self) -> float:
+        """The whole room's acoustic energy (``CudaAcousticFDTD.energy``), from every part's sums."""
+        solver = self.slabs[0].solver
+        terms = np.sum([s.energy_terms() for s in self.slabs], axis=0)
+        return energy_from_terms(terms, solver.medium, float(solver.grid.dx), self.dt)
 
     @property
     def p(self) -> np.ndarray:
@@ -379,6 +391,19 @@ class DistributedSlabRoom(_SlabSet):
     def p(self) -> np.ndarray:
         """This rank's owned planes of p."""
         return self._assemble(lambda s: s.solver.p)
+
+    def energy(self) -> float:
+        """The whole room's acoustic energy: every rank's sums, all-reduced (collective)."""
+        import torch
+        import torch.distributed as dist
+
+        terms = torch.tensor(self.slab.energy_terms(), dtype=torch.float64)
+        if dist.get_backend(self.group) == "nccl":
+            terms = terms.cuda(self.slab.solver.device)
+        dist.all_reduce(terms, group=self.group)
+        solver = self.slab.solver
+        return energy_from_terms(terms.cpu().numpy(), solver.medium, float(solver.grid.dx),
+                                 self.dt)
 
     def gather_recordings(self, dst: int = 0) -> np.ndarray | None:
         """Every receiver's recording on rank ``dst`` (None elsewhere)."""

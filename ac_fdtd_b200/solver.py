@@ -60,6 +60,20 @@ def config_from_block(block):
     return config, keep
 
 
+def energy_from_terms(terms, medium, dx: float, dt: float) -> float:
+    """The reference's energy (``scheme.py:365-389``) from the seven sums of ``acf_energy_terms``:
+    dx^3 (sum p^2 / (2 rho c^2) + sum rho v^2 / 2 - dt/2 sum v . grad p)."""
+    rho = float(medium.density)
+    c = float(medium.sound_speed)
+    potential = terms[0] / (2.0 * rho * c**2)
+    kinetic = 0.0
+    coupling = 0.0
+    for axis in range(3):
+        kinetic += 0.5 * rho * terms[1 + axis]
+        coupling += terms[4 + axis]
+    return dx**3 * (potential + kinetic - 0.5 * dt * coupling)
+
+
 def _free_native(handle):
     if handle:
         _native.library().acf_destroy(handle)
@@ -444,13 +458,22 @@ class CudaAcousticFDTD:
                                "the solver state is not valid")
 
     # ------------------------------------------------------------------ diagnostics
-    def energy_terms(self) -> np.ndarray:
-        """The seven FP64 device sums behind :meth:`energy` (see ``acf_energy_terms``)."""
+    def energy_terms(self, planes: tuple[int, int] | None = None,
+                     far_face: bool = True) -> np.ndarray:
+        """The seven FP64 device sums behind :meth:`energy` (see ``acf_energy_terms``);
+        ``planes=(x_begin, x_end)`` restricts them to those x planes (``far_face``: with the
+        face nx when x_end = nx), as a slab of a larger room needs."""
         self._flush()
         terms = np.zeros(7)
-        _native.check(self._lib.acf_energy_terms(self._handle, float(self.grid.dx),
-                                                 _as_double_pointer(terms), self._stream),
-                      "acf_energy_terms")
+        if planes is None:
+            _native.check(self._lib.acf_energy_terms(self._handle, float(self.grid.dx),
+                                                     _as_double_pointer(terms), self._stream),
+                          "acf_energy_terms")
+        else:
+            _native.check(self._lib.acf_energy_terms_planes(
+                self._handle, float(self.grid.dx), int(planes[0]), int(planes[1]),
+                int(bool(far_face)), _as_double_pointer(terms), self._stream),
+                "acf_energy_terms_planes")
         return terms
 
     def energy(self) -> float:
@@ -458,16 +481,7 @@ class CudaAcousticFDTD:
 
         The sums are accumulated in FP64 on the device in either precision.
         """
-        terms = self.energy_terms()
-        rho = float(self.medium.density)
-        c = float(self.medium.sound_speed)
-        potential = terms[0] / (2.0 * rho * c**2)
-        kinetic = 0.0
-        coupling = 0.0
-        for axis in range(3):
-            kinetic += 0.5 * rho * terms[1 + axis]
-            coupling += terms[4 + axis]
-        return float(self.grid.dx) ** 3 * (potential + kinetic - 0.5 * self.dt * coupling)
+        return energy_from_terms(self.energy_terms(), self.medium, float(self.grid.dx), self.dt)
 
     def set_coefficients(self, walls=None, absorbing_layer=None, air_absorption=None) -> None:
         """Replace the wall, layer and air coefficients, keeping the grid and the state.

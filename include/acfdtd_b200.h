@@ -178,6 +178,11 @@ int acf_set_launch(acf_solver *solver, int32_t block_threads, int32_t planes);
  * pair (src/ac_fdtd/scheme.py:365-389): terms[0] = sum p^2; terms[1+a] = sum v_a^2 over all
  * faces; terms[4+a] = sum over interior faces of v_a * (p_hi - p_lo) / dx. Synchronous. */
 int acf_energy_terms(acf_solver *solver, double dx, double terms[7], acf_stream stream);
+/* The same sums over the x planes [x_begin, x_end) only: their cells (with their y and z
+ * faces) and the x faces x_begin .. x_end - 1, plus the far face nx when x_end = nx and
+ * far_face is set. The parts of a room cut into x slabs sum to the whole room's terms. */
+int acf_energy_terms_planes(acf_solver *solver, double dx, int64_t x_begin, int64_t x_end,
+                            int32_t far_face, double terms[7], acf_stream stream);
 
 /* ---- Adjoint (single rooms) ----------------------------------------------------------
  *

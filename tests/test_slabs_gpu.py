@@ -71,6 +71,8 @@ def test_slabs_equal_the_whole_room_bitwise(parts, dtype, scheme):
     group.run(steps - 23)
     assert group.step_index == steps
     assert_same(group, whole)
+    # energy: every part's sums over its owned cells and faces add up to the whole room's
+    assert group.energy() == pytest.approx(whole.energy(), rel=1e-11, abs=0)
     group.close()
     whole.close()
 
@@ -86,6 +88,24 @@ def test_slabs_match_the_oracle():
     np.testing.assert_array_equal(group.p, oracle.p)
     np.testing.assert_array_equal(group.recorded_pressure, oracle.recorded_pressure)
     group.close()
+
+
+def test_energy_over_plane_ranges_adds_up_to_the_room():
+    whole = CudaAcousticFDTD(GRID, dtype=np.float64, **CONFIG)
+    populate(whole, 25)
+    whole.run(25)
+    terms = whole.energy_terms()
+    np.testing.assert_array_equal(whole.energy_terms(planes=(0, GRID.nx)), terms)
+    for cut in (1, 6, 12):
+        parts = whole.energy_terms(planes=(0, cut)) + whole.energy_terms(planes=(cut, GRID.nx))
+        for got, want in zip(parts, terms, strict=True):   # another summation order only
+            assert got == pytest.approx(want, rel=1e-9)
+    without_far = whole.energy_terms(planes=(0, GRID.nx), far_face=False)
+    np.testing.assert_array_equal(without_far[[0, 2, 3, 4, 5, 6]], terms[[0, 2, 3, 4, 5, 6]])
+    assert without_far[1] <= terms[1]
+    with pytest.raises(RuntimeError):
+        whole.energy_terms(planes=(3, GRID.nx + 1))
+    whole.close()
 
 
 def test_plane_views_address_the_solvers_planes():
@@ -121,6 +141,7 @@ def test_a_one_rank_distributed_room_is_the_whole_room():
         whole.run(steps)
         np.testing.assert_array_equal(room.p, whole.p)
         np.testing.assert_array_equal(room.gather_recordings(), whole.recorded_pressure)
+        assert room.energy() == whole.energy()
         room.close()
     finally:
         dist.destroy_process_group()
