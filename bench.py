@@ -352,6 +352,7 @@ def run_ours(args) -> None:
     adjoint = None if args.skip_extras else adjoint_cost(args)
     inversion = None if args.skip_extras else batched_adjoint_cost(args)
     precision = None if args.skip_extras else precision_check(args)
+    slabs = None if args.skip_extras else slab_overhead(args)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -372,6 +373,7 @@ def run_ours(args) -> None:
         "adjoint": adjoint,
         "batched_inversion": inversion,
         "precision": precision,
+        "slabs_one_gpu": slabs,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -383,6 +385,39 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def slab_overhead(args) -> dict:
+    """The x-slab decomposition's own cost with every part on this GPU: the headline room whole
+    and cut into 2 and 4 slabs (fused scheme, 300 steps), recordings compared bit for bit."""
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse
+    from ac_fdtd_b200.slabs import SlabGroup
+
+    grid, objects, points = workload(args.size)
+    T, warm = 300, 20
+    out = {"workload": f"the headline room, {args.size}^3 fp32, fused scheme, {T} steps, every "
+                       f"part on one GPU (ghost planes by device copies)"}
+    whole_recording = None
+    for parts in (1, 2, 4):
+        room = (CudaAcousticFDTD(grid, dtype=np.float32, scheme="fused", **objects) if parts == 1
+                else SlabGroup(grid, dtype=np.float32, parts=parts, scheme="fused", **objects))
+        room.add_volume_source(points[0], gaussian_pulse(T + warm, room.dt, 4000.0))
+        for point in points[1:]:
+            room.add_pressure_receiver(point)
+        room.run(warm)
+        room.synchronize()
+        ms = _device_ms(lambda room=room: room.run(T), torch)
+        recording = room.recorded_pressure
+        if whole_recording is None:
+            whole_recording = recording
+        out[f"parts_{parts}"] = {
+            "gcups": grid.n_cells * T / (ms * 1e-3) / 1e9,
+            "recordings_bitwise_equal_to_whole_room": bool(np.array_equal(recording, whole_recording)),
+        }
+        room.close()
+    return out
 
 
 def _errors(single, double) -> dict:

@@ -247,6 +247,24 @@ def test_l2_prefetch_forced_on_matches_the_oracle(dtype, scheme):
     assert_same_state(cuda, oracle)
 
 
+def test_l2_prefetch_follows_the_size_of_the_fields():
+    """On by default once the fields a step streams exceed L2 (126 MB on a B200): a 200^3
+    fp32 room's seven fields take 235 MB; a 96^3 room's 27 MB, or 43 MB with the fused
+    scheme's second copy of p and v."""
+    from ac_fdtd_b200 import AirAbsorption, Grid
+
+    big = CudaAcousticFDTD(Grid(dx=0.02, nx=200, ny=200, nz=200), dtype=np.float32,
+                           air_absorption=AirAbsorption())
+    small = CudaAcousticFDTD(Grid(dx=0.02, nx=96, ny=96, nz=96), dtype=np.float32,
+                             air_absorption=AirAbsorption(), scheme="fused")
+    assert big.prefetch and not small.prefetch
+    big.set_prefetch(False)
+    small.set_prefetch(True)
+    assert small.prefetch and not big.prefetch
+    big.close()
+    small.close()
+
+
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_staged_geometries_match_the_oracle(dtype):
     """Rows per CTA, ring depth and planes per CTA change only which CTA computes a cell and
