@@ -145,3 +145,37 @@ def test_gloo_ranks_exchanging_ghost_planes_reproduce_the_whole_array(world):
         assert p.exitcode == 0
     assembled = np.concatenate([part for _, _, part in parts])
     np.testing.assert_array_equal(assembled, _stencil(u0, steps))
+
+
+# ---------------------------------------------------------------- point routing (stub ABI)
+
+@pytest.fixture
+def stub(monkeypatch):
+    from ac_fdtd_b200 import _native
+    from tests.test_host_logic import StubLibrary
+
+    lib = StubLibrary()
+    monkeypatch.setattr(_native, "_lib", lib)
+    monkeypatch.setattr(_native, "library", lambda: lib)
+    return lib
+
+
+def test_points_go_to_the_part_owning_their_cell(stub):
+    from ac_fdtd_b200.slabs import SlabGroup
+
+    grid = Grid(dx=0.05, nx=10, ny=4, nz=5)
+    group = SlabGroup(grid, dtype=np.float32, parts=3, walls=WallAdmittances.uniform(0.2))
+    assert [(s.x0, s.x1, s.gx0) for s in group.slabs] == [(0, 4, 0), (4, 7, 3), (7, 10, 6)]
+    assert [s.solver.coefficients.shape[0] for s in group.slabs] == [5, 5, 4]
+    for x, part in ((0.0, 0), (0.199, 0), (0.2, 1), (0.349, 1), (0.35, 2), (0.5, 2), (9.0, 2)):
+        owners = [s.owned_cell((x, 0.1, 0.1)) for s in group.slabs]
+        assert [q for q, c in enumerate(owners) if c is not None] == [part], x
+        i = grid.cell_index((x, 0.1, 0.1))[0]
+        assert owners[part] == (i - group.slabs[part].gx0, 2, 2)
+    receivers = [group.add_pressure_receiver((x, 0.1, 0.1)) for x in (0.46, 0.01, 0.3)]
+    assert receivers == [0, 1, 2]
+    assert group._receivers == [(2, 0), (0, 0), (1, 0)]
+    group.add_volume_source((0.26, 0.1, 0.1), np.ones(3))
+    assert [len(s.solver._sources) for s in group.slabs] == [0, 1, 0]
+    flat, _ = group.slabs[1].solver._sources[0]
+    assert np.unravel_index(flat, group.slabs[1].solver._shape) == (2, 2, 2)
