@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
     "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch", "acf_copy_plane",
-    "acf_solver_device", "acf_energy_terms_planes",
+    "acf_solver_device", "acf_energy_terms_planes", "acf_run_slabs",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED = 0, 1, 2
@@ -146,6 +146,8 @@ _SIGNATURES = {
     "acf_copy_plane": (ctypes.c_int, [_P, _I64, _P, _I64, ctypes.c_int, _P]),
     "acf_solver_device": (ctypes.c_int, [_P]),
     "acf_energy_terms_planes": (ctypes.c_int, [_P, ctypes.c_double, _I64, _I64, ctypes.c_int32, _DP, _P]),
+    "acf_run_slabs": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                     ctypes.POINTER(ctypes.c_int32), _I64, _I64, _P]),
 }
 
 

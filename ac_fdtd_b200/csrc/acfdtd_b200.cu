@@ -131,6 +131,12 @@ struct Room {
     int32_t nx, ny, nz, nchunks;
     int32_t prefetch;              // 1: marching threads ask L2 for their next plane ahead
     int32_t reserved;
+    // A slab of a room cut along x: the single-room pressure sweep updates the planes
+    // [own_lo, own_hi) only, and also stores p of planes own_lo and own_hi - 1 into the
+    // neighbours' ghost planes (null: no neighbour on that side; a peer address when the
+    // neighbour lives on another GPU). A whole room: [0, nx), no ghosts.
+    int32_t own_lo, own_hi;
+    T *ghost_lo, *ghost_hi;
     int64_t pz, plane, field;      // row pitch, plane pitch, elements per field
     T *p, *vx, *vy, *vz, *psi;     // psi: n_relax fields back to back
     T cv, cp, cs, relax_scale;
@@ -547,6 +553,9 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
 
         // ---- stores
         Vec4<T>::store(s.p + base, Pn);
+        // A slab's boundary planes also go to the neighbours' ghost planes (same in-plane offset).
+        if (s.ghost_lo != nullptr && i == s.own_lo) Vec4<T>::store(s.ghost_lo + column, Pn);
+        if (s.ghost_hi != nullptr && i == s.own_hi - 1) Vec4<T>::store(s.ghost_hi + column, Pn);
 #pragma unroll
         for (int r = 0; r < NR; r++) Vec4<T>::store(s.psi + r * s.field + base, S[r]);
         if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
@@ -1384,9 +1393,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 2 : 4)) pressure_sweep(
     if (c >= p.room.nchunks || j >= p.room.ny) return;
     const bool any_point = (p.room.n_src | p.room.n_rec) != 0;
     const int64_t step = any_point ? (*p.step_base + p.local_step) : 0;
-    const int i_begin = blockIdx.z * p.planes;
-    pressure_column<T, LAYER, WALLS, NR>(p.room, i_begin, min(p.room.nx, i_begin + p.planes), j,
-                                         c, step);
+    const int first = blockIdx.z * p.planes;
+    const int i_begin = max(first, p.room.own_lo);
+    const int i_end = min(min(p.room.nx, first + p.planes), p.room.own_hi);
+    if (i_begin >= i_end) return;   // planes outside a slab's own range (its ghost planes)
+    pressure_column<T, LAYER, WALLS, NR>(p.room, i_begin, i_end, j, c, step);
 }
 
 // The same pressure sweep, also writing the forward history the adjoint needs.
@@ -2477,6 +2488,8 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     s.nz = h.nz;
     s.nchunks = (int32_t)((h.nz + kVec - 1) / kVec);
     s.prefetch = prefetch_planes(b) ? 1 : 0;
+    s.own_lo = 0;
+    s.own_hi = h.nx;
     s.pz = h.pz;
     s.plane = h.plane;
     s.field = h.field;
@@ -3291,13 +3304,8 @@ int read_recording(acf_batch *b, int room, int64_t r, int64_t first_step, int64_
     return ACF_OK;
 }
 
-int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
-    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
-    if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
-    if (n_steps == 0) return ACF_OK;
-    DeviceGuard guard(b->device);
-    cudaStream_t st = (cudaStream_t)stream;
-    // Recording capacity for every step this run can write.
+// Recording capacity for every step a run of [step_offset, step_offset + n_steps) can write.
+int ensure_recording(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st) {
     for (RoomHost &h : b->rooms) {
         if (h.n_rec == 0) continue;
         const int64_t need = step_offset + n_steps - h.rec_origin;
@@ -3317,8 +3325,152 @@ int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream str
         b->graph_dirty = b->adj_graphs_dirty = true;
         b->room_table_dirty = true;
     }
+    return ACF_OK;
+}
+
+int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
+    if (n_steps == 0) return ACF_OK;
+    DeviceGuard guard(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_recording(b, n_steps, step_offset, st);
+    if (rc) return rc;
     return b->precision == 8 ? run_impl<double>(b, n_steps, step_offset, st)
                              : run_impl<float>(b, n_steps, step_offset, st);
+}
+
+// A room cut into x slabs, one single-room two-sweep solver per part, advanced together. Each
+// step launches every part's velocity sweep, then every part's pressure sweep; a pressure
+// sweep updates its own planes only and stores its first and last of them into the
+// neighbours' ghost planes as well (peer stores when a neighbour lives on another GPU), so no
+// exchange follows the step. Parts on one GPU run in launch order on `st`. Parts on several
+// GPUs run on each device's default stream, ordered by events and never by a wait inside a
+// kernel: a velocity sweep waits for the neighbours' pressure sweeps of the previous step
+// (they wrote its ghost planes), a pressure sweep for the neighbours' velocity sweeps of the
+// same step (they read the ghost planes it overwrites).
+template <typename T>
+int run_slabs_impl(acf_batch *const *parts, int n, const int32_t *own_lo, const int32_t *own_hi,
+                   int64_t n_steps, int64_t step_offset, cudaStream_t st) {
+    bool one_device = true;
+    for (int q = 1; q < n; q++) one_device = one_device && parts[q]->device == parts[0]->device;
+    std::vector<StepParams<T>> params((size_t)n);
+    std::vector<LaunchShape> shapes((size_t)n);
+    for (int q = 0; q < n; q++) {
+        acf_batch *b = parts[q];
+        StepParams<T> &p = params[q];
+        p.room = make_room<T>(b, 0);
+        p.room.own_lo = own_lo[q];
+        p.room.own_hi = own_hi[q];
+        if (q > 0)   // the left neighbour's right ghost plane: just past its own planes
+            p.room.ghost_lo = (T *)parts[q - 1]->field_ptr(0, ACF_FIELD_P) + (int64_t)own_hi[q - 1] * p.room.plane;
+        if (q + 1 < n)   // the right neighbour's left ghost plane: just before its own planes
+            p.room.ghost_hi = (T *)parts[q + 1]->field_ptr(0, ACF_FIELD_P) + (int64_t)(own_lo[q + 1] - 1) * p.room.plane;
+        p.step_base = b->step_base;
+        p.planes = b->planes;
+        shapes[q] = single_shape(b);
+    }
+    std::vector<cudaStream_t> streams((size_t)n, one_device ? st : (cudaStream_t)0);
+    std::vector<cudaEvent_t> vel_done((size_t)n, nullptr), pres_done((size_t)n, nullptr);
+    auto release = [&]() {
+        for (int q = 0; q < n; q++) {
+            DeviceGuard g(parts[q]->device);
+            if (vel_done[q]) cudaEventDestroy(vel_done[q]);
+            if (pres_done[q]) cudaEventDestroy(pres_done[q]);
+        }
+    };
+    if (!one_device) {
+        for (int q = 0; q < n; q++) {
+            DeviceGuard g(parts[q]->device);
+            for (int r : {q - 1, q + 1}) {
+                if (r < 0 || r >= n || parts[r]->device == parts[q]->device) continue;
+                int can = 0;
+                cudaDeviceCanAccessPeer(&can, parts[q]->device, parts[r]->device);
+                if (!can) {
+                    release();
+                    return fail(ACF_ERR_STATE, "GPU %d cannot store into GPU %d's memory",
+                                parts[q]->device, parts[r]->device);
+                }
+                const cudaError_t e = cudaDeviceEnablePeerAccess(parts[r]->device, 0);
+                if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+                else if (e != cudaSuccess) {
+                    release();
+                    return fail(ACF_ERR_CUDA, "peer access %d -> %d: %s", parts[q]->device,
+                                parts[r]->device, cudaGetErrorString(e));
+                }
+            }
+            if (cudaEventCreateWithFlags(&vel_done[q], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&pres_done[q], cudaEventDisableTiming) != cudaSuccess) {
+                release();
+                return fail(ACF_ERR_CUDA, "event creation failed");
+            }
+        }
+    }
+    auto wait_neighbours = [&](int q, const std::vector<cudaEvent_t> &done) {
+        for (int r : {q - 1, q + 1})
+            if (r >= 0 && r < n) cudaStreamWaitEvent(streams[q], done[r], 0);
+    };
+    for (int q = 0; q < n; q++) {
+        DeviceGuard g(parts[q]->device);
+        set_step_base<<<1, 1, 0, streams[q]>>>(parts[q]->step_base, step_offset);
+        parts[q]->launches += 1;
+    }
+    for (int64_t t = 0; t < n_steps; t++) {
+        for (int q = 0; q < n; q++) {
+            DeviceGuard g(parts[q]->device);
+            if (!one_device && t > 0) wait_neighbours(q, pres_done);
+            StepParams<T> &p = params[q];
+            p.local_step = (int32_t)t;
+            const LaunchShape &L = shapes[q];
+            if (parts[q]->rooms[0].has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, streams[q]>>>(p);
+            else velocity_sweep<T, false><<<L.grid, L.block, 0, streams[q]>>>(p);
+            if (!one_device) cudaEventRecord(vel_done[q], streams[q]);
+        }
+        for (int q = 0; q < n; q++) {
+            DeviceGuard g(parts[q]->device);
+            if (!one_device) wait_neighbours(q, vel_done);
+            const RoomHost &h = parts[q]->rooms[0];
+            dispatch_pressure<T, SinglePressure>(h.has_layer, h.has_walls, h.n_relax, params[q],
+                                                 shapes[q].grid, shapes[q].block, streams[q]);
+            if (!one_device) cudaEventRecord(pres_done[q], streams[q]);
+            parts[q]->launches += 2;
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    release();
+    if (e != cudaSuccess) return fail(ACF_ERR_CUDA, "slab step: %s", cudaGetErrorString(e));
+    return ACF_OK;
+}
+
+int run_slabs(acf_solver *const *parts, int32_t n, const int32_t *own_lo, const int32_t *own_hi,
+              int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    if (!parts || !own_lo || !own_hi || n < 1) return fail(ACF_ERR_ARGUMENT, "null or empty part list");
+    if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
+    for (int q = 0; q < n; q++) {
+        const acf_batch *b = parts[q];
+        if (!b) return fail(ACF_ERR_ARGUMENT, "null part %d", q);
+        const RoomHost &h = b->rooms[0];
+        const RoomHost &h0 = parts[0]->rooms[0];
+        if (b->scheme != ACF_SCHEME_TWO_SWEEPS)
+            return fail(ACF_ERR_STATE, "part %d: slabs step with the two-sweep scheme", q);
+        if (b->precision != parts[0]->precision || h.ny != h0.ny || h.nz != h0.nz)
+            return fail(ACF_ERR_ARGUMENT, "part %d differs in precision, ny or nz", q);
+        const bool left = q > 0, right = q + 1 < n;
+        if (own_lo[q] != (left ? 1 : 0) || own_hi[q] <= own_lo[q] || own_hi[q] != h.nx - (right ? 1 : 0))
+            return fail(ACF_ERR_ARGUMENT, "part %d: own planes [%d, %d) do not fit %d planes with "
+                        "ghosts", q, own_lo[q], own_hi[q], h.nx);
+    }
+    if (n_steps == 0) return ACF_OK;
+    for (int q = 0; q < n; q++) {
+        DeviceGuard g(parts[q]->device);
+        int rc = ensure_recording(parts[q], n_steps, step_offset, (cudaStream_t)stream);
+        if (rc) return rc;
+    }
+    DeviceGuard guard(parts[0]->device);
+    acf_batch *const *b = (acf_batch *const *)parts;
+    return parts[0]->precision == 8
+               ? run_slabs_impl<double>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream)
+               : run_slabs_impl<float>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream);
 }
 
 int set_launch(acf_batch *b, int32_t block_threads, int32_t planes, int32_t ctas_per_sm) {
@@ -4304,6 +4456,11 @@ int acf_copy_plane(acf_solver *dst, int64_t dst_plane, const acf_solver *src, in
 }
 
 int acf_solver_device(const acf_solver *h) { return h ? h->device : -1; }
+
+int acf_run_slabs(acf_solver *const *parts, int32_t n_parts, const int32_t *own_lo,
+                  const int32_t *own_hi, int64_t n_steps, int64_t step_offset, acf_stream stream) {
+    return run_slabs(parts, n_parts, own_lo, own_hi, n_steps, step_offset, stream);
+}
 
 int acf_profile_enable(acf_solver *h, int32_t enable) { return profile_enable(h, enable); }
 

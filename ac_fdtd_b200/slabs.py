@@ -11,13 +11,17 @@ After every step each part sends its first owned p plane to the left neighbour's
 and its last owned p plane to the right neighbour's left ghost. The next velocity sweep then
 computes every owned face, including the two faces shared with ghosts, from current pressures,
 so only pressure planes travel: (ny + 1) x pz elements each way per cut and step (604 KB at
-384^2 fp32 in the padded layout). Ghost cells are themselves updated by the sweeps and then
-overwritten by the exchange; nothing owned reads them in between.
+384^2 fp32 in the padded layout). Nothing owned reads a ghost cell except that pressure, in
+the velocity sweep; where the sweeps also update ghost cells (the copy path), the exchange
+overwrites them before the next step.
 
 Two ways to run the parts:
 
-* ``SlabGroup`` -- every part in this process (one GPU or several), planes copied by
-  ``acf_copy_plane`` on the device;
+* ``SlabGroup`` -- every part in this process (one GPU or several). With the two-sweep scheme
+  the exchange is fused into the pressure sweep: each part's sweep stores its first and last
+  own planes straight into the neighbours' ghost planes (peer stores across GPUs,
+  ``acf_run_slabs``), and the steps are ordered so that no kernel waits on another; the other
+  schemes copy the ghost planes after each step (``acf_copy_plane``);
 * ``DistributedSlabRoom`` -- this rank's part, one process per GPU, planes exchanged by
   ``exchange_ghosts`` over ``torch.distributed`` (NCCL between GPUs; gloo in the CPU tests).
 
@@ -28,6 +32,7 @@ backend's addition. Energy sums each part's owned cells and faces on its GPU
 
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 
 import numpy as np
@@ -258,12 +263,27 @@ class SlabGroup(_SlabSet):
                 s.solver.synchronize()
 
     def run(self, n_steps: int) -> None:
+        """Advance every part. With the two-sweep scheme each pressure sweep also stores its
+        boundary planes into the neighbours' ghost planes (``acf_run_slabs``: no exchange step);
+        the other schemes step part by part and copy the ghost planes after each step."""
         n_steps = int(n_steps)
         if n_steps <= 0:
             return
         for s in self.slabs:
             s.solver.flush()      # state written on the host reaches the device first
-        self.exchange()
+        self.exchange()           # ghost planes from the current state
+        if all(s.solver.scheme == "two_sweeps" for s in self.slabs):
+            n = len(self.slabs)
+            for s in self.slabs:
+                s.solver.prepare_points()
+            handles = (ctypes.c_void_p * n)(*[s.solver._handle.value for s in self.slabs])
+            own_lo = (ctypes.c_int32 * n)(*[s.first_owned for s in self.slabs])
+            own_hi = (ctypes.c_int32 * n)(*[s.last_owned + 1 for s in self.slabs])
+            _native.check(self._lib.acf_run_slabs(handles, n, own_lo, own_hi, n_steps,
+                                                  self.step_index, None), "acf_run_slabs")
+            for s in self.slabs:
+                s.solver.advanced(n_steps)
+            return
         for _ in range(n_steps):
             for s in self.slabs:
                 s.solver.run(1)

@@ -429,6 +429,16 @@ class CudaAcousticFDTD:
         """Upload what was written into the host snapshots now (``run`` does it by itself)."""
         self._flush()
 
+    def prepare_points(self) -> None:
+        """Push added sources and receivers to the device now (``run`` does it by itself); for
+        callers that advance the solver through another entry point (``acf_run_slabs``)."""
+        self._push_points()
+
+    def advanced(self, n_steps: int) -> None:
+        """Record that another entry point advanced this solver by ``n_steps``."""
+        self.step_index += int(n_steps)
+        self._mirror_current.clear()
+
     @property
     def device(self) -> int:
         """The GPU this solver's state lives on."""

@@ -389,7 +389,17 @@ def run_ours(args) -> None:
 
 def slab_overhead(args) -> dict:
     """The x-slab decomposition's own cost with every part on this GPU: the headline room whole
-    and cut into 2 and 4 slabs (fused scheme, 300 steps), recordings compared bit for bit."""
+    and cut into 2 and 4 slabs (300 steps), recordings compared bit for bit. Two sweeps: the
+    pressure sweep stores the boundary planes into the neighbours' ghosts (acf_run_slabs);
+    fused scheme: the ghost planes are copied after each step."""
+    out = {"workload": f"the headline room, {args.size}^3 fp32, 300 steps, every part on one GPU"}
+    for scheme, path in (("two_sweeps", "exchange fused into the pressure sweep"),
+                         ("fused", "ghost planes copied after each step")):
+        out[scheme] = {"exchange": path, **_slab_runs(args, scheme)}
+    return out
+
+
+def _slab_runs(args, scheme: str) -> dict:
     import torch
 
     from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse
@@ -397,12 +407,11 @@ def slab_overhead(args) -> dict:
 
     grid, objects, points = workload(args.size)
     T, warm = 300, 20
-    out = {"workload": f"the headline room, {args.size}^3 fp32, fused scheme, {T} steps, every "
-                       f"part on one GPU (ghost planes by device copies)"}
+    out = {}
     whole_recording = None
     for parts in (1, 2, 4):
-        room = (CudaAcousticFDTD(grid, dtype=np.float32, scheme="fused", **objects) if parts == 1
-                else SlabGroup(grid, dtype=np.float32, parts=parts, scheme="fused", **objects))
+        room = (CudaAcousticFDTD(grid, dtype=np.float32, scheme=scheme, **objects) if parts == 1
+                else SlabGroup(grid, dtype=np.float32, parts=parts, scheme=scheme, **objects))
         room.add_volume_source(points[0], gaussian_pulse(T + warm, room.dt, 4000.0))
         for point in points[1:]:
             room.add_pressure_receiver(point)

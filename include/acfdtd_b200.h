@@ -261,6 +261,18 @@ int acf_copy_plane(acf_solver *dst, int64_t dst_plane, const acf_solver *src, in
 /* The GPU a solver's state lives on (-1 for a null solver). No counterpart in the reference. */
 int acf_solver_device(const acf_solver *solver);
 
+/* Advance a room cut into x slabs: parts[q] holds slab q (left to right) with its ghost planes,
+ * its own planes being [own_lo[q], own_hi[q]) -- own_lo = 1 where a left neighbour exists else
+ * 0, own_hi = nx - 1 where a right neighbour exists else nx. Each step runs every part's
+ * velocity sweep, then every part's pressure sweep, which updates its own planes and also stores
+ * its first and last own planes of p into the neighbours' ghost planes (peer stores across
+ * GPUs; peer access is enabled as needed). The ghost planes must hold the neighbours' p before
+ * the first step (acf_copy_plane). Two-sweep scheme, single rooms of equal precision, ny and
+ * nz. Parts on one GPU run on `stream`; parts on several GPUs on each device's default stream,
+ * ordered by events. Asynchronous. No counterpart in the reference. */
+int acf_run_slabs(acf_solver *const *parts, int32_t n_parts, const int32_t *own_lo,
+                  const int32_t *own_hi, int64_t n_steps, int64_t step_offset, acf_stream stream);
+
 /* Instrumentation: when enabled, acf_run launches step by step with CUDA events around each
  * sweep and accumulates their device time. */
 int acf_profile_enable(acf_solver *solver, int32_t enable);

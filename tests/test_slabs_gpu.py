@@ -145,3 +145,25 @@ def test_a_one_rank_distributed_room_is_the_whole_room():
         room.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_the_slab_runner_refuses_parts_that_do_not_fit():
+    import ctypes
+
+    from ac_fdtd_b200 import _native
+
+    group = SlabGroup(GRID, dtype=np.float32, parts=2, **CONFIG)
+    lib = _native.library()
+    handles = (ctypes.c_void_p * 2)(*[s.solver._handle.value for s in group.slabs])
+    good_lo = [s.first_owned for s in group.slabs]
+    good_hi = [s.last_owned + 1 for s in group.slabs]
+    for lo, hi in (([1, 1], good_hi), (good_lo, [good_hi[0] + 1, good_hi[1]]),
+                   (good_lo, [good_hi[0], good_hi[1] - 1])):
+        status = lib.acf_run_slabs(handles, 2, (ctypes.c_int32 * 2)(*lo),
+                                   (ctypes.c_int32 * 2)(*hi), 1, 0, None)
+        assert status == 1          # ACF_ERR_ARGUMENT, before any launch
+    group.slabs[1].solver.set_scheme("fused")
+    status = lib.acf_run_slabs(handles, 2, (ctypes.c_int32 * 2)(*good_lo),
+                               (ctypes.c_int32 * 2)(*good_hi), 1, 0, None)
+    assert status == 4              # ACF_ERR_STATE: the runner steps two-sweep parts
+    group.close()
