@@ -201,7 +201,7 @@ class _DeviceArray:
 
 
 class _SlabSet:
-    """Receivers, recordings and assembled fields over a list of parts (all or this rank's)."""
+    """Fields assembled over a list of parts (every part, or this rank's)."""
 
     slabs: list[SlabRoom]
 
@@ -210,8 +210,10 @@ class _SlabSet:
 
 
 class SlabGroup(_SlabSet):
-    """Every part of one room in this process, stepped in lockstep with device plane copies.
+    """Every part of one room in this process, stepped in lockstep.
 
+    With the two-sweep scheme the ghost exchange is part of each pressure sweep (peer stores,
+    ``acf_run_slabs``); with the others the ghost planes are copied after each step.
     ``devices`` (optional) lists the GPU of each part (cycled); by default all parts share the
     library's current device. Results equal ``CudaAcousticFDTD`` on the whole room bit for bit.
     """
