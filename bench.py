@@ -12,7 +12,9 @@ to 4 kHz at a seeded interior cell and four seeded receivers, 4000 leapfrog step
 goes through the public API with host buffers: upload the full state from pinned host memory,
 run, read back the recordings and the final pressure. The reference arm times the reference's
 own compiled C backend (``oracle/_ref``) on the host cores over a bounded sample of the same
-workload. Multi-GPU runs are independent replicas of the room (one per rank, weak scaling).
+workload. Multi-GPU runs are independent replicas of the room (one per rank, weak scaling);
+``--slabs`` cuts the one room into an x slab per rank instead (strong scaling, one line with
+``value`` and clocks only).
 """
 
 from __future__ import annotations
@@ -205,6 +207,75 @@ def physical_gpu(local: int) -> str:
     """The GPU (index or UUID, as CUDA_VISIBLE_DEVICES names it) that local rank `local` runs on."""
     visible = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
     return visible[local] if local < len(visible) else str(local)
+
+
+def run_slab_mode(args) -> None:
+    """``--slabs``: the headline room cut into one x slab per rank, a ghost p plane exchanged
+    each way per cut and step (``DistributedSlabRoom``; one batched isend/irecv over NCCL), for
+    strong scaling of one room. The default mode (replicas) gives the headline line."""
+    import datetime
+    import socket
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    gpu = physical_gpu(int(os.environ.get("LOCAL_RANK", "0")))
+    os.environ["CUDA_VISIBLE_DEVICES"] = gpu
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(0)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", 0))
+    else:       # a one-rank group, so the same class runs
+        with socket.socket() as sock:
+            sock.bind(("127.0.0.1", 0))
+            port = sock.getsockname()[1]
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                                world_size=1)
+    from ac_fdtd_b200 import gaussian_pulse
+    from ac_fdtd_b200.slabs import DistributedSlabRoom
+
+    grid, objects, points = workload(args.size)
+    room = DistributedSlabRoom(grid, dtype=np.float32, device=0, **objects)
+    T = args.time_steps
+    room.add_volume_source(points[0], gaussian_pulse(T, room.dt, 4000.0))
+    for point in points[1:]:
+        room.add_pressure_receiver(point)
+
+    def one_run():
+        room.slab.solver.step_index = 0
+        room.run(T)
+
+    for _ in range(args.warmup):
+        one_run()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu) as clocks:
+        dist.barrier()
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            one_run()
+        end.record()
+        torch.cuda.synchronize()
+        dist.barrier()
+    elapsed = torch.tensor([start.elapsed_time(end)], dtype=torch.float64,
+                           device="cuda" if world > 1 else "cpu")
+    dist.all_reduce(elapsed, op=dist.ReduceOp.MAX)
+    elapsed_ms = float(elapsed.item())
+    room.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": grid.n_cells * T * args.steps / (elapsed_ms * 1e-3) / 1e9,
+            "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**config_dict(args, grid), "parallelism": f"x slabs x{world}",
+                       "exchange": "ghost p planes, one batched isend/irecv per rank and step"},
+            "clocks": clocks.summary(),
+        }), flush=True)
 
 
 def run_ours(args) -> None:
@@ -715,9 +786,14 @@ def main() -> None:
                              "or 'staged,rows,stages,planes,vector'")
     parser.add_argument("--adjoint-steps", type=int, default=3000)
     parser.add_argument("--inversion-steps", type=int, default=2500)
+    parser.add_argument("--slabs", action="store_true",
+                        help="cut the room into one x slab per rank (strong scaling) instead of "
+                             "running a replica per rank")
     args = parser.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.slabs:
+        run_slab_mode(args)
     else:
         run_ours(args)
 
