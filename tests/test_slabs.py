@@ -72,6 +72,21 @@ def test_every_owned_cell_gets_the_rooms_wall_pair_and_layer_profiles(parts):
             (block.vel_coef, block.pres_coef, block.src_coef, block.relax_scale, block.dt)
 
 
+def test_walls_given_per_patch_cut_cell_by_cell_too():
+    from ac_fdtd_b200.boundaries import WallPatches
+
+    grid = Grid(dx=0.05, nx=8, ny=6, nz=7)
+    patches = WallPatches(np.random.default_rng(3).uniform(0.0, 0.8, (6, 3, 3)))
+    block = room_coefficients(grid, AIR, 1.0, np.float32, patches)
+    for x0, x1 in slab_ranges(grid.nx, 3):
+        local, gx0 = slab_coefficients(block, x0, x1)
+        for i in range(x0, x1):
+            for j in range(grid.ny):
+                for k in range(grid.nz):
+                    assert _pair_used(local.wall_shell, local.shape, (i - gx0, j, k)) == \
+                        _pair_used(block.wall_shell, block.shape, (i, j, k))
+
+
 def test_rigid_rooms_and_rooms_without_layer_cut_too():
     block = room_coefficients(Grid(dx=0.05, nx=6, ny=3, nz=4), AIR, 1.0, np.float32)
     local, gx0 = slab_coefficients(block, 2, 4)
