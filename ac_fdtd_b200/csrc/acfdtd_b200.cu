@@ -3460,6 +3460,13 @@ int run_slabs(acf_solver *const *parts, int32_t n, const int32_t *own_lo, const 
             return fail(ACF_ERR_ARGUMENT, "part %d: own planes [%d, %d) do not fit %d planes with "
                         "ghosts", q, own_lo[q], own_hi[q], h.nx);
     }
+    bool one_device = true;
+    for (int q = 1; q < n; q++) one_device = one_device && parts[q]->device == parts[0]->device;
+    // A stream belongs to one device: parts on several GPUs run on each device's legacy default
+    // stream (ordered by events between devices), so a caller's stream could order nothing.
+    if (!one_device && stream != nullptr)
+        return fail(ACF_ERR_ARGUMENT, "parts on several GPUs: pass a null stream (each device's "
+                    "default stream is used)");
     if (n_steps == 0) return ACF_OK;
     for (int q = 0; q < n; q++) {
         DeviceGuard g(parts[q]->device);

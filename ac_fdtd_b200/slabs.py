@@ -298,6 +298,11 @@ class SlabGroup(_SlabSet):
     def energy(self) -> float:
         """The whole room's acoustic energy (``CudaAcousticFDTD.energy``), from every part's sums."""
         solver = self.slabs[0].solver
+        if self._several_devices:
+            # The last pressure sweep of a part stores into its neighbours' ghost planes from
+            # the neighbour's GPU; each part's sums read its ghost p plane on its own stream,
+            # which nothing orders after those peer stores. Finish every GPU's work first.
+            self.synchronize()
         terms = np.sum([s.energy_terms() for s in self.slabs], axis=0)
         return energy_from_terms(terms, solver.medium, float(solver.grid.dx), self.dt)
 

@@ -170,32 +170,53 @@ def cpu_baseline(size: int, budget_s: float = 12.0) -> dict:
     elapsed = time.perf_counter() - start
     value = grid.n_cells * steps / elapsed / 1e9
     return {"value": value, "unit": METRIC, "cores": int(cores), "kind": kind,
-            "host_cpus": os.cpu_count(),
+            "host_cpus": os.cpu_count(), "cpu_model": cpu_model(),
             "sample": f"{size}^3 fp32 same room, {steps} leapfrog steps after 4 warm-up steps, "
-                      f"{elapsed:.1f} s"}
+                      f"{elapsed:.1f} s",
+            "sample_leapfrog_steps": steps, "sample_ms": elapsed * 1e3}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    values = []
+    values, sample_ms, leapfrog_steps = [], [], []
     last = None
     for _ in range(args.warmup):
         cpu_baseline(args.size, budget_s=2.0)
     for _ in range(args.steps):
         last = cpu_baseline(args.size, budget_s=args.cpu_budget)
         values.append(last["value"])
+        sample_ms.append(last["sample_ms"])
+        leapfrog_steps.append(last["sample_leapfrog_steps"])
     from ac_fdtd_b200 import Grid
 
     grid = Grid(dx=343.2 / 40000.0, nx=args.size, ny=args.size, nz=args.size)
     value = float(statistics.median(values))
+    # One bench step of this arm is one bounded sample of the workload: `sample_leapfrog_steps`
+    # leapfrog steps of the 384^3 room, timed in full; ms_per_step is that sample's time, so
+    # steps x ms_per_step is the work that actually ran. The rate extrapolates to the full
+    # 4000-step run only through `value`.
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": grid.n_cells / (value * 1e9) * 1e3 * args.time_steps,
+        "ms_per_step": float(statistics.mean(sample_ms)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(args, grid),
+        "data": "synthetic",
+        "config": {**config_dict(args, grid),
+                   "bench_step": "one bounded sample of the room: sample_leapfrog_steps leapfrog "
+                                 "steps from a fresh solver (CPU time budget per sample)",
+                   "sample_leapfrog_steps": leapfrog_steps},
         "cpu_baseline": {**last, "value": value},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -401,23 +422,39 @@ def run_ours(args) -> None:
     p_out = pinned_array(grid.shape, np.float32)
     p0[...] = np.random.default_rng(rank).standard_normal(grid.shape).astype(np.float32) * 1e-3
 
-    def e2e_step():
+    phase_ms = {"h2d_ms": 0.0, "run_ms": 0.0, "d2h_ms": 0.0}
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def e2e_step(timed: bool):
+        # Each phase is bracketed by CUDA events on the solver's stream (the legacy default
+        # stream, torch's current one); set_state and get_state return after their copies.
         solver.step_index = 0
+        marks[0].record()
         h2d = solver.set_state(p=p0, velocity=v0, relaxation=psi0)
+        marks[1].record()
         solver.run(T)
+        marks[2].record()
         recorded = solver.recorded_pressure
         d2h = solver.get_state(p=p_out) + recorded.nbytes
+        marks[3].record()
+        if timed:
+            marks[3].synchronize()
+            for key, (a, b) in zip(phase_ms, ((0, 1), (1, 2), (2, 3))):
+                phase_ms[key] += marks[a].elapsed_time(marks[b])
         return h2d, d2h
 
     for _ in range(min(args.warmup, 1)):
-        e2e_step()
+        e2e_step(False)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        h2d, d2h = e2e_step()
+        h2d, d2h = e2e_step(True)
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = cell_updates / e2e_s / 1e9
+    phases = {k: v / args.steps for k, v in phase_ms.items()}
+    phases["h2d_GBps"] = h2d / (phases["h2d_ms"] * 1e-3) / 1e9 if phases["h2d_ms"] > 0 else None
+    phases["d2h_GBps"] = d2h / (phases["d2h_ms"] * 1e-3) / 1e9 if phases["d2h_ms"] > 0 else None
 
     batched = None if args.skip_extras else batched_vs_per_room(args)
     adjoint = None if args.skip_extras else adjoint_cost(args)
@@ -437,7 +474,8 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "path": f"CudaAcousticFDTD.set_state (pinned host) -> run({T}) -> "
-                        "recorded_pressure, get_state (pinned host)"},
+                        "recorded_pressure, get_state (pinned host)",
+                "phases_per_step": phases},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "batched": batched,
@@ -448,6 +486,8 @@ def run_ours(args) -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
+        if not args.skip_extras:
+            line["comparators"] = comparators(args)
     elif rank == 0:
         line["cpu_baseline"] = None
     solver.close()
@@ -455,7 +495,213 @@ def run_ours(args) -> None:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
+        line["extras_summary"] = extras_summary(line)     # last key: the end of the line
         print(json.dumps(line), flush=True)
+
+
+def extras_summary(line: dict) -> dict:
+    """The headline figures of the extra sections, compact, so that the end of the JSON line
+    (what a log tail keeps) carries them."""
+    def get(*path):
+        node = line
+        for key in path:
+            if not isinstance(node, dict) or key not in node:
+                return None
+            node = node[key]
+        return round(node, 4) if isinstance(node, float) else node
+
+    return {
+        "gcups": get("value"), "e2e_gcups": get("e2e", "value"), "frac": get("roofline", "frac"),
+        "e2e_h2d_ms": get("e2e", "phases_per_step", "h2d_ms"),
+        "e2e_run_ms": get("e2e", "phases_per_step", "run_ms"),
+        "e2e_d2h_ms": get("e2e", "phases_per_step", "d2h_ms"),
+        "cpu_ref_gcups": get("cpu_baseline", "value"),
+        "batched_speedup": get("batched", "speedup"),
+        "batched_ceiling": get("batched", "batching_ceiling_speedup"),
+        "small_rooms_speedup": get("batched", "small_rooms", "speedup"),
+        "grad_ratio_walls": get("adjoint", "walls_and_signal", "ratio"),
+        "grad_ratio_air": get("adjoint", "walls_signal_and_air", "ratio"),
+        "inversion_ratio": get("batched_inversion", "ratio"),
+        "fp32_rel_l2_384": get("precision", "room_384", "fp32_vs_fp64", "rel_l2"),
+        "fp64_gcups_384": get("precision", "room_384", "fp64_gcups"),
+        "torch_cuda_gcups_384": get("comparators", "gpu", "room_384_fp32", "gcups"),
+        "c_fp64_gcups_384": get("comparators", "cpu", "c_fp64_room_384", "gcups"),
+        "numpy_gcups_64": get("comparators", "cpu", "numpy_fp64_room_64", "gcups"),
+    }
+
+
+def reference_package():
+    """The unmodified reference package installed under ``baseline/_ref`` (git-ignored, made
+    by ``__graft_entry__.build()``), or None. Appended to the path, so only ``ac_fdtd`` itself
+    can resolve from there."""
+    path = ROOT / "baseline" / "_ref"
+    if not (path / "ac_fdtd" / "__init__.py").exists():
+        return None
+    if str(path) not in sys.path:
+        sys.path.append(str(path))
+    import ac_fdtd
+
+    return ac_fdtd
+
+
+def _as_reference(ref, grid, objects: dict):
+    """The reference's own value objects with the same parameters as ours."""
+    import dataclasses
+
+    rgrid = ref.Grid(dx=grid.dx, nx=grid.nx, ny=grid.ny, nz=grid.nz)
+    kinds = {"walls": ref.WallAdmittances, "absorbing_layer": ref.AbsorbingLayer,
+             "air_absorption": ref.AirAbsorption}
+    out = {}
+    for key, value in objects.items():
+        if value is not None:
+            out[key] = kinds[key](**{f.name: getattr(value, f.name)
+                                     for f in dataclasses.fields(value)})
+    return rgrid, out
+
+
+def comparators(args) -> dict:
+    """Comparators beside the C fp32 reference arm, each through the reference's own code path
+    (never this package's kernels):
+
+    * ``gpu``: the reference's whole-array Torch backend ``TorchAcousticFDTD(device="cuda")``
+      (ac-fdtd ``src/ac_fdtd/torch_backend.py:234-316``) on this GPU -- the 384^3 room in fp32
+      over a bounded sample after 3 warm-up steps, and the 64^3 plain room (walls 0.15, 2000
+      steps) in fp64 and fp32 in full -- beside this package on the same 64^3 runs;
+    * ``cpu``: the reference's C backend in fp64 on the 384^3 room (bounded sample), C fp64
+      and the NumPy reference in full on the 64^3 room, and the per-room C run over the 64
+      uneven rooms (a bounded number of steps per room), on this host's cores.
+    """
+    import torch
+
+    from ac_fdtd_b200 import AIR, CudaAcousticFDTD, gaussian_pulse
+    from ac_fdtd_b200.sources import gaussian_derivative_pulse
+    from ac_fdtd_b200.workloads import plain_room_small, uneven_rooms
+
+    ref = reference_package()
+    out = {"reference_package": "baseline/_ref/ac_fdtd (unmodified)" if ref else None}
+    grid1, objects1, source1, receivers1 = plain_room_small()
+    T1 = 2000
+
+    def small_signal(dt):      # d/dt of the 1 kHz Gaussian, as the 64^3 configuration has it
+        return gaussian_derivative_pulse(T1, dt, 1000.0)
+
+    gpu = {}
+    if ref is None:
+        gpu["unavailable"] = "the reference package is not installed under baseline/_ref"
+    else:
+        from ac_fdtd.torch_backend import TorchAcousticFDTD
+
+        grid, objects, points = workload(args.size)
+        rgrid, robjects = _as_reference(ref, grid, objects)
+        solver = TorchAcousticFDTD(rgrid, device="cuda", dtype=torch.float32, **robjects)
+        solver.add_volume_source(points[0], ref.gaussian_pulse(args.time_steps, solver.dt, 4000.0))
+        for point in points[1:]:
+            solver.add_pressure_receiver(point)
+        solver.run(3)
+        steps = 100
+        ms = _device_ms(lambda: solver.run(steps), torch)
+        gpu["room_384_fp32"] = {
+            "gcups": grid.n_cells * steps / (ms * 1e-3) / 1e9,
+            "sample": f"{steps} leapfrog steps of the {args.size}^3 room after 3 warm-up steps, "
+                      f"{ms:.0f} ms, CUDA events",
+        }
+        del solver
+        torch.cuda.empty_cache()
+        rgrid1, robjects1 = _as_reference(ref, grid1, objects1)
+        for dtype, tdtype in ((np.float64, torch.float64), (np.float32, torch.float32)):
+            name = np.dtype(dtype).name
+            solver = TorchAcousticFDTD(rgrid1, device="cuda", dtype=tdtype, **robjects1)
+            solver.add_volume_source(source1, small_signal(solver.dt))
+            for point in receivers1:
+                solver.add_pressure_receiver(point)
+            ms = _device_ms(lambda: solver.run(T1), torch)
+            torch_rec = solver.recorded_pressure
+            ours = CudaAcousticFDTD(grid1, dtype=dtype, **objects1)
+            from ac_fdtd_b200.autotune import apply_tuned
+
+            apply_tuned(ours)
+            ours.add_volume_source(source1, small_signal(ours.dt))
+            for point in receivers1:
+                ours.add_pressure_receiver(point)
+            ours.run(3)          # warm-up: graph capture
+            ours.reset_state()
+            ours.step_index = 0
+            ours_ms = _device_ms(lambda: ours.run(T1), torch)
+            ours_rec = ours.recorded_pressure
+            ours.close()
+            gpu[f"room_64_{name}"] = {
+                "reference_torch_gcups": grid1.n_cells * T1 / (ms * 1e-3) / 1e9,
+                "ours_gcups": grid1.n_cells * T1 / (ours_ms * 1e-3) / 1e9,
+                "speedup": ms / ours_ms,
+                "receiver_max_diff_over_peak": float(np.max(np.abs(ours_rec - torch_rec))
+                                                     / np.max(np.abs(torch_rec))),
+                "sample": f"{T1} steps in full, one run, CUDA events",
+            }
+            del solver
+    out["gpu"] = gpu
+
+    cpu = {"host_cpus": os.cpu_count(), "cpu_model": cpu_model()}
+    from oracle import ref_c
+
+    if ref_c.available():
+        grid, objects, points = workload(args.size)
+        solver = ref_c.RefCSolver(grid, AIR, dtype=np.float64, threads=0, **objects)
+        solver.add_volume_source(points[0], gaussian_pulse(args.time_steps, solver.dt, 4000.0))
+        for point in points[1:]:
+            solver.add_pressure_receiver(point)
+        solver.run(2)
+        steps = 60
+        t0 = time.perf_counter()
+        solver.run(steps)
+        elapsed = time.perf_counter() - t0
+        cpu["c_fp64_room_384"] = {"gcups": grid.n_cells * steps / elapsed / 1e9,
+                                  "threads": solver.threads,
+                                  "sample": f"{steps} leapfrog steps after 2, {elapsed:.1f} s"}
+        del solver
+        solver = ref_c.RefCSolver(grid1, AIR, dtype=np.float64, threads=0, **objects1)
+        solver.add_volume_source(source1, small_signal(solver.dt))
+        for point in receivers1:
+            solver.add_pressure_receiver(point)
+        t0 = time.perf_counter()
+        solver.run(T1)
+        elapsed = time.perf_counter() - t0
+        cpu["c_fp64_room_64"] = {"gcups": grid1.n_cells * T1 / elapsed / 1e9,
+                                 "threads": solver.threads,
+                                 "sample": f"{T1} steps in full, {elapsed:.1f} s"}
+        rooms = uneven_rooms()
+        per_room_steps = 10
+        cells = 0
+        elapsed = 0.0
+        threads = 0
+        for spec, source, receivers in rooms:
+            solver = ref_c.RefCSolver(spec["grid"], AIR, dtype=np.float32, threads=0,
+                                      walls=spec["walls"], air_absorption=spec["air_absorption"])
+            threads = solver.threads
+            solver.add_volume_source(source, gaussian_pulse(args.batch_steps, solver.dt, 2000.0))
+            for point in receivers:
+                solver.add_pressure_receiver(point)
+            t0 = time.perf_counter()
+            solver.run(per_room_steps)
+            elapsed += time.perf_counter() - t0
+            cells += spec["grid"].n_cells
+        cpu["c_fp32_uneven_rooms_per_room"] = {
+            "gcups": cells * per_room_steps / elapsed / 1e9, "threads": threads,
+            "sample": f"each of the 64 rooms for {per_room_steps} steps ({elapsed:.1f} s)"}
+    else:
+        cpu["c"] = "unavailable: oracle/_ref not built"
+    if ref is not None:
+        solver = ref.AcousticFDTD(ref.Grid(dx=grid1.dx, nx=grid1.nx, ny=grid1.ny, nz=grid1.nz),
+                                  walls=ref.WallAdmittances.from_absorption(0.15))
+        solver.add_volume_source(source1, small_signal(solver.dt))
+        for point in receivers1:
+            solver.add_pressure_receiver(point)
+        t0 = time.perf_counter()
+        solver.run(T1)
+        elapsed = time.perf_counter() - t0
+        cpu["numpy_fp64_room_64"] = {"gcups": grid1.n_cells * T1 / elapsed / 1e9, "threads": 1,
+                                     "sample": f"{T1} steps in full, {elapsed:.1f} s"}
+    out["cpu"] = cpu
+    return out
 
 
 def slab_overhead(args) -> dict:
@@ -592,18 +838,31 @@ def _device_ms(fn, torch) -> float:
 
 def batched_vs_per_room(args) -> dict:
     """64 uneven rooms (60-200 cells per axis, fp32, walls + ISO air): one RoomBatch against the
-    same rooms run one after another, each as its own CudaAcousticFDTD (CUDA graphs in both)."""
-    import torch
-
-    from ac_fdtd_b200 import CudaAcousticFDTD, RoomBatch, gaussian_pulse
+    same rooms run one after another, each as its own CudaAcousticFDTD (CUDA graphs in both).
+    The same comparison on 64 small rooms (24-64 cells per axis), where launch gaps dominate the
+    per-room arm, shows what batching buys when each room alone cannot fill the GPU."""
     from ac_fdtd_b200.workloads import uneven_rooms
 
     T = args.batch_steps
-    rooms = uneven_rooms()
-    specs = [r[0] for r in rooms]
-    cells = int(sum(spec["grid"].n_cells for spec in specs))
+    out = _batch_vs_rooms(uneven_rooms(), T, args)
+    out["workload"] = (f"64 rooms 3-10 m per axis at dx 5 cm ({out['cells']} cells, 60-200 per "
+                       f"axis), fp32, walls alpha~U(0.05,0.5), ISO air T~U(15,25) C RH~U(30,70) %, "
+                       f"1 source + 2 receivers per room, {T} steps (CUDA graphs in both arms)")
+    small = _batch_vs_rooms(uneven_rooms(seed=6, lengths=(1.2, 3.2)), T, args)
+    small["workload"] = (f"64 small rooms 1.2-3.2 m per axis at dx 5 cm ({small['cells']} cells, "
+                         f"24-64 per axis), otherwise as above, {T} steps")
+    out["small_rooms"] = small
+    return out
+
+
+def _batch_vs_rooms(rooms, T: int, args) -> dict:
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, RoomBatch, gaussian_pulse
     from ac_fdtd_b200.autotune import apply_tuned_batch
 
+    specs = [r[0] for r in rooms]
+    cells = int(sum(spec["grid"].n_cells for spec in specs))
     batch = RoomBatch(specs, dtype=np.float32)
     batch_geometry = apply_tuned_batch(batch)
     for r, (spec, source, receivers) in enumerate(rooms):
@@ -643,19 +902,28 @@ def batched_vs_per_room(args) -> dict:
         per_room[scheme] = min(_device_ms(run_rooms, torch) for _ in range(2))
         for solver in solvers:
             solver.close()
-    per_room_ms = min(per_room.values())
+    best_scheme = min(per_room, key=per_room.get)
+    per_room_ms = per_room[best_scheme]
     peak, peak_kind = measured_peak_hbm()
     batched_gcups = cells * T / (batch_ms * 1e-3) / 1e9
+    per_room_gcups = cells * T / (per_room_ms * 1e-3) / 1e9
+    batch_bytes = 56 if batch_geometry[0] == "fused" else 72
+    room_bytes = 56 if best_scheme == "fused" else 72
+    per_room_frac = per_room_gcups * room_bytes / peak
     return {
-        "workload": f"64 rooms 3-10 m per axis at dx 5 cm ({cells} cells, 60-200 per axis), fp32, "
-                    f"walls alpha~U(0.05,0.5), ISO air T~U(15,25) C RH~U(30,70) %, 1 source + 2 "
-                    f"receivers per room, {T} steps (CUDA graphs in both arms)",
+        "cells": cells,
         "batched_gcups": batched_gcups,
-        "per_room_gcups": cells * T / (per_room_ms * 1e-3) / 1e9,
+        "per_room_gcups": per_room_gcups,
         "per_room_gcups_by_scheme": {k: cells * T / (v * 1e-3) / 1e9 for k, v in per_room.items()},
         "speedup": per_room_ms / batch_ms,
-        f"batched_hbm_frac_of_{peak_kind}": batched_gcups * (56 if batch_geometry[0] == "fused" else 72) / peak,
-        "bytes_per_cell": 56 if batch_geometry[0] == "fused" else 72,
+        f"batched_hbm_frac_of_{peak_kind}": batched_gcups * batch_bytes / peak,
+        "bytes_per_cell": batch_bytes,
+        f"per_room_hbm_frac_of_{peak_kind}": per_room_frac,
+        "per_room_scheme": best_scheme,
+        "per_room_bytes_per_cell": room_bytes,
+        # a batch moves at most the peak, on the fused step's 56 bytes per cell at the least:
+        # against the per-room arm no batching can be faster than this
+        "batching_ceiling_speedup": (peak / 56) / per_room_gcups,
         "launches_in_setup_and_runs": launches,
         "batch_launch": {"scheme": batch_geometry[0], "block_threads": batch_geometry[1],
                          "planes": batch_geometry[2], "ctas_per_sm": batch_geometry[3],

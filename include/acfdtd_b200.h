@@ -269,7 +269,8 @@ int acf_solver_device(const acf_solver *solver);
  * GPUs; peer access is enabled as needed). The ghost planes must hold the neighbours' p before
  * the first step (acf_copy_plane). Two-sweep scheme, single rooms of equal precision, ny and
  * nz. Parts on one GPU run on `stream`; parts on several GPUs on each device's default stream,
- * ordered by events. Asynchronous. No counterpart in the reference. */
+ * ordered by events, and `stream` must then be null (ACF_ERR_ARGUMENT otherwise: a stream
+ * belongs to one device). Asynchronous. No counterpart in the reference. */
 int acf_run_slabs(acf_solver *const *parts, int32_t n_parts, const int32_t *own_lo,
                   const int32_t *own_hi, int64_t n_steps, int64_t step_offset, acf_stream stream);
 

@@ -33,9 +33,12 @@ def available() -> bool:
     return library_path(np.float64).exists() and library_path(np.float32).exists()
 
 
-def build(reference: str = "/root/reference") -> bool:
-    """Compile the reference C backend if its sources are present; True if the libs exist."""
-    if Path(reference, "src/ac_fdtd/c/acfdtd.c").exists():
+def build(reference: str | None = None) -> bool:
+    """Compile the reference C backend from the ac-fdtd checkout at ``reference`` (default: the
+    ``AC_FDTD_REFERENCE`` environment variable) if its sources are there; True if the libraries
+    exist afterwards. Without a checkout, only libraries built earlier count."""
+    reference = reference or os.environ.get("AC_FDTD_REFERENCE")
+    if reference and Path(reference, "src/ac_fdtd/c/acfdtd.c").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), f"REFERENCE={reference}"], check=True,
                        capture_output=True)
     return available()

@@ -2,7 +2,9 @@
 
 Run in the build container, where the reference is mounted (it is not on the GPU machines):
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py <path of the ac-fdtd checkout> [part ...]
+
+(or set AC_FDTD_REFERENCE to that path and pass only the parts).
 
 The reference is copied to a scratch directory first, because its C backend compiles its
 shared library next to its own source. Outputs (all committed, all small):
@@ -22,6 +24,7 @@ shared library next to its own source. Outputs (all committed, all small):
 from __future__ import annotations
 
 import hashlib
+import os
 import json
 import shutil
 import sys
@@ -355,7 +358,7 @@ def make_autograd(ref_pkg) -> tuple[dict, dict]:
     return data, meta
 
 
-def main(reference: str = "/root/reference", *parts: str) -> None:
+def main(reference: str, *parts: str) -> None:
     """Regenerate every fixture, or only the named parts (setup, trajectories, rooms, impulse,
     io); golden.json keeps the entries of the parts not regenerated."""
     scratch = Path(tempfile.mkdtemp(prefix="acfdtd_ref_"))
@@ -400,4 +403,11 @@ def main(reference: str = "/root/reference", *parts: str) -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    arguments = sys.argv[1:]
+    if arguments and Path(arguments[0], "src", "ac_fdtd").is_dir():
+        main(*arguments)
+    elif os.environ.get("AC_FDTD_REFERENCE"):
+        main(os.environ["AC_FDTD_REFERENCE"], *arguments)
+    else:
+        sys.exit("usage: make_golden.py <ac-fdtd checkout> [part ...] "
+                 "(or set AC_FDTD_REFERENCE)")

@@ -167,3 +167,50 @@ def test_the_slab_runner_refuses_parts_that_do_not_fit():
                                (ctypes.c_int32 * 2)(*good_hi), 1, 0, None)
     assert status == 4              # ACF_ERR_STATE: the runner steps two-sweep parts
     group.close()
+
+
+def _gpu_count() -> int:
+    import torch
+
+    return torch.cuda.device_count() if torch.cuda.is_available() else 0
+
+
+@pytest.mark.skipif(_gpu_count() < 2, reason="needs two GPUs: peer stores between devices")
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_slabs_on_two_gpus_equal_the_whole_room_bitwise(dtype):
+    """Parts alternate between GPUs 0 and 1: each pressure sweep stores its boundary planes into
+    the neighbour's ghost plane on the other GPU (plain peer stores, no multicast), and the
+    steps are ordered by events between the devices."""
+    steps = 50
+    whole = CudaAcousticFDTD(GRID, dtype=dtype, **CONFIG)
+    group = SlabGroup(GRID, dtype=dtype, parts=4, devices=[0, 1], **CONFIG)
+    assert {s.solver.device for s in group.slabs} == {0, 1}
+    initial = np.random.default_rng(7).standard_normal(GRID.shape).astype(dtype)
+    whole.p[:] = initial
+    start_from(group, initial)
+    populate(whole, steps)
+    populate(group, steps)
+    whole.run(steps)
+    group.run(17)
+    group.run(steps - 17)
+    assert_same(group, whole)
+    # right after a run: the parts' sums must see the neighbours' last peer stores
+    assert group.energy() == pytest.approx(whole.energy(), rel=1e-11, abs=0)
+    group.close()
+    whole.close()
+
+
+def test_the_slab_runner_refuses_a_stream_for_parts_on_several_gpus():
+    import ctypes
+
+    from ac_fdtd_b200 import _native
+
+    if _gpu_count() < 2:
+        pytest.skip("needs two GPUs")
+    group = SlabGroup(GRID, dtype=np.float32, parts=2, devices=[0, 1], **CONFIG)
+    lib = _native.library()
+    handles = (ctypes.c_void_p * 2)(*[s.solver._handle.value for s in group.slabs])
+    lo = (ctypes.c_int32 * 2)(*[s.first_owned for s in group.slabs])
+    hi = (ctypes.c_int32 * 2)(*[s.last_owned + 1 for s in group.slabs])
+    assert lib.acf_run_slabs(handles, 2, lo, hi, 1, 0, ctypes.c_void_p(1)) == 1
+    group.close()
