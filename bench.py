@@ -508,7 +508,7 @@ def extras_summary(line: dict) -> dict:
             if not isinstance(node, dict) or key not in node:
                 return None
             node = node[key]
-        return round(node, 4) if isinstance(node, float) else node
+        return float(f"{node:.5g}") if isinstance(node, float) else node
 
     return {
         "gcups": get("value"), "e2e_gcups": get("e2e", "value"), "frac": get("roofline", "frac"),
