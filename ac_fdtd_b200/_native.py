@@ -19,6 +19,10 @@ FIELD_P, FIELD_VX, FIELD_VY, FIELD_VZ, FIELD_PSI0 = 0, 1, 2, 3, 4
 _STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "bad state",
            5: "non-finite state"}
 
+#: Bits of a handle's device status word (acf_device_status).
+STATUS_WAIT_TIMEOUT, STATUS_NON_FINITE = 1, 2
+ERR_STATE, ERR_NUMERIC = 4, 5
+
 #: Every entry point declared in include/acfdtd_b200.h.
 EXPORTED_SYMBOLS = (
     "acf_abi_version", "acf_struct_size", "acf_last_error", "acf_device_count",
@@ -37,7 +41,9 @@ EXPORTED_SYMBOLS = (
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
     "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch", "acf_copy_plane",
-    "acf_solver_device", "acf_energy_terms_planes", "acf_run_slabs",
+    "acf_solver_device", "acf_energy_terms_planes", "acf_run_slabs", "acf_batch_device_status",
+    "acf_set_wait_test", "acf_schroeder_decay", "acf_decay_fit", "acf_clarity",
+    "acf_spectral_divide",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED = 0, 1, 2
@@ -134,6 +140,14 @@ _SIGNATURES = {
     "acf_adjoint_checkpoint_interval": (ctypes.c_int32, [_P]),
     "acf_set_device": (ctypes.c_int, [ctypes.c_int32]),
     "acf_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "acf_batch_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "acf_set_wait_test": (ctypes.c_int, [_P, _I64, ctypes.c_int32]),
+    "acf_schroeder_decay": (ctypes.c_int, [_P, _I64, _I64, ctypes.c_double, _P, _P]),
+    "acf_decay_fit": (ctypes.c_int, [_P, _I64, _I64, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, _P, _P, _P]),
+    "acf_clarity": (ctypes.c_int, [_P, _I64, _I64, _I64, _P, _P]),
+    "acf_spectral_divide": (ctypes.c_int, [_P, _P, _I64, _I64, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, _P, _P, _P]),
     "acf_batch_adjoint_prepare": (ctypes.c_int, [_P, _I64]),
     "acf_batch_adjoint_shell_size": (ctypes.c_int64, [_P, ctypes.c_int32]),
     "acf_batch_forward_record": (ctypes.c_int, [_P, _I64, _I64, _P]),

@@ -25,7 +25,7 @@ from . import _native
 from .coefficients import room_coefficients
 from .grid import cell_index
 from .medium import AIR
-from .solver import DEFAULT_STEPS_PER_GRAPH, _as_double_pointer
+from .solver import DEFAULT_STEPS_PER_GRAPH, _as_double_pointer, raise_for_status
 
 __all__ = ["RoomBatch"]
 
@@ -252,7 +252,13 @@ class RoomBatch:
                       "acf_batch_reset_state")
 
     def synchronize(self) -> None:
+        """Wait for the device, then raise if a sweep of any room produced a non-finite
+        pressure (``ACF_ERR_NUMERIC``); the batch's state is then not valid."""
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")
+        status = ctypes.c_int32(0)
+        _native.check(self._lib.acf_batch_device_status(self._handle, ctypes.byref(status)),
+                      "acf_batch_device_status")
+        raise_for_status(status.value)
 
     def set_launch(self, block_threads: int = 128, planes: int = 8, ctas_per_sm: int = 0) -> None:
         _native.check(self._lib.acf_batch_set_launch(self._handle, int(block_threads), int(planes),

@@ -123,6 +123,31 @@ __device__ __forceinline__ void prefetch_l2(const T *a) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
 
+// Bits of a handle's device status word.
+constexpr int32_t kStatusWaitTimeout = 1;   // a staged sweep gave up waiting for its copies
+constexpr int32_t kStatusNonFinite = 2;     // a sweep produced a NaN or infinite pressure
+
+__device__ __forceinline__ unsigned lane_id() {
+    unsigned lane;
+    asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+    return lane;
+}
+
+// Non-finite detector: acc = fma(x, 0, acc) is acc + 0 for every finite x (one rounding, exact)
+// and NaN once any x was NaN or infinite; NaN then stays. One fused instruction per value.
+template <typename T>
+__device__ __forceinline__ T finite_acc(T acc, T x) {
+    if constexpr (sizeof(T) == 4) return __fmaf_rn(x, 0.0f, acc);
+    else return __fma_rn(x, 0.0, acc);
+}
+
+// Raise kStatusNonFinite once per warp whose threads saw a non-finite value.
+__device__ __forceinline__ void report_nonfinite(int32_t *status, bool bad) {
+    const unsigned mask = __ballot_sync(__activemask(), bad);
+    if (bad && status != nullptr && lane_id() == (unsigned)(__ffs(mask) - 1))
+        atomicOr(status, kStatusNonFinite);
+}
+
 // ------------------------------------------------------------------------------------------
 // What the sweeps read about one room. Plain data, identical on host and device.
 
@@ -156,6 +181,9 @@ struct Room {
     const int64_t *rec_col;
     T *rec;
     int64_t rec_stride, rec_origin;
+    // Status word of the handle (device memory): the sweeps that write p set kStatusNonFinite
+    // in it when a pressure they produced is NaN or infinite. Null: not checked.
+    int32_t *status;
 };
 
 // Forward history kept for the adjoint: per step, p^n and p-tilde^n -- pressure before the step
@@ -472,6 +500,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
     const int64_t column = (int64_t)j * s.pz + k0;
     T XL[kVec];  // vx on the lower x face of the current plane
     Vec4<T>::ldg(s.vx + (int64_t)i_begin * s.plane + column, XL);
+    T bad = T(0);   // NaN once a pressure this column produced is not finite
 
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
@@ -550,6 +579,8 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
 
         if (REC && hist->shell && boundary) record_shell(s, *hist, i, j, k0, step, P, PT);
         if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) bad = finite_acc(bad, Pn[e]);
 
         // ---- stores
         Vec4<T>::store(s.p + base, Pn);
@@ -562,6 +593,7 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
 #pragma unroll
         for (int e = 0; e < kVec; e++) XL[e] = XH[e];
     }
+    report_nonfinite(s.status, bad != bad);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -615,6 +647,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
 
     // Carried from plane to plane: p(i) and the updated vx on face i.
     T P[kVec], XL[kVec];
+    T bad = T(0);   // NaN once a pressure this column produced is not finite
     {
         const int64_t base = (int64_t)i_begin * s.plane + column;
         Vec4<T>::ldg(s.p + base, P);
@@ -725,6 +758,8 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
             Pn[e] = pe;
         }
         if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) bad = finite_acc(bad, Pn[e]);
 
         // ---- stores: p, the three lower faces, the far boundary faces, psi in place. A z
         // element k == nz inside this chunk is the top face, already updated in ZL (no
@@ -748,6 +783,7 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
             P[e] = PX[e];
         }
     }
+    report_nonfinite(s.status, bad != bad);
 }
 
 // Resident blocks of 256 threads the compiler must fit (register budget 65536 / (256 x this)).
@@ -806,8 +842,14 @@ struct StagedParams {
     int32_t block_x;                // compute threads per row (a multiple of 32)
     int64_t stage_elems;            // elements of one ring buffer
     int64_t off_vx, off_vy, off_vz, off_psi;
-    int32_t *error;                 // set to 1 when a wait ran out
+    int32_t *error;                 // kStatusWaitTimeout is raised here when a wait ran out
     float2 pairs[16];               // single precision: coefficients duplicated into both lanes
+    // Test hooks, neutral by default: the time limit of every wait, and one x plane whose copies
+    // the producer of the grid's first CTA leaves out (-1: none), so that its consumers' waits
+    // run out and the kernel returns with kStatusWaitTimeout raised instead of hanging.
+    uint64_t wait_limit_ns;
+    int32_t skip_plane;
+    int32_t reserved;
 };
 
 // Slots of StagedParams::pairs; the Neg slots hold the negated coefficient.
@@ -870,14 +912,14 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait: false when the phase completed neither within kWaitLimitNs nor within
-// kWaitLimitIterations tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Bounded wait: false when the phase completed neither within `limit_ns` (kWaitLimitNs unless
+// a test shortened it) nor within kWaitLimitIterations tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t start = global_ns();
     for (int it = 0; it < kWaitLimitIterations; it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - start > kWaitLimitNs) return false;
+        if (global_ns() - start > limit_ns) return false;
     }
     return false;
 }
@@ -991,7 +1033,9 @@ fused_staged_sweep(const StagedParams<T> g) {
 
     // Plane i into buffer `slot`. Plane i_end (<= nx, inside every field's nx + 1 planes) is
     // only read for p and vx, and its relaxation states belong to the next CTA along x.
+    const bool skipping = g.skip_plane >= 0 && blockIdx.x == 0 && blockIdx.y == 0;
     auto issue = [&](int i, int slot) {
+        if (skipping && i == g.skip_plane) return;   // test hook: this plane never arrives
         T *dst = ring + (int64_t)slot * g.stage_elems;
         const int64_t plane = (int64_t)i * s.plane;
         const int64_t own = plane + (int64_t)j0 * s.pz;
@@ -1108,7 +1152,7 @@ fused_staged_sweep(const StagedParams<T> g) {
             bool ok = true;
             for (int q = i_begin + S; q <= i_end; q++) {
                 const int u = q - i_begin;
-                if (!mbar_wait(empty + u % S, (uint32_t)(u / S - 1) & 1u)) {
+                if (!mbar_wait(empty + u % S, (uint32_t)(u / S - 1) & 1u, g.wait_limit_ns)) {
                     ok = false;
                     break;
                 }
@@ -1116,17 +1160,18 @@ fused_staged_sweep(const StagedParams<T> g) {
                 issued = q;
             }
             if (!ok) {
-                atomicExch(g.error, 1);
+                atomicOr(g.error, kStatusWaitTimeout);
                 // The latest plane issued into each buffer must land before the CTA exits.
                 for (int q = max(i_begin, issued - S + 1); q <= issued; q++) {
                     const int u = q - i_begin;
-                    mbar_wait(full + u % S, (uint32_t)(u / S) & 1u);
+                    mbar_wait(full + u % S, (uint32_t)(u / S) & 1u, g.wait_limit_ns);
                 }
             }
         }
         return;
     }
 
+    T bad = T(0);   // NaN once a pressure this thread produced is not finite
     // x damping profiles of the current plane, loaded one plane ahead.
     T fi_cell_next = T(1), fi1_face_next = T(1);
     if (LAYER && active) {
@@ -1137,10 +1182,10 @@ fused_staged_sweep(const StagedParams<T> g) {
         const int u = i - i_begin;
         const int slot = u % S, nslot = (u + 1) % S;
         // Buffer `slot` (plane i) was already waited for as the next plane, except at the start.
-        bool ready = u > 0 || mbar_wait(full + slot, 0u);
-        ready = ready && mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u);
+        bool ready = u > 0 || mbar_wait(full + slot, 0u, g.wait_limit_ns);
+        ready = ready && mbar_wait(full + nslot, (uint32_t)((u + 1) / S) & 1u, g.wait_limit_ns);
         if (!ready) {
-            atomicExch(g.error, 1);
+            atomicOr(g.error, kStatusWaitTimeout);
             return;
         }
         const T fi_cell_here = fi_cell_next, fi1_face_here = fi1_face_next;
@@ -1236,6 +1281,7 @@ fused_staged_sweep(const StagedParams<T> g) {
                     }
                     if (NR > 0) pe = sub2(pe, mul2(d, g.pairs[kPairNegRelaxScale]));   // pe + d * scale
                     pe = sub2(pe, mul2(d, g.pairs[kPairCp]));
+                    bad = finite_acc(finite_acc(bad, pe.x), pe.y);
                     if (WALLS && wall_cell) {
                         float fu, fp;
                         if (k0 + a < s.nz && wall_pair(s, i, j, k0 + a, fu, fp)) pe.x = pe.x * fu - P[a] * fp;
@@ -1304,6 +1350,7 @@ fused_staged_sweep(const StagedParams<T> g) {
                         }
                     }
                     Pn[e] = pe;
+                    bad = finite_acc(bad, pe);
                 }
 
             }
@@ -1372,6 +1419,262 @@ fused_staged_sweep(const StagedParams<T> g) {
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + slot);
     }
+    report_nonfinite(s.status, bad != bad);
+}
+
+// ------------------------------------------------------------------------------------------
+// The fused step in single precision, lean in instructions (rooms with nz a multiple of 4).
+//
+// Bound by HBM only while its warps issue fast enough: fused_column spends about 190
+// thread-instructions per cell, so under the power cap's lower SM clock the step slowed with the
+// clock. This column performs the same operations with a third of the instructions:
+//   * the two-lane f32x2 arithmetic of the staged sweep (same rounding, lane for lane);
+//   * damping only by factors that are not exactly 1: a product by 1.0 is the identity, so a
+//     thread skips the multiplications of an axis whose profile is 1 at its row, chunk or plane
+//     (the middle of a room with a sponge on its x faces damps nothing) and the products it does
+//     form keep the x, y, z order -- results are unchanged bit for bit;
+//   * z profiles of the chunk held in registers, x profiles loaded once per plane;
+//   * with nz a multiple of 4 no chunk holds padding, so the only per-element edge is the k = 0
+//     face of the first chunk; every other test is uniform over a plane or a row.
+
+struct LeanParams {
+    FusedParams<float> f;
+    float2 pairs[16];      // the slots of StagedParams::pairs
+};
+
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+template <bool LAYER, bool WALLS, int NR>
+__device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, int i_end, int j, int c,
+                                            int64_t step) {
+    const FusedParams<float> &f = g.f;
+    const Room<float> &s = f.room;
+    const int k0 = c * kVec;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
+    const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    bool all_points = false;
+    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const bool wall_column = !y_lo || !y_hi || !z_lo || !z_hi;
+    const float2 cv2 = g.pairs[kPairCv], cp2 = g.pairs[kPairCp];
+    const float cv = cv2.x;
+
+    float fj_cell = 1.f, fj_face = 1.f, fj1_face = 1.f, fkf4 = 1.f;
+    float2 fkc01 = dup2(1.f), fkc23 = dup2(1.f), fkf01 = dup2(1.f), fkf23 = dup2(1.f);
+    bool damp_y = false, damp_z = false;
+    if (LAYER) {
+        fj_cell = __ldg(s.cell[1] + j);
+        fj_face = __ldg(s.face[1] + j);
+        fj1_face = __ldg(s.face[1] + j + 1);
+        fkc01 = make_float2(__ldg(s.cell[2] + k0), __ldg(s.cell[2] + k0 + 1));
+        fkc23 = make_float2(__ldg(s.cell[2] + k0 + 2), __ldg(s.cell[2] + k0 + 3));
+        fkf01 = make_float2(__ldg(s.face[2] + k0), __ldg(s.face[2] + k0 + 1));
+        fkf23 = make_float2(__ldg(s.face[2] + k0 + 2), __ldg(s.face[2] + k0 + 3));
+        fkf4 = __ldg(s.face[2] + k0 + 4);
+        damp_y = fj_cell != 1.f || fj_face != 1.f || fj1_face != 1.f;
+        damp_z = fkc01.x != 1.f || fkc01.y != 1.f || fkc23.x != 1.f || fkc23.y != 1.f ||
+                 fkf01.x != 1.f || fkf01.y != 1.f || fkf23.x != 1.f || fkf23.y != 1.f || fkf4 != 1.f;
+    }
+
+    // Carried from plane to plane: p(i) and the updated vx on face i.
+    float4 P;
+    float2 XL01, XL23;
+    float2 bad2 = dup2(0.f);   // NaN once a pressure this column produced is not finite
+    {
+        const int64_t base = (int64_t)i_begin * s.plane + column;
+        P = __ldg(reinterpret_cast<const float4 *>(s.p + base));
+        const float4 V = __ldg(reinterpret_cast<const float4 *>(s.vx + base));
+        XL01 = lo2(V);
+        XL23 = hi2(V);
+        if (i_begin > 0) {
+            const float4 Q = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.plane));
+            XL01 = sub2(XL01, mul2(cv2, sub2(lo2(P), lo2(Q))));
+            XL23 = sub2(XL23, mul2(cv2, sub2(hi2(P), hi2(Q))));
+        }
+        if (LAYER) {
+            const float fi_face = __ldg(s.face[0] + i_begin);
+            if (fi_face != 1.f) {
+                XL01 = mul2(XL01, dup2(fi_face));
+                XL23 = mul2(XL23, dup2(fi_face));
+            }
+            if (damp_y) {
+                XL01 = mul2(XL01, dup2(fj_cell));
+                XL23 = mul2(XL23, dup2(fj_cell));
+            }
+            if (damp_z) {
+                XL01 = mul2(XL01, fkc01);
+                XL23 = mul2(XL23, fkc23);
+            }
+        }
+    }
+
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        const bool x_inner = i + 1 < s.nx;
+        if (s.prefetch && i + 1 < i_end) {   // the next plane's own-row inputs into L2
+            const int64_t next = base + s.plane;
+            if (i + 2 < s.nx) prefetch_l2(s.p + next + s.plane);
+            prefetch_l2(s.vx + next + s.plane);
+            prefetch_l2(s.vy + next);
+            prefetch_l2(s.vz + next);
+#pragma unroll
+            for (int r = 0; r < NR; r++) prefetch_l2(s.psi + r * s.field + next);
+        }
+        // ---- loads (all read-only: the next state goes to the other buffer)
+        float4 PX = P, PYm = P, PYp = P;
+        if (x_inner) PX = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.plane));
+        const float4 VXo = __ldg(reinterpret_cast<const float4 *>(s.vx + base + s.plane));
+        if (y_lo) PYm = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.pz));
+        if (y_hi) PYp = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.pz));
+        const float4 VY = __ldg(reinterpret_cast<const float4 *>(s.vy + base));
+        const float4 VYp = __ldg(reinterpret_cast<const float4 *>(s.vy + base + s.pz));
+        const float4 VZ = __ldg(reinterpret_cast<const float4 *>(s.vz + base));
+        const float p_below = z_lo ? __ldg(s.p + base - 1) : 0.f;
+        const float p_above = z_hi ? __ldg(s.p + base + kVec) : 0.f;
+        const float vz_above = __ldg(s.vz + base + kVec);   // face k0 + 4 <= nz: inside the row
+        float4 S[NR > 0 ? NR : 1];
+#pragma unroll
+        for (int r = 0; r < NR; r++) S[r] = *reinterpret_cast<const float4 *>(s.psi + r * s.field + base);
+        float fi_cell = 1.f, fi1_face = 1.f;
+        if (LAYER) {
+            fi_cell = __ldg(s.cell[0] + i);
+            fi1_face = __ldg(s.face[0] + i + 1);
+        }
+
+        // ---- updated faces: x upper (carried on), y lower and upper, z lower and upper
+        const float2 P01 = lo2(P), P23 = hi2(P);
+        float2 XH01 = lo2(VXo), XH23 = hi2(VXo);
+        if (x_inner) {
+            XH01 = sub2(XH01, mul2(cv2, sub2(lo2(PX), P01)));
+            XH23 = sub2(XH23, mul2(cv2, sub2(hi2(PX), P23)));
+        }
+        float2 YL01 = lo2(VY), YL23 = hi2(VY);
+        if (y_lo) {
+            YL01 = sub2(YL01, mul2(cv2, sub2(P01, lo2(PYm))));
+            YL23 = sub2(YL23, mul2(cv2, sub2(P23, hi2(PYm))));
+        }
+        float2 YH01 = lo2(VYp), YH23 = hi2(VYp);
+        if (y_hi) {
+            YH01 = sub2(YH01, mul2(cv2, sub2(lo2(PYp), P01)));
+            YH23 = sub2(YH23, mul2(cv2, sub2(hi2(PYp), P23)));
+        }
+        float2 ZL01 = sub2(lo2(VZ), mul2(cv2, sub2(P01, make_float2(p_below, P.x))));
+        float2 ZL23 = sub2(hi2(VZ), mul2(cv2, sub2(P23, make_float2(P.y, P.z))));
+        if (!z_lo) ZL01.x = VZ.x;                 // face k = 0: a boundary, never updated
+        float ZH3 = vz_above;
+        if (z_hi) ZH3 = ZH3 - cv * (p_above - P.w);
+        if (LAYER) {   // x, y, z order; an axis whose factors here are all 1 is skipped
+            if (fi_cell != 1.f || fi1_face != 1.f) {
+                const float2 a = dup2(fi1_face), b = dup2(fi_cell);
+                XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
+                YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
+                YH01 = mul2(YH01, b); YH23 = mul2(YH23, b);
+                ZL01 = mul2(ZL01, b); ZL23 = mul2(ZL23, b);
+                ZH3 = ZH3 * fi_cell;
+            }
+            if (damp_y) {
+                const float2 a = dup2(fj_cell), b = dup2(fj_face), e = dup2(fj1_face);
+                XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
+                YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
+                YH01 = mul2(YH01, e); YH23 = mul2(YH23, e);
+                ZL01 = mul2(ZL01, a); ZL23 = mul2(ZL23, a);
+                ZH3 = ZH3 * fj_cell;
+            }
+            if (damp_z) {
+                XH01 = mul2(XH01, fkc01); XH23 = mul2(XH23, fkc23);
+                YL01 = mul2(YL01, fkc01); YL23 = mul2(YL23, fkc23);
+                YH01 = mul2(YH01, fkc01); YH23 = mul2(YH23, fkc23);
+                ZL01 = mul2(ZL01, fkf01); ZL23 = mul2(ZL23, fkf23);
+                ZH3 = ZH3 * fkf4;
+            }
+        }
+
+        // ---- pressure, as the pressure sweep computes it
+        float2 d01 = sub2(XH01, XL01), d23 = sub2(XH23, XL23);
+        d01 = add2(d01, sub2(YH01, YL01));
+        d23 = add2(d23, sub2(YH23, YL23));
+        d01 = add2(d01, sub2(make_float2(ZL01.y, ZL23.x), ZL01));
+        d23 = add2(d23, sub2(make_float2(ZL23.y, ZH3), ZL23));
+        float2 pe01 = P01, pe23 = P23;
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            const float2 t01 = mul2(d01, g.pairs[kPairGain + r]), t23 = mul2(d23, g.pairs[kPairGain + r]);
+            const float2 o01 = sub2(lo2(S[r]), t01), o23 = sub2(hi2(S[r]), t23);
+            // offset * decay + target, and pe + offset * mean, as minus the negated products
+            const float2 n01 = sub2(t01, mul2(o01, g.pairs[kPairNegDecay + r]));
+            const float2 n23 = sub2(t23, mul2(o23, g.pairs[kPairNegDecay + r]));
+            pe01 = sub2(pe01, mul2(o01, g.pairs[kPairNegMean + r]));
+            pe23 = sub2(pe23, mul2(o23, g.pairs[kPairNegMean + r]));
+            S[r] = make_float4(n01.x, n01.y, n23.x, n23.y);
+        }
+        if (NR > 0) {
+            pe01 = sub2(pe01, mul2(d01, g.pairs[kPairNegRelaxScale]));
+            pe23 = sub2(pe23, mul2(d23, g.pairs[kPairNegRelaxScale]));
+        }
+        pe01 = sub2(pe01, mul2(d01, cp2));
+        pe23 = sub2(pe23, mul2(d23, cp2));
+        // Any non-finite p, v or psi reaches pe here; walls, damping and sources are finite.
+        bad2 = __ffma2_rn(pe01, dup2(0.f), bad2);
+        bad2 = __ffma2_rn(pe23, dup2(0.f), bad2);
+        float Pn[kVec] = {pe01.x, pe01.y, pe23.x, pe23.y};
+        if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
+            const float Po[kVec] = {P.x, P.y, P.z, P.w};
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                float fu, fp;
+                if (wall_pair(s, i, j, k0 + e, fu, fp)) Pn[e] = Pn[e] * fu - Po[e] * fp;
+            }
+        }
+        if (LAYER) {
+            if (fi_cell != 1.f) {
+#pragma unroll
+                for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * fi_cell;
+            }
+            if (damp_y) {
+#pragma unroll
+                for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * fj_cell;
+            }
+            if (damp_z) {
+                Pn[0] = Pn[0] * fkc01.x;
+                Pn[1] = Pn[1] * fkc01.y;
+                Pn[2] = Pn[2] * fkc23.x;
+                Pn[3] = Pn[3] * fkc23.y;
+            }
+        }
+        if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
+
+        // ---- stores: p, the three lower faces, the far boundary faces, psi in place
+        *reinterpret_cast<float4 *>(f.np + base) = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
+        *reinterpret_cast<float4 *>(f.nvx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
+        *reinterpret_cast<float4 *>(f.nvy + base) = make_float4(YL01.x, YL01.y, YL23.x, YL23.y);
+        *reinterpret_cast<float4 *>(f.nvz + base) = make_float4(ZL01.x, ZL01.y, ZL23.x, ZL23.y);
+        if (!x_inner)
+            *reinterpret_cast<float4 *>(f.nvx + base + s.plane) = make_float4(XH01.x, XH01.y, XH23.x, XH23.y);
+        if (!y_hi)
+            *reinterpret_cast<float4 *>(f.nvy + base + s.pz) = make_float4(YH01.x, YH01.y, YH23.x, YH23.y);
+        if (!z_hi) f.nvz[base + kVec] = ZH3;
+#pragma unroll
+        for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(s.psi + r * s.field + base) = S[r];
+        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
+        XL01 = XH01;
+        XL23 = XH23;
+        P = PX;
+    }
+    report_nonfinite(s.status, bad2.x != bad2.x || bad2.y != bad2.y);
+}
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(float, LAYER, NR)) lean_sweep(const LeanParams g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= g.f.room.nchunks || j >= g.f.room.ny) return;
+    const bool any_point = (g.f.room.n_src | g.f.room.n_rec) != 0;
+    const int64_t step = any_point ? (*g.f.step_base + g.f.local_step) : 0;
+    const int i_begin = blockIdx.z * g.f.planes;
+    lean_column<LAYER, WALLS, NR>(g, i_begin, min(g.f.room.nx, i_begin + g.f.planes), j, c, step);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -2394,6 +2697,15 @@ struct acf_batch {
 
     int64_t launches = 0;
 
+    // The device status word (kStatus* bits), copied to pinned host memory after every run so
+    // that the next run can report a non-finite state without waiting for the device.
+    int32_t *status_host = nullptr;
+    cudaEvent_t status_event = nullptr;
+    bool status_pending = false;
+    // Test hooks of the staged sweep (acf_set_wait_test): 0 / -1 leave it as built.
+    uint64_t test_wait_limit_ns = 0;
+    int32_t test_skip_plane = -1;
+
     // CUDA graphs of the adjoint path: forward record, recompute, adjoint steps
     struct Graph {
         cudaGraphExec_t exec = nullptr;
@@ -2483,6 +2795,7 @@ template <typename T>
 Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     const RoomHost &h = b->rooms[r];
     Room<T> s{};
+    s.status = b->error_flag();
     s.nx = h.nx;
     s.ny = h.ny;
     s.nz = h.nz;
@@ -2659,6 +2972,28 @@ struct FusedStep {
 };
 
 template <typename T, bool L, bool W, int NR>
+struct LeanStep {
+    static void launch(const LeanParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_sweep<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+// The packed coefficients of the single-precision kernels: each rounded to float once, the
+// negated slots negated after that rounding, so each is exactly minus the scalar's value.
+void fill_pairs(float2 *pairs, const RoomHost &h) {
+    auto put = [&](int slot, double v) { pairs[slot] = make_float2((float)v, (float)v); };
+    auto put_neg = [&](int slot, double v) { pairs[slot] = make_float2(-(float)v, -(float)v); };
+    put(kPairCv, h.coef[0]);
+    put(kPairCp, h.coef[1]);
+    put_neg(kPairNegRelaxScale, h.coef[3]);
+    for (int r = 0; r < h.n_relax; r++) {
+        put(kPairGain + r, h.gain[r]);
+        put_neg(kPairNegDecay + r, h.decay[r]);
+        put_neg(kPairNegMean + r, h.mean[r]);
+    }
+}
+
+template <typename T, bool L, bool W, int NR>
 struct BatchFused {
     static void launch(const FusedBatchParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
         fused_batch<T, L, W, NR><<<g, b, 0, st>>>(p);
@@ -2770,28 +3105,28 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
             g.off_vz = lay.off_vz;
             g.off_psi = lay.off_psi;
             g.error = b->error_flag();
-            if (sizeof(T) == 4) {
-                auto put = [&](int slot, double v) { g.pairs[slot] = make_float2((float)v, (float)v); };
-                put(kPairCv, h.coef[0]);
-                put(kPairCp, h.coef[1]);
-                // negated after the rounding to float, so each is exactly minus the scalar's value
-                auto put_neg = [&](int slot, double v) {
-                    g.pairs[slot] = make_float2(-(float)v, -(float)v);
-                };
-                put_neg(kPairNegRelaxScale, h.coef[3]);
-                for (int r = 0; r < h.n_relax; r++) {
-                    put(kPairGain + r, h.gain[r]);
-                    put_neg(kPairNegDecay + r, h.decay[r]);
-                    put_neg(kPairNegMean + r, h.mean[r]);
-                }
-            }
+            g.wait_limit_ns = b->test_wait_limit_ns ? b->test_wait_limit_ns : kWaitLimitNs;
+            g.skip_plane = b->test_skip_plane;
+            if (sizeof(T) == 4) fill_pairs(g.pairs, h);
             g.block_x = staged_block_x(h, b->staged_vector);
             const dim3 block(g.block_x * b->staged_rows + 32);
             const dim3 grid((h.ny + b->staged_rows - 1) / b->staged_rows, (h.nx + b->planes - 1) / b->planes);
             dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
         } else {
             const LaunchShape L = single_shape(b);
-            dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
+            bool lean = false;
+            if constexpr (sizeof(T) == 4) {
+                if (h.nz % kVec == 0) {   // the lean single-precision column (no padding lanes)
+                    LeanParams g{};
+                    g.f = f;
+                    fill_pairs(g.pairs, h);
+                    dispatch_pressure<float, LeanStep>(h.has_layer, h.has_walls, h.n_relax, g, L.grid,
+                                                       L.block, st);
+                    lean = true;
+                }
+            }
+            if (!lean)
+                dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
         }
         h.cur ^= 1;
         if (events) {
@@ -3007,6 +3342,8 @@ void free_batch(acf_batch *b) {
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     for (auto &e : b->ring)
         if (e) cudaEventDestroy(e);
+    if (b->status_event) cudaEventDestroy(b->status_event);
+    if (b->status_host) cudaFreeHost(b->status_host);
     for (auto &r : b->rooms) free_room(r);
     cudaFree(b->adj.hist_shell);
     cudaFree(b->adj.checkpoints);
@@ -3109,6 +3446,11 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
         offset += (size_t)round_up(((int64_t)b->n_fields() * h.field + h.pz) * (int64_t)es, 256);
     }
     b->state_bytes = offset;
+    // Test hook: ACF_INJECT_ALLOC_FAILURE set (non-empty, not "0") makes this allocation fail
+    // as an exhausted device would, before any device memory is taken.
+    if (const char *inject = getenv("ACF_INJECT_ALLOC_FAILURE"); inject && *inject && strcmp(inject, "0") != 0)
+        return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of state failed (injected by "
+                    "ACF_INJECT_ALLOC_FAILURE)", b->state_bytes);
     if (cudaMalloc(&b->state, b->state_bytes) != cudaSuccess)
         return fail(ACF_ERR_MEMORY, "cudaMalloc of %zu bytes of state failed", b->state_bytes);
     ACF_CUDA(cudaMemset(b->state, 0, b->state_bytes));
@@ -3159,6 +3501,10 @@ int create_batch(int32_t n_rooms, const acf_config *configs, acf_batch *b) {
     if (cudaMalloc(&b->step_base, 2 * sizeof(int64_t)) != cudaSuccess)
         return fail(ACF_ERR_MEMORY, "cudaMalloc of step counter failed");
     ACF_CUDA(cudaMemset(b->step_base, 0, 2 * sizeof(int64_t)));
+    if (cudaHostAlloc((void **)&b->status_host, sizeof(int32_t), cudaHostAllocDefault) != cudaSuccess)
+        return fail(ACF_ERR_MEMORY, "pinned status word allocation failed");
+    *b->status_host = 0;
+    ACF_CUDA(cudaEventCreateWithFlags(&b->status_event, cudaEventDisableTiming));
     cudaDeviceGetAttribute(&b->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, b->device);
     cudaDeviceGetAttribute(&b->smem_per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
     b->energy_blocks = 4 * b->sms;
@@ -3299,7 +3645,7 @@ int read_recording(acf_batch *b, int room, int64_t r, int64_t first_step, int64_
     cudaStream_t st = (cudaStream_t)stream;
     const size_t es = b->elem();
     ACF_CUDA(cudaMemcpyAsync(dst, (char *)h.rec + ((size_t)r * h.rec_capacity + col) * es, (size_t)n * es,
-                             cudaMemcpyDeviceToHost, st));
+                             cudaMemcpyDefault, st));
     ACF_CUDA(cudaStreamSynchronize(st));
     return ACF_OK;
 }
@@ -3328,16 +3674,49 @@ int ensure_recording(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStr
     return ACF_OK;
 }
 
+// The status copied after the previous run, if it has landed: ACF_ERR_NUMERIC when a sweep saw a
+// non-finite pressure, ACF_ERR_STATE when a staged sweep's wait ran out (the state is then not
+// valid either way). Never waits for the device.
+int pending_status(acf_batch *b) {
+    if (!b->status_pending) return ACF_OK;
+    const cudaError_t q = cudaEventQuery(b->status_event);
+    if (q == cudaErrorNotReady) return ACF_OK;
+    if (q != cudaSuccess) return fail(ACF_ERR_CUDA, "status event: %s", cudaGetErrorString(q));
+    b->status_pending = false;
+    const int32_t word = *b->status_host;
+    if (word & kStatusNonFinite)
+        return fail(ACF_ERR_NUMERIC, "a sweep produced a non-finite pressure (NaN or infinity) in "
+                    "an earlier run; the state is not valid");
+    if (word & kStatusWaitTimeout)
+        return fail(ACF_ERR_STATE, "a staged sweep gave up waiting for its bulk copies in an "
+                    "earlier run; the state is not valid");
+    return ACF_OK;
+}
+
 int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream stream) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null handle");
     if (n_steps < 0 || step_offset < 0) return fail(ACF_ERR_ARGUMENT, "negative step count or offset");
     if (n_steps == 0) return ACF_OK;
     DeviceGuard guard(b->device);
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = ensure_recording(b, n_steps, step_offset, st);
+    int rc = pending_status(b);
     if (rc) return rc;
-    return b->precision == 8 ? run_impl<double>(b, n_steps, step_offset, st)
-                             : run_impl<float>(b, n_steps, step_offset, st);
+    rc = ensure_recording(b, n_steps, step_offset, st);
+    if (rc) return rc;
+    rc = b->precision == 8 ? run_impl<double>(b, n_steps, step_offset, st)
+                           : run_impl<float>(b, n_steps, step_offset, st);
+    if (rc) return rc;
+    // The status word after this run, read by the next run once the copy has landed (a run
+    // captured into the caller's graph leaves it to acf_device_status).
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    ACF_CUDA(cudaStreamIsCapturing(st, &capturing));
+    if (capturing == cudaStreamCaptureStatusNone) {
+        ACF_CUDA(cudaMemcpyAsync(b->status_host, b->error_flag(), sizeof(int32_t),
+                                 cudaMemcpyDeviceToHost, st));
+        ACF_CUDA(cudaEventRecord(b->status_event, st));
+        b->status_pending = true;
+    }
+    return ACF_OK;
 }
 
 // A room cut into x slabs, one single-room two-sweep solver per part, advanced together. Each
@@ -3509,6 +3888,20 @@ int profile_read(acf_batch *b, double *velocity_ms, double *pressure_ms, int64_t
     *velocity_ms = b->prof_velocity_ms;
     *pressure_ms = b->prof_pressure_ms;
     *launches = b->prof_launches;
+    return ACF_OK;
+}
+
+// The status word (kStatus* bits) after every queued kernel has finished; clears it.
+int device_status(acf_batch *b, int32_t *status) {
+    if (!b || !status) return fail(ACF_ERR_ARGUMENT, "null argument");
+    DeviceGuard guard(b->device);
+    ACF_CUDA(cudaDeviceSynchronize());
+    int32_t flag = 0;
+    ACF_CUDA(cudaMemcpy(&flag, b->error_flag(), sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag) ACF_CUDA(cudaMemset(b->error_flag(), 0, sizeof(flag)));
+    b->status_pending = false;
+    *b->status_host = 0;
+    *status = flag;
     return ACF_OK;
 }
 
@@ -4325,6 +4718,205 @@ int batch_adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, d
     return ACF_OK;
 }
 
+// ------------------------------------------------------------------------------------------
+// Impulse-response post-processing in FP64 (ac-fdtd src/ac_fdtd/metrics.py:57-111 and the
+// spectral division of src/ac_fdtd/sources.py:80-108): the steps after the time loop, on the
+// receiver signals where the recordings already are. One CTA per channel; every sum in FP64.
+
+constexpr int kPostThreads = 1024;
+
+// Exclusive scan of one double per thread over the CTA (kPostThreads threads, thread order);
+// `shared` holds 32 doubles. Returns the sum of the values of the threads before this one;
+// *total gets the CTA's sum.
+__device__ double block_exclusive_scan(double v, double *shared, double *total) {
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double inclusive = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double up = __shfl_up_sync(0xffffffffu, inclusive, d);
+        if (lane >= (unsigned)d) inclusive += up;
+    }
+    double within = __shfl_up_sync(0xffffffffu, inclusive, 1);
+    if (lane == 0) within = 0.0;
+    if (lane == 31) shared[warp] = inclusive;
+    __syncthreads();
+    if (warp == 0) {
+        double w = shared[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double up = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= (unsigned)d) w += up;
+        }
+        shared[lane] = w;
+    }
+    __syncthreads();
+    const double before = warp > 0 ? shared[warp - 1] : 0.0;
+    *total = shared[31];
+    __syncthreads();
+    return lane == 0 ? before : before + within;
+}
+
+__device__ double block_sum(double v, double *shared) {
+    double total;
+    block_exclusive_scan(v, shared, &total);
+    return total;
+}
+
+__device__ int64_t block_min(int64_t v, int64_t *shared) {
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = min(v, (int64_t)__shfl_xor_sync(0xffffffffu, v, d));
+    if (lane == 0) shared[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t w = shared[lane];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) w = min(w, (int64_t)__shfl_xor_sync(0xffffffffu, w, d));
+        if (lane == 0) shared[0] = w;
+    }
+    __syncthreads();
+    const int64_t out = shared[0];
+    __syncthreads();
+    return out;
+}
+
+// Schroeder's backward integral I(k) = sum_{m >= k} h(m)^2, as 10 log10 max(I(k) / I(0),
+// 1e-300) floored at `floor_db` (metrics.py:57-69). Thread t owns a contiguous run of the
+// reversed signal; one CTA scan of the runs' sums gives each run's starting value.
+__global__ void __launch_bounds__(kPostThreads) schroeder_decay_kernel(const double *response, int64_t n,
+                                                                       double floor_db, double *decay) {
+    __shared__ double shared[32];
+    const double *h = response + (int64_t)blockIdx.x * n;
+    double *out = decay + (int64_t)blockIdx.x * n;
+    const int64_t run = (n + kPostThreads - 1) / kPostThreads;
+    const int64_t q0 = min((int64_t)threadIdx.x * run, n), q1 = min(q0 + run, n);
+    double mine = 0.0;
+    for (int64_t q = q0; q < q1; q++) {
+        const double x = h[n - 1 - q];
+        mine += x * x;
+    }
+    double total;
+    double running = block_exclusive_scan(mine, shared, &total);   // the later runs in time
+    for (int64_t q = q0; q < q1; q++) {
+        const double x = h[n - 1 - q];
+        running += x * x;
+        const double level = 10.0 * log10(fmax(running / total, 1e-300));
+        out[n - 1 - q] = fmax(level, floor_db);
+    }
+}
+
+// Seconds per 60 dB from a least-squares line through the decay curve between the first sample
+// at or below `upper` dB and the first at or below `lower` dB (metrics.py:72-84); NaN and
+// `failed[c] = 1` when the curve does not reach `lower` after `upper`, where the reference
+// raises.
+__global__ void __launch_bounds__(kPostThreads) decay_fit_kernel(const double *decay, int64_t n,
+                                                                 double sample_rate, double upper,
+                                                                 double lower, double *seconds,
+                                                                 int32_t *failed) {
+    __shared__ double shared[32];
+    __shared__ int64_t ishared[32];
+    const double *d = decay + (int64_t)blockIdx.x * n;
+    int64_t first_upper = n, first_lower = n;
+    for (int64_t k = threadIdx.x; k < n; k += kPostThreads) {
+        const double v = d[k];
+        if (v <= upper && k < first_upper) first_upper = k;
+        if (v <= lower && k < first_lower) first_lower = k;
+    }
+    int64_t start = block_min(first_upper, ishared), end = block_min(first_lower, ishared);
+    if (start == n) start = 0;   // numpy.argmax of an all-false mask
+    if (end == n) end = 0;
+    if (end <= start) {
+        if (threadIdx.x == 0) {
+            seconds[blockIdx.x] = __longlong_as_double(0x7ff8000000000000ll);
+            failed[blockIdx.x] = 1;
+        }
+        return;
+    }
+    const double m = (double)(end - start);
+    double sx = 0.0, sy = 0.0;
+    for (int64_t k = start + threadIdx.x; k < end; k += kPostThreads) {
+        sx += (double)k / sample_rate;
+        sy += d[k];
+    }
+    const double mean_x = block_sum(sx, shared) / m, mean_y = block_sum(sy, shared) / m;
+    double sxy = 0.0, sxx = 0.0;
+    for (int64_t k = start + threadIdx.x; k < end; k += kPostThreads) {
+        const double x = (double)k / sample_rate - mean_x;
+        sxy += x * (d[k] - mean_y);
+        sxx += x * x;
+    }
+    const double slope = block_sum(sxy, shared) / block_sum(sxx, shared);
+    if (threadIdx.x == 0) {
+        seconds[blockIdx.x] = -60.0 / slope;
+        failed[blockIdx.x] = 0;
+    }
+}
+
+// Early-to-late energy ratio in dB with the split at sample `boundary` (metrics.py:104-110).
+__global__ void __launch_bounds__(kPostThreads) clarity_kernel(const double *response, int64_t n,
+                                                               int64_t boundary, double *db) {
+    __shared__ double shared[32];
+    const double *h = response + (int64_t)blockIdx.x * n;
+    double early = 0.0, late = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += kPostThreads) {
+        const double e = h[k] * h[k];
+        if (k < boundary) early += e;
+        else late += e;
+    }
+    early = block_sum(early, shared);
+    late = block_sum(late, shared);
+    if (threadIdx.x == 0) db[blockIdx.x] = 10.0 * log10(early / late);
+}
+
+// Largest |S(f)|^2 of the excitation's spectrum (the regularisation's scale).
+__global__ void __launch_bounds__(kPostThreads) spectrum_peak_power(const double2 *source, int64_t bins,
+                                                                   double *peak) {
+    __shared__ double shared[32];
+    double best = 0.0;
+    for (int64_t k = threadIdx.x; k < bins; k += kPostThreads) {
+        const double a = hypot(source[k].x, source[k].y);
+        best = fmax(best, a * a);
+    }
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, d));
+    if (lane == 0) shared[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+        double w = shared[lane];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, d));
+        if (lane == 0) *peak = w;
+    }
+}
+
+// R(f) = X(f) conj(S(f)) / (|S(f)|^2 + reg * max |S|^2), zero above max_frequency, for every
+// channel's spectrum X (sources.py:103-107). Bin k is at k * bin_hz, as numpy.fft.rfftfreq.
+__global__ void spectral_divide_kernel(const double2 *spectra, const double2 *source, int64_t channels,
+                                       int64_t bins, double bin_hz, double max_frequency,
+                                       double regularisation, const double *peak, double2 *out) {
+    const int64_t at = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (at >= channels * bins) return;
+    const int64_t k = at % bins;
+    double2 r = make_double2(0.0, 0.0);
+    if (!((double)k * bin_hz > max_frequency)) {
+        const double2 x = spectra[at], src = source[k];
+        const double a = hypot(src.x, src.y);
+        const double denominator = a * a + regularisation * *peak;
+        // x * conj(src): (x.x src.x - x.y (-src.y)) + (x.x (-src.y) + x.y src.x) i
+        const double re = x.x * src.x - x.y * -src.y;
+        const double im = x.x * -src.y + x.y * src.x;
+        r = make_double2(re / denominator, im / denominator);
+    }
+    out[at] = r;
+}
+
+int check_post_args(const void *a, const void *b, int64_t channels, int64_t n) {
+    if (!a || !b) return fail(ACF_ERR_ARGUMENT, "null device array");
+    if (channels < 1 || channels > 65535 || n < 1) return fail(ACF_ERR_ARGUMENT, "need 1..65535 channels of at least one sample");
+    return ACF_OK;
+}
+
 }  // namespace
 
 // ==========================================================================================
@@ -4505,14 +5097,19 @@ int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages, int32_t vector)
     return ACF_OK;
 }
 
-int acf_device_status(acf_solver *h, int32_t *status) {
-    if (!h || !status) return fail(ACF_ERR_ARGUMENT, "null argument");
-    DeviceGuard guard(h->device);
-    ACF_CUDA(cudaDeviceSynchronize());
-    int32_t flag = 0;
-    ACF_CUDA(cudaMemcpy(&flag, h->error_flag(), sizeof(flag), cudaMemcpyDeviceToHost));
-    if (flag) ACF_CUDA(cudaMemset(h->error_flag(), 0, sizeof(flag)));
-    *status = flag;
+int acf_device_status(acf_solver *h, int32_t *status) { return device_status(h, status); }
+
+int acf_batch_device_status(acf_batch *b, int32_t *status) { return device_status(b, status); }
+
+int acf_set_wait_test(acf_solver *h, int64_t wait_limit_ns, int32_t skip_plane) {
+    if (!h) return fail(ACF_ERR_ARGUMENT, "null handle");
+    if (wait_limit_ns != 0 && (wait_limit_ns < 1000000 || wait_limit_ns > (int64_t)kWaitLimitNs))
+        return fail(ACF_ERR_ARGUMENT, "wait limit must be 0 (as built) or in [1 ms, %llu ns], got %lld",
+                    (unsigned long long)kWaitLimitNs, (long long)wait_limit_ns);
+    if (skip_plane < -1) return fail(ACF_ERR_ARGUMENT, "skip_plane must be -1 (none) or a plane index");
+    h->test_wait_limit_ns = (uint64_t)wait_limit_ns;
+    h->test_skip_plane = skip_plane;
+    h->graph_dirty = true;     // the staged parameters are baked into captured graphs
     return ACF_OK;
 }
 
@@ -4798,6 +5395,52 @@ int acf_energy_terms_noalloc(const void *p, const void *vx, const void *vy, cons
                                                            (const float *)vy, (const float *)vz,
                                                            nx, ny, nz, inv_dx, scratch);
     energy_finish<<<1, 32, 0, st>>>(scratch, nx + 1, terms_device);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+int acf_schroeder_decay(const double *response, int64_t channels, int64_t n, double floor_db,
+                        double *decay, acf_stream stream) {
+    int rc = check_post_args(response, decay, channels, n);
+    if (rc) return rc;
+    schroeder_decay_kernel<<<(unsigned)channels, kPostThreads, 0, (cudaStream_t)stream>>>(response, n, floor_db, decay);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+int acf_decay_fit(const double *decay, int64_t channels, int64_t n, double sample_rate, double upper_db,
+                  double lower_db, double *seconds, int32_t *failed, acf_stream stream) {
+    int rc = check_post_args(decay, seconds, channels, n);
+    if (rc) return rc;
+    if (!failed) return fail(ACF_ERR_ARGUMENT, "null device array");
+    if (!(sample_rate > 0.0)) return fail(ACF_ERR_ARGUMENT, "sample rate must be positive");
+    decay_fit_kernel<<<(unsigned)channels, kPostThreads, 0, (cudaStream_t)stream>>>(decay, n, sample_rate, upper_db,
+                                                                                lower_db, seconds, failed);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+int acf_clarity(const double *response, int64_t channels, int64_t n, int64_t boundary, double *db,
+                acf_stream stream) {
+    int rc = check_post_args(response, db, channels, n);
+    if (rc) return rc;
+    clarity_kernel<<<(unsigned)channels, kPostThreads, 0, (cudaStream_t)stream>>>(response, n, boundary, db);
+    ACF_CUDA(cudaGetLastError());
+    return ACF_OK;
+}
+
+int acf_spectral_divide(const void *spectra, const void *source, int64_t channels, int64_t bins,
+                        double bin_hz, double max_frequency, double regularisation, double *scratch,
+                        void *out, acf_stream stream) {
+    int rc = check_post_args(spectra, source, channels, bins);
+    if (rc) return rc;
+    if (!scratch || !out) return fail(ACF_ERR_ARGUMENT, "null device array");
+    cudaStream_t st = (cudaStream_t)stream;
+    spectrum_peak_power<<<1, kPostThreads, 0, st>>>((const double2 *)source, bins, scratch);
+    const int64_t total = channels * bins;
+    spectral_divide_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        (const double2 *)spectra, (const double2 *)source, channels, bins, bin_hz, max_frequency,
+        regularisation, scratch, (double2 *)out);
     ACF_CUDA(cudaGetLastError());
     return ACF_OK;
 }

@@ -153,19 +153,56 @@ class ImpulseResponse:
     max_frequency: float
     grid: Grid
 
+    def decay_metrics(self, device: bool = True) -> dict:
+        """T20, T30, EDT (seconds), C50 and C80 (dB) of every receiver's response, computed in
+        FP64 on the GPU (``ac_fdtd_b200.postprocess``) or, with ``device=False``, on the host
+        in the reference's arithmetic. A response too short for a fit gives NaN there."""
+        if device:
+            from . import postprocess as where
+        else:
+            where = _HostMetrics
+        out = {}
+        for name, fit in (("t20", lambda s: where.reverberation_time(s, self.sample_rate, 20.0)),
+                          ("t30", lambda s: where.reverberation_time(s, self.sample_rate, 30.0)),
+                          ("edt", lambda s: where.early_decay_time(s, self.sample_rate))):
+            values = []
+            for signal in self.signals:
+                try:
+                    values.append(float(fit(signal)))
+                except ValueError:
+                    values.append(float("nan"))
+            out[name] = np.array(values)
+        for name, split in (("c50", 0.05), ("c80", 0.08)):
+            out[name] = np.array([float(where.clarity(signal, self.sample_rate, split))
+                                  for signal in self.signals])
+        return out
+
+
+class _HostMetrics:
+    reverberation_time = staticmethod(lambda *a: reverberation_time(*a))
+    early_decay_time = staticmethod(lambda *a: early_decay_time(*a))
+    clarity = staticmethod(lambda *a: clarity(*a))
+
 
 def simulate_impulse_response(room: Room, source, receivers, max_frequency: float,
                               duration: float | None = None,
                               points_per_wavelength: float = DEFAULT_POINTS_PER_WAVELENGTH,
                               courant: float = 1.0, *, dtype=np.float64,
-                              solver_class=CudaAcousticFDTD, **solver_options) -> ImpulseResponse:
+                              solver_class=CudaAcousticFDTD, postprocess: str | None = None,
+                              **solver_options) -> ImpulseResponse:
     """Excite ``room`` at ``source`` and return the impulse responses at ``receivers``.
 
     Same steps and defaults as ac-fdtd's ``simulate_impulse_response``; ``dtype`` defaults to
     float64 as there, and float32 is the fast setting. ``solver_class`` may be any class with
     the reference solver's constructor and methods (the reference's own ``AcousticFDTD``
-    included).
+    included). ``postprocess``: ``"device"`` deconvolves on the GPU in FP64 from the recordings
+    in device memory (the default with the CUDA solver; equal to the reference's host
+    arithmetic to rounding), ``"host"`` in the reference's NumPy arithmetic (bit for bit).
     """
+    if postprocess is None:
+        postprocess = "device" if issubclass(solver_class, CudaAcousticFDTD) else "host"
+    if postprocess not in ("device", "host"):
+        raise ValueError(f"postprocess must be 'device' or 'host', got {postprocess!r}")
     grid = Grid.from_max_frequency(room.dimensions, max_frequency=max_frequency,
                                    sound_speed=room.medium.sound_speed,
                                    points_per_wavelength=points_per_wavelength)
@@ -180,9 +217,16 @@ def simulate_impulse_response(room: Room, source, receivers, max_frequency: floa
     for receiver in receivers:
         solver.add_pressure_receiver(receiver)
     solver.run(n_steps)
-    recorded = solver.recorded_pressure
+    if postprocess == "device":
+        from . import postprocess as device
+
+        on_device = solver.recorded_pressure_device()
+        signals = device.deconvolve(on_device, excitation, solver.dt, max_frequency)
+        recorded = on_device.cpu().numpy()
+    else:
+        recorded = solver.recorded_pressure
+        signals = deconvolve(recorded, excitation, solver.dt, max_frequency)
     return ImpulseResponse(
-        signals=deconvolve(recorded, excitation, solver.dt, max_frequency),
-        recorded=recorded, excitation=excitation, sample_rate=1.0 / solver.dt,
+        signals=signals, recorded=recorded, excitation=excitation, sample_rate=1.0 / solver.dt,
         max_frequency=max_frequency, grid=grid,
     )

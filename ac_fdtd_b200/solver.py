@@ -98,6 +98,18 @@ class _PinnedBlock:
             self.pointer = ctypes.c_void_p()
 
 
+def raise_for_status(word: int) -> None:
+    """Turn a device status word (``acf_device_status``) into the error it reports."""
+    if word & _native.STATUS_NON_FINITE:
+        raise _native.NativeError(_native.ERR_NUMERIC, "acf_device_status",
+                                  "a sweep produced a non-finite pressure (NaN or infinity); "
+                                  "the state is not valid")
+    if word & _native.STATUS_WAIT_TIMEOUT:
+        raise _native.NativeError(_native.ERR_STATE, "acf_device_status",
+                                  "a staged sweep timed out waiting for its bulk copies; the "
+                                  "solver state is not valid")
+
+
 def pinned_array(shape, dtype=np.float32) -> np.ndarray:
     """A zeroed numpy array in page-locked host memory (full-speed host<->device copies)."""
     array = np.asarray(_PinnedBlock(_native.library(), tuple(shape), np.dtype(dtype)))
@@ -391,6 +403,25 @@ class CudaAcousticFDTD:
             )
         return np.stack(rows)
 
+    def recorded_pressure_device(self):
+        """``recorded_pressure`` as a CUDA tensor ``(channel, sample)`` in the solver's dtype,
+        copied device to device (for post-processing on the GPU; ``postprocess``)."""
+        import torch
+
+        self._push_points()
+        starts = {start for _, start in self._receivers}
+        if len(starts) > 1:
+            raise ValueError("receivers were added at different steps; their recordings are ragged")
+        n = self.step_index - (starts.pop() if starts else 0)
+        dtype = torch.float64 if self.dtype == np.float64 else torch.float32
+        out = torch.empty((len(self._receivers), max(n, 0)), dtype=dtype,
+                          device=f"cuda:{self.device}")
+        for r, (_, start) in enumerate(self._receivers):
+            if n > 0:
+                _native.check(self._lib.acf_read_recording(
+                    self._handle, r, start, n, out[r].data_ptr(), self._stream), "acf_read_recording")
+        return out
+
     def recording(self, receiver: int) -> np.ndarray:
         """Samples of one receiver since it was added."""
         self._push_points()
@@ -454,18 +485,19 @@ class CudaAcousticFDTD:
         return int(pointer.value or 0), (int(strides[0]), int(strides[1]), int(strides[2]))
 
     def synchronize(self) -> None:
+        """Wait for the device, then raise if a sweep reported a non-finite pressure or a
+        staged sweep gave up waiting (``check_device``)."""
         _native.check(self._lib.acf_synchronize(self._stream), "acf_synchronize")
-        if self.scheme == "staged":
-            self.check_device()
+        self.check_device()
 
     def check_device(self) -> None:
-        """Raise if a staged sweep gave up waiting for its copies (the state is then invalid)."""
+        """Raise :class:`~ac_fdtd_b200._native.NativeError` if a sweep produced a non-finite
+        pressure (status ``ACF_ERR_NUMERIC``) or a staged sweep gave up waiting for its copies
+        (``ACF_ERR_STATE``); the state is then not valid. Clears the device's report."""
         status = ctypes.c_int32(0)
         _native.check(self._lib.acf_device_status(self._handle, ctypes.byref(status)),
                       "acf_device_status")
-        if status.value:
-            raise RuntimeError("a staged sweep timed out waiting for its bulk copies; "
-                               "the solver state is not valid")
+        raise_for_status(status.value)
 
     # ------------------------------------------------------------------ diagnostics
     def energy_terms(self, planes: tuple[int, int] | None = None,

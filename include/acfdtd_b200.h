@@ -102,7 +102,10 @@ int acf_device_count(int *count);
  * selection need not change. No counterpart in the reference (one CPU pool per process). */
 int acf_set_device(int32_t device);
 
-/* Handle lifetime. acf_create allocates zeroed device state on the current device. */
+/* Handle lifetime. acf_create allocates zeroed device state on the current device. With the
+ * environment variable ACF_INJECT_ALLOC_FAILURE set (non-empty, not "0"), acf_create and
+ * acf_batch_create fail with ACF_ERR_MEMORY before allocating, as on an exhausted device: a
+ * test hook for callers' error paths. */
 int acf_create(const acf_config *config, acf_solver **out);
 int acf_destroy(acf_solver *solver);
 int acf_is_double(const acf_solver *solver);
@@ -120,8 +123,8 @@ int acf_set_sources(acf_solver *solver, int64_t n, const int64_t *cell, const in
 int acf_set_receivers(acf_solver *solver, int64_t n, const int64_t *cell,
                       const int64_t *start_step);
 
-/* Copy `n` samples of receiver r, starting at absolute step `first_step`, to host memory
- * `dst` (solver precision). Synchronous. */
+/* Copy `n` samples of receiver r, starting at absolute step `first_step`, to `dst` (host or
+ * device memory, solver precision). Synchronous. */
 int acf_read_recording(acf_solver *solver, int64_t receiver, int64_t first_step, int64_t n,
                        void *dst, acf_stream stream);
 
@@ -162,10 +165,23 @@ int acf_get_prefetch(const acf_solver *solver);
  * automatic stages, 4 elements. No counterpart in the reference. */
 int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages, int32_t vector);
 
-/* 0 when no kernel of this solver reported a failed wait; 1 (and the flag cleared) when a
- * staged sweep gave up waiting for its copies, in which case the state is not valid.
- * Synchronizes the solver's device. No counterpart in the reference. */
+/* The solver's device status word, then cleared: 0 when nothing was reported; bit 1 when a
+ * staged sweep gave up waiting for its copies; bit 2 when a sweep produced a non-finite
+ * pressure (NaN or infinity: every sweep that writes p checks what it writes). Either way the
+ * state is not valid. Synchronizes the solver's device. acf_run and acf_batch_run also read
+ * the word copied after the previous run, without waiting for the device, and return
+ * ACF_ERR_NUMERIC (bit 2) or ACF_ERR_STATE (bit 1) before launching anything. The reference
+ * has no such check (its NumPy and C loops run on whatever the state holds). */
 int acf_device_status(acf_solver *solver, int32_t *status);
+int acf_batch_device_status(acf_batch *batch, int32_t *status);
+
+/* Test hook of the staged sweep, for exercising its bounded waits without a fault: every wait
+ * gives up after `wait_limit_ns` (0: the built-in two seconds; else 1 ms to two seconds), and
+ * the producer of the grid's first CTA leaves out the copies of x plane `skip_plane` (-1:
+ * none), so that CTA's consumers wait for data that never arrives, run out of time, raise bit
+ * 1 of the status word and return; the producer drains the copies it did issue before the CTA
+ * exits. No counterpart in the reference. */
+int acf_set_wait_test(acf_solver *solver, int64_t wait_limit_ns, int32_t skip_plane);
 
 /* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
 int acf_set_graph(acf_solver *solver, int32_t steps_per_graph);
@@ -283,7 +299,42 @@ int acf_profile_read(acf_solver *solver, double *velocity_ms, double *pressure_m
 /* Kernels launched by this handle since creation (sweeps, graph replays counted per kernel). */
 int64_t acf_launch_count(const acf_solver *solver);
 
-/* ---- Batches of rooms -------------------------------------------------------------------
+/* ---- Impulse-response post-processing (FP64, on the device) ----------------------------
+ *
+ * The steps after the time loop of the reference's room workflow (src/ac_fdtd/room.py:121-176),
+ * on receiver signals in device memory: `channels` signals of `n` samples, back to back. Every
+ * array argument is a device pointer; each call is asynchronous on `stream` and allocates
+ * nothing. Sums are FP64 in another order than NumPy's sequential ones, so results agree with
+ * the reference to rounding (about 1e-14 relative), not bit for bit. */
+
+/* Schroeder decay curve in dB, 10 log10 max(I(k)/I(0), 1e-300) floored at `floor_db`, with
+ * I(k) the backward integral of the squared signal (src/ac_fdtd/metrics.py:57-69). */
+int acf_schroeder_decay(const double *response, int64_t channels, int64_t n, double floor_db,
+                        double *decay, acf_stream stream);
+
+/* Seconds per 60 dB of a least-squares line through each decay curve, between the first
+ * sample at or below `upper_db` and the first at or below `lower_db` (metrics.py:72-101: T20
+ * is (-5, -25), EDT (0, -10)). `seconds` and `failed` hold one value per channel; failed[c] = 1
+ * (seconds NaN) where the curve does not reach `lower_db` after `upper_db`, where the reference
+ * raises ValueError. */
+int acf_decay_fit(const double *decay, int64_t channels, int64_t n, double sample_rate, double upper_db,
+                  double lower_db, double *seconds, int32_t *failed, acf_stream stream);
+
+/* Early-to-late energy ratio in dB per channel, split before sample `boundary` (C50 with
+ * boundary = round(0.05 fs); metrics.py:104-110). */
+int acf_clarity(const double *response, int64_t channels, int64_t n, int64_t boundary, double *db,
+                acf_stream stream);
+
+/* The division step of the reference's deconvolution (src/ac_fdtd/sources.py:103-107) on
+ * spectra from a real-to-complex FFT (interleaved complex doubles): out = X conj(S) /
+ * (|S|^2 + regularisation max|S|^2), zero in bins k with k * bin_hz > max_frequency, for each
+ * of `channels` spectra X of `bins` bins and the excitation's spectrum S. `scratch` is one
+ * device double. The FFTs themselves are the caller's (a library FFT). */
+int acf_spectral_divide(const void *spectra, const void *source, int64_t channels, int64_t bins,
+                        double bin_hz, double max_frequency, double regularisation, double *scratch,
+                        void *out, acf_stream stream);
+
+/* ---- Batches of rooms/* ---- Batches of rooms -------------------------------------------------------------------
  *
  * Many rooms of different sizes advanced together: each sweep is one persistent launch over a
  * flat tile table covering every room, and runs replay CUDA graphs of both sweeps. No

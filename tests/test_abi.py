@@ -59,3 +59,6 @@ def test_null_arguments_are_refused():
     assert lib.acf_run(None, 1, 0, None) == 1
     assert lib.acf_upload(None, 0, None, None) == 1
     assert lib.acf_launch_count(None) == -1
+    assert lib.acf_set_wait_test(None, 0, -1) == 1
+    assert lib.acf_batch_device_status(None, None) == 1
+    assert lib.acf_device_status(None, None) == 1

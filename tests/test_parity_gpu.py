@@ -340,3 +340,73 @@ def test_an_explicit_device_gives_the_same_results():
     batch.set_field(0, 0, np.random.default_rng(0).standard_normal(GRID.shape))
     batch.run(5)
     assert np.all(np.isfinite(batch.p(0)))
+
+
+@pytest.mark.parametrize("faces", [None, ((0, 0), (0, 1)), ((1, 1), (2, 0))])
+def test_lean_single_precision_fused_column_matches_the_oracle(faces):
+    """Single precision with nz a multiple of 4 runs the fused step through the lean column
+    (packed arithmetic, damping skipped where the profile is exactly 1). Grids with one chunk,
+    one row, one plane, sponges on every face or on some only (so rows, chunks and planes
+    with and without damping meet in one warp), walls, air, points on the edges: the
+    oracle's float32 bits, with the L2 prefetch off and on."""
+    from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid
+
+    layer = AbsorbingLayer(thickness=3) if faces is None else AbsorbingLayer(thickness=3, faces=faces)
+    configuration = dict(walls=WallAdmittances(0.4, 0.1, 0.0, 0.7, 0.2, 0.05),
+                         absorbing_layer=layer, air_absorption=AirAbsorption())
+    for shape in ((13, 11, 24), (1, 1, 4), (6, 1, 8), (2, 9, 4), (9, 10, 40), (5, 3, 12),
+                  (4, 37, 132)):
+        grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
+        initial = np.random.default_rng(sum(shape)).standard_normal(shape).astype(np.float32)
+        corner = tuple((n - 0.5) * 0.02 for n in shape)
+        oracle = OracleFDTD(grid, AIR, dtype=np.float32, **configuration)
+        solvers = [oracle]
+        for prefetch in (False, True):
+            cuda = CudaAcousticFDTD(grid, dtype=np.float32, scheme="fused", steps_per_graph=6,
+                                    **configuration)
+            cuda.set_prefetch(prefetch)
+            solvers.append(cuda)
+        for solver in solvers:
+            solver.p[:] = initial
+            solver.add_volume_source((0.0, 0.0, 0.0), np.hanning(12))
+            solver.add_volume_source(corner, np.hanning(7))
+            solver.add_pressure_receiver(corner)
+            solver.add_pressure_receiver((0.0, corner[1], 0.0))
+        for solver in solvers:
+            solver.run(33)
+        for cuda in solvers[1:]:
+            assert_same_state(cuda, oracle)
+            for got, (want, *_rest) in zip(cuda.relaxation_states, oracle.relax, strict=True):
+                np.testing.assert_array_equal(got, want)
+            cuda.close()
+
+
+@pytest.mark.parametrize("planes", [1, 3, 16])
+def test_lean_column_plane_groups_and_graphs(planes):
+    """Blocks marching 1, 3 or 16 planes (a group ending inside the sponge, the last group
+    short), in graph replays and run in pieces, on a 48^2 x 64 room with the bench's sponge on
+    both x faces: the two-sweep scheme's bits."""
+    from ac_fdtd_b200 import AbsorbingLayer, AirAbsorption, Grid
+
+    grid = Grid(dx=0.01, nx=50, ny=48, nz=64)
+    configuration = dict(walls=WallAdmittances(0.3, 0.2, 0.1, 0.05, 0.25, 0.15),
+                         absorbing_layer=AbsorbingLayer(thickness=8, faces=((0, 0), (0, 1))),
+                         air_absorption=AirAbsorption())
+    initial = np.random.default_rng(5).standard_normal(grid.shape).astype(np.float32)
+    out = []
+    for scheme in ("two_sweeps", "fused"):
+        cuda = CudaAcousticFDTD(grid, dtype=np.float32, scheme=scheme, steps_per_graph=8,
+                                **configuration)
+        if scheme == "fused":
+            cuda.set_launch(64, planes)
+        cuda.p[:] = initial
+        cuda.add_volume_source((0.2, 0.2, 0.3), np.hanning(20))
+        cuda.add_pressure_receiver((0.45, 0.3, 0.1))
+        for n in (17, 1, 24):
+            cuda.run(n)
+        out.append((cuda.p.copy(), cuda.recorded_pressure, [v.copy() for v in cuda.velocity]))
+        cuda.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    for a, b in zip(out[0][2], out[1][2], strict=True):
+        np.testing.assert_array_equal(a, b)

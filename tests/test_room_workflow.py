@@ -75,7 +75,28 @@ def test_workflow_on_the_gpu_reproduces_the_reference_bitwise(impulse, scheme):
     data = _golden_impulse()
     ir = simulate_impulse_response(make_room(impulse), tuple(impulse["source"]),
                                    [tuple(r) for r in impulse["receivers"]],
-                                   impulse["max_frequency"], scheme=scheme)
+                                   impulse["max_frequency"], scheme=scheme, postprocess="host")
     np.testing.assert_array_equal(ir.recorded, data["recorded"])
     np.testing.assert_array_equal(ir.signals, data["signals"])
     assert ir.sample_rate == impulse["sample_rate"]
+
+
+@pytest.mark.gpu
+def test_workflow_with_device_postprocessing_matches_the_reference(impulse):
+    """The default with the CUDA solver: recordings stay on the GPU and are deconvolved there in
+    FP64 (cuFFT, this library's spectral division); the reference's signals to 1e-12 of their
+    peak, and its decay metrics to 1e-12 relative."""
+    data = _golden_impulse()
+    ir = simulate_impulse_response(make_room(impulse), tuple(impulse["source"]),
+                                   [tuple(r) for r in impulse["receivers"]],
+                                   impulse["max_frequency"], scheme="fused")
+    np.testing.assert_array_equal(ir.recorded, data["recorded"])
+    peak = np.max(np.abs(data["signals"]))
+    assert np.max(np.abs(ir.signals - data["signals"])) <= 1e-12 * peak
+    f = impulse["formulae"]
+    metrics = ir.decay_metrics()
+    assert metrics["t20"][0] == pytest.approx(f["t20"], rel=1e-12)
+    assert metrics["edt"][0] == pytest.approx(f["edt"], rel=1e-12)
+    host = ir.decay_metrics(device=False)
+    for name in ("t20", "edt", "c50", "c80"):
+        np.testing.assert_allclose(metrics[name], host[name], rtol=1e-12)
