@@ -43,10 +43,10 @@ EXPORTED_SYMBOLS = (
     "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch", "acf_copy_plane",
     "acf_solver_device", "acf_energy_terms_planes", "acf_run_slabs", "acf_batch_device_status",
     "acf_set_wait_test", "acf_schroeder_decay", "acf_decay_fit", "acf_clarity",
-    "acf_spectral_divide",
+    "acf_spectral_divide", "acf_pressure_only_energy_terms",
 )
 
-SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED = 0, 1, 2
+SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED, SCHEME_PRESSURE_ONLY = 0, 1, 2, 3
 
 GRAD_WALLS, GRAD_AIR = 1, 2
 
@@ -142,6 +142,7 @@ _SIGNATURES = {
     "acf_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "acf_batch_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "acf_set_wait_test": (ctypes.c_int, [_P, _I64, ctypes.c_int32]),
+    "acf_pressure_only_energy_terms": (ctypes.c_int, [_P, _DP, _P]),
     "acf_schroeder_decay": (ctypes.c_int, [_P, _I64, _I64, ctypes.c_double, _P, _P]),
     "acf_decay_fit": (ctypes.c_int, [_P, _I64, _I64, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, _P, _P, _P]),

@@ -55,11 +55,14 @@ def _candidates(schemes, candidates, staged_candidates):
             yield (scheme, *geometry)
 
 
-def _key(solver) -> str:
+def _key(solver, schemes=SCHEMES) -> str:
     nx, ny, nz = solver._shape
     block = solver.coefficients
-    return json.dumps([nx, ny, nz, solver.dtype.name, block.n_relax,
-                       block.layer_cell is not None, block.wall_shell is not None])
+    key = [nx, ny, nz, solver.dtype.name, block.n_relax, block.layer_cell is not None,
+           block.wall_shell is not None]
+    if tuple(schemes) != SCHEMES:       # a race over other schemes is cached apart
+        key.append(sorted(schemes))
+    return json.dumps(key)
 
 
 def _load_file() -> dict:
@@ -127,7 +130,7 @@ def apply_tuned(solver, candidates=CANDIDATES, schemes=SCHEMES,
                 staged_candidates=STAGED_CANDIDATES):
     """Set the fastest scheme and geometry for this configuration (tuned once per shape
     class); returns (scheme, threads, planes) or ("staged", rows, stages, planes, vector)."""
-    key = _key(solver)
+    key = _key(solver, schemes)
     if key not in _cache:
         stored = _load_file().get(key)
         if stored:

@@ -1678,6 +1678,215 @@ __global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(float, LAYER, NR)) l
 }
 
 // ------------------------------------------------------------------------------------------
+// The pressure-only scheme: the second-order wave equation on p alone, two fields instead of
+// 4 + R (the scheme the reference plans as its milestone M8, PLAN.md:52-56, and has not built).
+//
+// Eliminating v from the staggered pair gives, exactly in real arithmetic, for a room with
+// rigid or impedance walls and no sponge or air (a = sum over the cell's absorbing faces of
+// c dt xi / (2 dx), a = 0 inside; fu = 1/(1+a), fp = a/(1+a) the wall pair of the p-v scheme):
+//
+//   p^{n+1} = fu (2 p^n + lam2 L p^n) - (fu - fp) p^{n-1} - S^{n-1} + S^n,   lam2 = c_p c_v
+//
+// where L p = sum over the cell's interior neighbours of (p_nb - p) (the rigid-face Neumann
+// Laplacian: the p-v update never moves a boundary face) and S^n is the volume source added
+// after step n. The first step after entering the scheme takes the p-v step itself from
+// (p^n, v^{n-1/2}), with the velocities folded in:
+//
+//   p^{n+1} = fu (p^n - c_p D(v^{n-1/2}) + lam2 L p^n) - fp p^n + S^n
+//
+// (D the divergence over all faces, as the pressure sweep forms it), so the pressures equal the
+// p-v scheme's to rounding from then on; boundary faces keep their velocity in both schemes.
+// Per cell and step it reads p^n and p^{n-1} and writes p^{n+1} over p^{n-1}: 3 elements.
+
+template <typename T>
+struct PressureOnlyParams {
+    Room<T> room;       // geometry, wall pairs, points, status; p, v: the current copy
+    const T *cur;       // p^n
+    T *next;            // p^{n-1} on entry (not read by the first step), p^{n+1} on exit
+    T lam2;             // c_p c_v = (c dt / dx)^2, rounded once from FP64
+    const int64_t *step_base;
+    int32_t local_step;
+    int32_t planes;
+};
+
+template <typename T>
+__device__ __forceinline__ T fma_t(T a, T b, T c) {
+    if constexpr (sizeof(T) == 4) return __fmaf_rn(a, b, c);
+    else return __fma_rn(a, b, c);
+}
+
+template <typename T, bool WALLS, bool FIRST>
+__device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T> &g, int i_begin,
+                                                     int i_end, int j, int c, int64_t step) {
+    const Room<T> &s = g.room;
+    const int k0 = c * kVec;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
+    const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+    const bool wall_column = !y_lo || !y_hi || !z_lo || k0 + kVec >= s.nz;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    bool all_points = false;
+    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const T lam2 = g.lam2, cp = s.cp;
+    T bad = T(0);
+
+    T Pm[kVec], P[kVec];
+    Vec4<T>::ldg(g.cur + (int64_t)i_begin * s.plane + column, P);
+    if (i_begin > 0) Vec4<T>::ldg(g.cur + (int64_t)(i_begin - 1) * s.plane + column, Pm);
+    else {
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Pm[e] = P[e];
+    }
+
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        const bool x_hi = i + 1 < s.nx;
+        if (s.prefetch && i + 1 < i_end) {   // the next plane's own-row inputs into L2
+            if (i + 2 < s.nx) prefetch_l2(g.cur + base + 2 * s.plane);
+            if (!FIRST) prefetch_l2(g.next + base + s.plane);
+        }
+        T Pp[kVec], Ym[kVec], Yp[kVec], Q[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Pp[e] = Ym[e] = Yp[e] = Q[e] = P[e];
+        if (x_hi) Vec4<T>::ldg(g.cur + base + s.plane, Pp);
+        if (y_lo) Vec4<T>::ldg(g.cur + base - s.pz, Ym);
+        if (y_hi) Vec4<T>::ldg(g.cur + base + s.pz, Yp);
+        const T zb = z_lo ? __ldg(g.cur + base - 1) : P[0];
+        const T za = z_hi ? __ldg(g.cur + base + kVec) : P[kVec - 1];
+        T D[kVec];
+        if constexpr (FIRST) {
+            T XL[kVec], XH[kVec], YL[kVec], YH[kVec], Z[kVec];
+            Vec4<T>::ldg(s.vx + base, XL);
+            Vec4<T>::ldg(s.vx + base + s.plane, XH);
+            Vec4<T>::ldg(s.vy + base, YL);
+            Vec4<T>::ldg(s.vy + base + s.pz, YH);
+            Vec4<T>::ldg(s.vz + base, Z);
+            const T above = k0 + kVec <= s.nz ? __ldg(s.vz + base + kVec) : T(0);
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                D[e] = XH[e] - XL[e];
+                D[e] = D[e] + (YH[e] - YL[e]);
+                D[e] = D[e] + ((e + 1 < kVec ? Z[e + 1] : above) - Z[e]);
+            }
+        } else {
+            Vec4<T>::load(g.next + base, Q);     // p^{n-1}: read, then overwritten by p^{n+1}
+        }
+
+        T Pn[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            const T p = P[e];
+            if (k >= s.nz) {          // padding
+                Pn[e] = p;
+                continue;
+            }
+            const T zm = e == 0 ? zb : P[e - 1];
+            const T zp = k + 1 < s.nz ? (e + 1 < kVec ? P[e + 1] : za) : p;
+            const T lap = ((Pm[e] - p) + (Pp[e] - p)) + ((Ym[e] - p) + (Yp[e] - p)) + ((zm - p) + (zp - p));
+            T fu = T(1), fp = T(0);
+            const bool wall = WALLS && (wall_column || i == 0 || i == s.nx - 1) &&
+                              wall_pair(s, i, j, k, fu, fp);
+            T pn;
+            if constexpr (FIRST) {
+                const T t = fma_t(lam2, lap, fma_t(-cp, D[e], p));
+                pn = wall ? fu * t - fp * p : t;
+            } else {
+                const T q = fma_t(lam2, lap, p + p);
+                pn = wall ? fu * q - (fu - fp) * Q[e] : q - Q[e];
+            }
+            Pn[e] = pn;
+        }
+        if (any_mine) {
+            // - S^{n-1} (added by the previous step), then + S^n, in the order added
+            uint32_t m = all_points ? 0u : source_bits(points, s.n_src);
+            for (int q = all_points ? 0 : -1; all_points ? q < s.n_src : m != 0; q++) {
+                if (!all_points) {
+                    q = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.src_off[q] - base;
+                if (d < 0 || d >= kVec || k0 + d >= s.nz) continue;
+#pragma unroll
+                for (int e = 0; e < kVec; e++) {
+                    if (e != d) continue;
+                    if (!FIRST && step >= 1 && step - 1 < s.src_len[q])
+                        Pn[e] = Pn[e] - s.cs * s.src_sig[q * s.src_stride + step - 1];
+                    if (step < s.src_len[q]) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < kVec; e++) bad = finite_acc(bad, Pn[e]);
+        Vec4<T>::store(g.next + base, Pn);
+        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            Pm[e] = P[e];
+            P[e] = Pp[e];
+        }
+    }
+    report_nonfinite(s.status, bad != bad);
+}
+
+template <typename T, bool WALLS, bool FIRST>
+__global__ void __launch_bounds__(256) pressure_only_sweep(const PressureOnlyParams<T> g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= g.room.nchunks || j >= g.room.ny) return;
+    const bool any_point = (g.room.n_src | g.room.n_rec) != 0;
+    const int64_t step = any_point ? (*g.step_base + g.local_step) : 0;
+    const int i_begin = blockIdx.z * g.planes;
+    pressure_only_column<T, WALLS, FIRST>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
+}
+
+// The two sums of the pressure-only scheme's conserved energy after a step, with cur = p^{n+1}
+// and prev = p^n: terms 0 and 1 of `partials` hold sum (cur - prev)^2 and sum cur L prev (L the
+// Neumann Laplacian of the scheme); the other five are zero. Layout as energy_partials.
+template <typename T>
+__global__ void __launch_bounds__(256) pressure_only_energy_partials(const Room<T> s, const T *cur,
+                                                                     const T *prev, double *partials) {
+    double a = 0.0, b = 0.0;
+    const int64_t total = (int64_t)s.nx * s.ny * s.nz;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < total;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(n % s.nz);
+        const int64_t row = n / s.nz;
+        const int j = (int)(row % s.ny);
+        const int i = (int)(row / s.ny);
+        const int64_t o = (int64_t)i * s.plane + (int64_t)j * s.pz + k;
+        const double u = (double)cur[o], v = (double)prev[o];
+        a += (u - v) * (u - v);
+        double lap = 0.0;
+        if (i > 0) lap += (double)prev[o - s.plane] - v;
+        if (i + 1 < s.nx) lap += (double)prev[o + s.plane] - v;
+        if (j > 0) lap += (double)prev[o - s.pz] - v;
+        if (j + 1 < s.ny) lap += (double)prev[o + s.pz] - v;
+        if (k > 0) lap += (double)prev[o - 1] - v;
+        if (k + 1 < s.nz) lap += (double)prev[o + 1] - v;
+        b += u * lap;
+    }
+    __shared__ double red[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 16; d > 0; d >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, d);
+        b += __shfl_down_sync(0xffffffffu, b, d);
+    }
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x < kEnergyTerms) {
+        double v = 0.0;
+        if (threadIdx.x < 2)
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x][w];
+        partials[blockIdx.x * kEnergyTerms + threadIdx.x] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // One room: 2D grid of (chunk, row) threads; blockIdx.z selects a group of `planes` x planes.
 
 template <typename T, bool LAYER>
@@ -2702,6 +2911,10 @@ struct acf_batch {
     int32_t *status_host = nullptr;
     cudaEvent_t status_event = nullptr;
     bool status_pending = false;
+    // Pressure-only scheme: the next step starts from the p-v state (p^n, v^{n-1/2}); cleared by
+    // that step, after which the velocities of either copy are stale.
+    bool po_first = true;
+    bool po_started = false;
     // Test hooks of the staged sweep (acf_set_wait_test): 0 / -1 leave it as built.
     uint64_t test_wait_limit_ns = 0;
     int32_t test_skip_plane = -1;
@@ -2758,6 +2971,9 @@ struct acf_batch {
     int scheme = ACF_SCHEME_TWO_SWEEPS;
     // one sweep per step into the second copy of p and v (fused, or fused-staged for one room)
     bool fused() const { return scheme == ACF_SCHEME_FUSED || scheme == ACF_SCHEME_FUSED_STAGED; }
+    bool pressure_only() const { return scheme == ACF_SCHEME_PRESSURE_ONLY; }
+    // Schemes whose step writes the other copy of the state, so that the current one alternates.
+    bool alternating() const { return fused() || pressure_only(); }
     int32_t *error_flag() const { return reinterpret_cast<int32_t *>(step_base + 1); }
     char *field_ptr(int r, int f) const {
         const RoomHost &h = rooms[r];
@@ -3081,6 +3297,34 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
         }
         return;
     }
+    if (b->pressure_only()) {
+        RoomHost &h = b->rooms[0];
+        PressureOnlyParams<T> g{};
+        g.room = make_room<T>(b, 0);
+        g.cur = (const T *)b->field_ptr(0, ACF_FIELD_P);
+        g.next = (T *)b->other_ptr(0, ACF_FIELD_P);
+        g.lam2 = (T)(h.coef[0] * h.coef[1]);
+        g.step_base = b->step_base;
+        g.local_step = local;
+        g.planes = b->planes;
+        const LaunchShape L = single_shape(b);
+        const bool first = b->po_first;
+        b->po_first = false;
+        b->po_started = true;
+        if (first) {
+            if (h.has_walls) pressure_only_sweep<T, true, true><<<L.grid, L.block, 0, st>>>(g);
+            else pressure_only_sweep<T, false, true><<<L.grid, L.block, 0, st>>>(g);
+        } else {
+            if (h.has_walls) pressure_only_sweep<T, true, false><<<L.grid, L.block, 0, st>>>(g);
+            else pressure_only_sweep<T, false, false><<<L.grid, L.block, 0, st>>>(g);
+        }
+        h.cur ^= 1;
+        if (events) {
+            cudaEventRecord(events[1], st);
+            cudaEventRecord(events[2], st);
+        }
+        return;
+    }
     if (b->fused()) {
         RoomHost &h = b->rooms[0];
         FusedParams<T> f{};
@@ -3196,7 +3440,7 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
             }
             launch_step<T>(b, 0, st, b->ring + 3 * slot);
             bump_step_base<<<1, 1, 0, st>>>(b->step_base, 1);
-            b->launches += b->fused() ? 2 : 3;
+            b->launches += b->alternating() ? 2 : 3;
         }
         for (int64_t t = std::max<int64_t>(0, n_steps - R); t < n_steps; t++) {
             int rc = drain(t % R);
@@ -3207,7 +3451,14 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
     }
 
     int64_t done = 0;
-    const bool fused = b->fused();
+    if (b->pressure_only() && b->po_first) {
+        // The step from the p-v state is not the repeated one: launch it before any graph.
+        launch_step<T>(b, 0, st, nullptr);
+        bump_step_base<<<1, 1, 0, st>>>(b->step_base, 1);
+        b->launches += 2;
+        n_steps -= 1;
+    }
+    const bool fused = b->alternating();
     // A fused graph holds an even number of steps, so a replay leaves the buffers as it found
     // them; one graph is kept per starting buffer.
     const int64_t G = fused ? (b->graph_steps + 1) / 2 * 2 : b->graph_steps;
@@ -3956,10 +4207,22 @@ int make_primary(acf_batch *b, cudaStream_t st) {
 
 int set_scheme(acf_batch *b, int32_t scheme) {
     if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
-    if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED && scheme != ACF_SCHEME_FUSED_STAGED)
+    if (scheme != ACF_SCHEME_TWO_SWEEPS && scheme != ACF_SCHEME_FUSED && scheme != ACF_SCHEME_FUSED_STAGED &&
+        scheme != ACF_SCHEME_PRESSURE_ONLY)
         return fail(ACF_ERR_ARGUMENT, "unknown scheme %d", scheme);
     if (scheme == ACF_SCHEME_FUSED_STAGED && b->rooms.size() != 1)
         return fail(ACF_ERR_STATE, "the staged scheme is for single rooms");
+    if (scheme == ACF_SCHEME_PRESSURE_ONLY) {
+        if (b->rooms.size() != 1) return fail(ACF_ERR_STATE, "the pressure-only scheme is for single rooms");
+        const RoomHost &h = b->rooms[0];
+        if (h.has_layer || h.n_relax > 0)
+            return fail(ACF_ERR_STATE, "the pressure-only scheme has no absorbing layer or air "
+                        "absorption (the second-order pressure equation keeps no velocity or "
+                        "relaxation state for them)");
+    }
+    if (b->pressure_only() && scheme != ACF_SCHEME_PRESSURE_ONLY && b->po_started)
+        return fail(ACF_ERR_STATE, "the pressure-only scheme keeps no velocities: reset the state "
+                    "before switching to a scheme that steps them");
     if (scheme == ACF_SCHEME_FUSED_STAGED) {
         const RoomHost &h = b->rooms[0];
         if (staged_block_x(h, b->staged_vector) * b->staged_rows > kStagedMaxConsumers)
@@ -3985,6 +4248,10 @@ int set_scheme(acf_batch *b, int32_t scheme) {
         ACF_CUDA(cudaStreamSynchronize(0));
     }
     if (scheme != b->scheme) b->graph_dirty = b->adj_graphs_dirty = b->room_table_dirty = true;
+    if (scheme == ACF_SCHEME_PRESSURE_ONLY && !b->pressure_only()) {
+        b->po_first = true;      // the next step starts from the p-v state as it is now
+        b->po_started = false;
+    }
     b->scheme = scheme;
     return ACF_OK;
 }
@@ -4987,6 +5254,8 @@ int acf_read_recording(acf_solver *h, int64_t r, int64_t first_step, int64_t n, 
 int acf_upload(acf_solver *h, int field, const void *src, acf_stream stream) {
     int rc = check_field(h, 0, field);
     if (rc) return rc;
+    if (h->pressure_only() && h->po_started && field != ACF_FIELD_P)
+        return fail(ACF_ERR_STATE, "the pressure-only scheme keeps no velocities after its first step");
     if (!src) return fail(ACF_ERR_ARGUMENT, "null source");
     DeviceGuard guard(h->device);
     return copy_field(h, 0, field, const_cast<void *>(src), true, (cudaStream_t)stream);
@@ -4995,6 +5264,8 @@ int acf_upload(acf_solver *h, int field, const void *src, acf_stream stream) {
 int acf_download(acf_solver *h, int field, void *dst, acf_stream stream) {
     int rc = check_field(h, 0, field);
     if (rc) return rc;
+    if (h->pressure_only() && h->po_started && field != ACF_FIELD_P)
+        return fail(ACF_ERR_STATE, "the pressure-only scheme keeps no velocities after its first step");
     if (!dst) return fail(ACF_ERR_ARGUMENT, "null destination");
     DeviceGuard guard(h->device);
     return copy_field(h, 0, field, dst, false, (cudaStream_t)stream);
@@ -5011,11 +5282,46 @@ int acf_set_launch(acf_solver *h, int32_t block_threads, int32_t planes) {
 }
 
 int acf_energy_terms(acf_solver *h, double dx, double terms[7], acf_stream stream) {
+    if (h && h->pressure_only() && h->po_started)
+        return fail(ACF_ERR_STATE, "the pressure-only scheme keeps no velocities: use "
+                    "acf_pressure_only_energy_terms");
     return energy_terms(h, 0, dx, terms, stream);
+}
+
+int acf_pressure_only_energy_terms(acf_solver *h, double terms[2], acf_stream stream) {
+    if (!h || !terms) return fail(ACF_ERR_ARGUMENT, "null argument");
+    if (!h->pressure_only() || !h->po_started)
+        return fail(ACF_ERR_STATE, "no pressure-only step has been taken since the scheme was selected");
+    DeviceGuard guard(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double out[kEnergyTerms];
+    if (h->precision == 8) {
+        const Room<double> s = make_room<double>(h, 0);
+        pressure_only_energy_partials<double><<<h->energy_blocks, 256, 0, st>>>(
+            s, (const double *)h->field_ptr(0, ACF_FIELD_P), (const double *)h->other_ptr(0, ACF_FIELD_P),
+            h->energy_scratch);
+    } else {
+        const Room<float> s = make_room<float>(h, 0);
+        pressure_only_energy_partials<float><<<h->energy_blocks, 256, 0, st>>>(
+            s, (const float *)h->field_ptr(0, ACF_FIELD_P), (const float *)h->other_ptr(0, ACF_FIELD_P),
+            h->energy_scratch);
+    }
+    energy_finish<<<1, 32, 0, st>>>(h->energy_scratch, h->energy_blocks,
+                                    h->energy_scratch + (size_t)h->energy_blocks * kEnergyTerms);
+    h->launches += 2;
+    ACF_CUDA(cudaGetLastError());
+    ACF_CUDA(cudaMemcpyAsync(out, h->energy_scratch + (size_t)h->energy_blocks * kEnergyTerms,
+                             kEnergyTerms * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACF_CUDA(cudaStreamSynchronize(st));
+    terms[0] = out[0];
+    terms[1] = out[1];
+    return ACF_OK;
 }
 
 int acf_energy_terms_planes(acf_solver *h, double dx, int64_t x_begin, int64_t x_end,
                             int32_t far_face, double terms[7], acf_stream stream) {
+    if (h && h->pressure_only() && h->po_started)
+        return fail(ACF_ERR_STATE, "the pressure-only scheme keeps no velocities");
     return energy_terms(h, 0, dx, terms, stream, x_begin, x_end, far_face);
 }
 
@@ -5123,11 +5429,15 @@ int acf_reset_state(acf_solver *h, acf_stream stream) {
     // The primary copy becomes current. No captured graph goes stale: the run graphs are kept
     // per starting copy, and the adjoint's graphs always work on the primary copy.
     h->rooms[0].cur = 0;
+    h->po_first = true;
+    h->po_started = false;
     ACF_CUDA(cudaMemsetAsync(h->field_ptr(0, ACF_FIELD_P), 0, h->room_block_bytes(0), (cudaStream_t)stream));
     return ACF_OK;
 }
 
 int acf_adjoint_prepare(acf_solver *h, int32_t flags, int64_t max_steps, int32_t checkpoint_every) {
+    if (h && h->pressure_only())
+        return fail(ACF_ERR_STATE, "the adjoint transposes the p-v step; select another scheme");
     return adjoint_prepare(h, flags, max_steps, checkpoint_every);
 }
 
@@ -5137,6 +5447,8 @@ int32_t acf_adjoint_checkpoint_interval(const acf_solver *h) { return h ? h->adj
 
 int acf_forward_record(acf_solver *h, int64_t n_steps, int64_t step_offset, acf_stream stream) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (h->pressure_only())
+        return fail(ACF_ERR_STATE, "the adjoint transposes the p-v step; select another scheme");
     if (!h->adj.fields) return fail(ACF_ERR_STATE, "call acf_adjoint_prepare first");
     if (n_steps < 1 || n_steps > h->adj.capacity)
         return fail(ACF_ERR_ARGUMENT, "n_steps %lld outside 1..%lld prepared", (long long)n_steps,

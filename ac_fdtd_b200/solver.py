@@ -295,6 +295,8 @@ class CudaAcousticFDTD:
 
     def reset_state(self) -> None:
         """Put the room at rest: p, v and the relaxation states to zero, on the device."""
+        self._pressure_only_started = False
+        self._mirror_exposed -= {_native.FIELD_VX, _native.FIELD_VY, _native.FIELD_VZ}
         self._flush()
         _native.check(self._lib.acf_reset_state(self._handle, self._stream), "acf_reset_state")
         self._mirror_current.clear()
@@ -452,6 +454,9 @@ class CudaAcousticFDTD:
                       "acf_run")
         self.step_index += n_steps
         self._mirror_current.clear()
+        if self.scheme == "pressure_only":      # no velocities are kept from here on
+            self._mirror_exposed -= {_native.FIELD_VX, _native.FIELD_VY, _native.FIELD_VZ}
+            self._pressure_only_started = True
 
     def step(self) -> None:
         self.run(1)
@@ -523,7 +528,23 @@ class CudaAcousticFDTD:
 
         The sums are accumulated in FP64 on the device in either precision.
         """
+        if self.scheme == "pressure_only" and getattr(self, "_pressure_only_started", False):
+            return self.pressure_only_energy()
         return energy_from_terms(self.energy_terms(), self.medium, float(self.grid.dx), self.dt)
+
+    def pressure_only_energy(self) -> float:
+        """The pressure-only scheme's conserved energy after its latest step, in joules:
+        dx^3 / (2 rho c^2) (sum (p^{n+1} - p^n)^2 / lam2 - sum p^{n+1} L p^n), lam2 = c_p c_v
+        and L the rigid-face Laplacian (``acf_pressure_only_energy_terms``). Constant with rigid
+        walls, non-increasing with impedance walls and no sources."""
+        self._flush()
+        terms = np.zeros(2)
+        _native.check(self._lib.acf_pressure_only_energy_terms(
+            self._handle, _as_double_pointer(terms), self._stream), "acf_pressure_only_energy_terms")
+        block = self.coefficients
+        lam2 = float(np.dtype(self.dtype).type(block.vel_coef * block.pres_coef))
+        rho, c = float(self.medium.density), float(self.medium.sound_speed)
+        return float(self.grid.dx) ** 3 / (2.0 * rho * c**2) * (terms[0] / lam2 - terms[1])
 
     def set_coefficients(self, walls=None, absorbing_layer=None, air_absorption=None) -> None:
         """Replace the wall, layer and air coefficients, keeping the grid and the state.
@@ -541,18 +562,30 @@ class CudaAcousticFDTD:
         self.coefficients = block
 
     SCHEMES = {"two_sweeps": _native.SCHEME_TWO_SWEEPS, "fused": _native.SCHEME_FUSED,
-               "staged": _native.SCHEME_FUSED_STAGED}
+               "staged": _native.SCHEME_FUSED_STAGED,
+               "pressure_only": _native.SCHEME_PRESSURE_ONLY}
 
     def set_scheme(self, scheme: str) -> None:
         """``"two_sweeps"`` (velocity sweep, then pressure sweep, in place), ``"fused"`` (one
         sweep into a second copy of p and v) or ``"staged"`` (the fused sweep with its inputs
         streamed into shared memory by bulk copies). Results are bit-identical; the fused steps
         move (8 + 2R) elements per cell instead of (12 + 2R) and need four more fields of
-        memory."""
+        memory. ``"pressure_only"``: the second-order wave equation on p alone (rigid or
+        impedance walls, no absorbing layer or air absorption), 3 elements per cell and step;
+        its first step is the p-v step from the state as it stands, so pressures and recordings
+        equal the other schemes' to rounding, and from then on no velocities are kept
+        (``velocity`` raises; ``energy`` is the scheme's own conserved quadratic form)."""
         if scheme not in self.SCHEMES:
             raise ValueError(f"scheme must be one of {sorted(self.SCHEMES)}, got {scheme!r}")
+        if scheme == "pressure_only" and (self.coefficients.layer_cell is not None
+                                          or self.n_relax > 0):
+            raise ValueError("the pressure-only scheme has no absorbing layer or air absorption: "
+                             "the second-order pressure equation keeps no velocity or relaxation "
+                             "state for them")
         self._flush()
         _native.check(self._lib.acf_set_scheme(self._handle, self.SCHEMES[scheme]), "acf_set_scheme")
+        if scheme == "pressure_only" and getattr(self, "scheme", None) != "pressure_only":
+            self._pressure_only_started = False
         self.scheme = scheme
         self._mirror_current.clear()
 

@@ -466,6 +466,7 @@ def run_ours(args) -> None:
     inversion = None if args.skip_extras else batched_adjoint_cost(args)
     precision = None if args.skip_extras else precision_check(args)
     slabs = None if args.skip_extras else slab_overhead(args)
+    pressure_only = None if args.skip_extras else pressure_only_cost(args)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -488,6 +489,7 @@ def run_ours(args) -> None:
         "batched_inversion": inversion,
         "precision": precision,
         "slabs_one_gpu": slabs,
+        "pressure_only": pressure_only,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -532,6 +534,9 @@ def extras_summary(line: dict) -> dict:
         "torch_cuda_gcups_384": get("comparators", "gpu", "room_384_fp32", "gcups"),
         "c_fp64_gcups_384": get("comparators", "cpu", "c_fp64_room_384", "gcups"),
         "numpy_gcups_64": get("comparators", "cpu", "numpy_fp64_room_64", "gcups"),
+        "pressure_only_gcups": get("pressure_only", "pressure_only", "gcups"),
+        "pressure_only_frac": get("pressure_only", "pressure_only", "hbm_frac_of_measured"),
+        "pressure_only_speedup": get("pressure_only", "speedup_over_fused"),
     }
 
 
@@ -706,6 +711,61 @@ def comparators(args) -> dict:
         cpu["numpy_fp64_room_64"] = {"gcups": grid1.n_cells * T1 / elapsed / 1e9, "threads": 1,
                                      "sample": f"{T1} steps in full, {elapsed:.1f} s"}
     out["cpu"] = cpu
+    return out
+
+
+def pressure_only_cost(args) -> dict:
+    """The pressure-only scheme against the p-v leapfrog on the headline room without its sponge
+    and air (neither exists in the second-order pressure equation): 384^3 fp32, the six walls,
+    the source and four receivers, 1000 steps each from rest. Kernel time from CUDA events
+    around every launch (one kernel per step in both schemes), run time from events around the
+    run; receivers compared between the schemes."""
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse
+    from ac_fdtd_b200.autotune import apply_tuned
+
+    grid, objects, points = workload(args.size)
+    walls = objects["walls"]
+    T = 1000
+    peak, peak_kind = measured_peak_hbm()
+    out = {"workload": f"{args.size}^3 fp32, the headline room's walls, no sponge, no air, "
+                       f"{len(points) - 1} receivers, {T} steps from rest"}
+    recordings = {}
+    for scheme, bytes_per_cell in (("fused", 32), ("pressure_only", 12)):
+        solver = CudaAcousticFDTD(grid, dtype=np.float32, walls=walls, scheme=scheme)
+        launch = launch_dict(apply_tuned(solver, schemes=(scheme,)))
+        solver.add_volume_source(points[0], gaussian_pulse(T, solver.dt, 4000.0))
+        for point in points[1:]:
+            solver.add_pressure_receiver(point)
+
+        def run(solver=solver):
+            solver.reset_state()
+            solver.step_index = 0
+            solver.run(T)
+
+        run()
+        run_ms = min(_device_ms(run, torch) for _ in range(2))
+        solver.reset_state()
+        solver.step_index = 0
+        solver.profile(True)
+        solver.run(200)
+        first_ms, second_ms, launches = solver.profile_read()
+        solver.profile(False)
+        kernel_ms = (first_ms + second_ms) / max(launches, 1)
+        recordings[scheme] = solver.recorded_pressure
+        solver.close()
+        achieved = grid.n_cells * bytes_per_cell / (kernel_ms * 1e-3) / 1e9
+        out[scheme] = {
+            "gcups": grid.n_cells * T / (run_ms * 1e-3) / 1e9, "bytes_per_cell": bytes_per_cell,
+            "avg_launch_ms": kernel_ms, "achieved_GBps": achieved,
+            f"hbm_frac_of_{peak_kind}": achieved / peak,
+            "kernel": "lean_sweep<false,walls,0>" if scheme == "fused" else "pressure_only_sweep<float,walls>",
+            "launch": launch,
+        }
+    rec = recordings["pressure_only"]
+    out["speedup_over_fused"] = out["pressure_only"]["gcups"] / out["fused"]["gcups"]
+    out["receivers_vs_fused_fp32"] = _errors(rec, recordings["fused"])
     return out
 
 

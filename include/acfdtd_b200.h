@@ -138,6 +138,14 @@ int acf_download(acf_solver *solver, int field, void *dst, acf_stream stream);
  * source samples (src/ac_fdtd/c/acfdtd.c:358-371). Asynchronous on `stream`. */
 int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream stream);
 
+/* The two FP64 sums of the pressure-only scheme's conserved energy after its latest step, with
+ * u = p^{n+1} and w = p^n: terms[0] = sum (u - w)^2, terms[1] = sum u L w. The energy
+ * E = dx^3 / (2 rho c^2) (terms[0] / lam2 - terms[1]) is constant for rigid walls and does not
+ * grow with impedance walls (it drops by dx^3/(2 rho c^2) sum a (p^{n+1} - p^{n-1})^2 / lam2 per
+ * step); it is the scheme's own quadratic form, not the p-v energy of acf_energy_terms.
+ * ACF_ERR_STATE before the scheme's first step. No counterpart in the reference. */
+int acf_pressure_only_energy_terms(acf_solver *solver, double terms[2], acf_stream stream);
+
 /* How a single room advances: two sweeps per step over one copy of the state, or one fused
  * sweep that reads the current p and v and writes the next ones to a second copy (4 more
  * fields of memory, (8 + 2R) instead of (12 + 2R) elements moved per cell). Both give
@@ -145,7 +153,20 @@ int acf_run(acf_solver *solver, int64_t n_steps, int64_t step_offset, acf_stream
  * ACF_SCHEME_FUSED_STAGED is the fused sweep with each CTA's share of every x plane streamed
  * into a shared-memory ring by bulk copies (see acf_set_staging); same memory, same results.
  * No counterpart in the reference (its C loop runs the two sweeps, acfdtd.c:355-376). */
-enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1, ACF_SCHEME_FUSED_STAGED = 2 };
+enum { ACF_SCHEME_TWO_SWEEPS = 0, ACF_SCHEME_FUSED = 1, ACF_SCHEME_FUSED_STAGED = 2,
+       ACF_SCHEME_PRESSURE_ONLY = 3 };
+
+/* ACF_SCHEME_PRESSURE_ONLY: the second-order wave equation on p alone, for a single room with
+ * rigid or impedance walls and no absorbing layer or air absorption (ACF_ERR_STATE otherwise).
+ * The reference plans it (its milestone M8, PLAN.md:52-56) and has not built it. With the
+ * velocities eliminated, p^{n+1} = fu (2 p^n + lam2 L p^n) - (fu - fp) p^{n-1} - S^{n-1} + S^n
+ * (L the rigid-face Laplacian, lam2 = c_p c_v, (fu, fp) the wall pair, S^n the source added
+ * after step n): 3 elements moved per cell and step instead of 8 + 2R. The first step after
+ * selecting it is the p-v step from the state as it stands (p^n, v^{n-1/2}), so the pressures
+ * and recordings equal the p-v scheme's to rounding. From then on the velocities are not kept:
+ * acf_download/acf_upload of vx, vy, vz and acf_energy_terms return ACF_ERR_STATE (use
+ * acf_pressure_only_energy_terms), as does switching to another scheme before
+ * acf_reset_state. Uploading p replaces p^n and keeps p^{n-1}. */
 int acf_set_scheme(acf_solver *solver, int32_t scheme);
 int acf_get_scheme(const acf_solver *solver);
 
