@@ -5062,8 +5062,23 @@ __global__ void __launch_bounds__(kPostThreads) schroeder_decay_kernel(const dou
         const double x = h[n - 1 - q];
         mine += x * x;
     }
-    double total;
-    double running = block_exclusive_scan(mine, shared, &total);   // the later runs in time
+    double sum_all;
+    const double start = block_exclusive_scan(mine, shared, &sum_all);   // the later runs in time
+    // The curve is normalised by I(0) itself, as the reference divides by its first entry: the
+    // thread holding sample 0 forms it with the same additions as its pass below, so the first
+    // level is exactly 0 dB.
+    __shared__ double first;
+    if (q0 < n && q1 == n) {
+        double running = start;
+        for (int64_t q = q0; q < q1; q++) {
+            const double x = h[n - 1 - q];
+            running += x * x;
+        }
+        first = running;
+    }
+    __syncthreads();
+    const double total = first;
+    double running = start;
     for (int64_t q = q0; q < q1; q++) {
         const double x = h[n - 1 - q];
         running += x * x;
