@@ -1445,7 +1445,11 @@ struct LeanParams {
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
-template <bool LAYER, bool WALLS, int NR>
+// ALIGNED: nz is a multiple of 4. Otherwise the last chunk of every row holds padding elements
+// (k >= nz), which this column leaves as they are, and the top face k = nz, which it damps
+// without a gradient update -- exactly as fused_column does -- with per-thread fix-ups that only
+// the threads of those chunks take.
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED = true>
 __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, int i_end, int j, int c,
                                             int64_t step) {
     const FusedParams<float> &f = g.f;
@@ -1454,6 +1458,9 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
     const int64_t column = (int64_t)j * s.pz + k0;
     const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
     const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+    // Padding chunk: `real` elements (1..3) lie inside the room, the next one is the top face.
+    const bool tail = !ALIGNED && k0 + kVec > s.nz;
+    const int real = tail ? s.nz - k0 : kVec;
     const bool any_point = (s.n_src | s.n_rec) != 0;
     bool all_points = false;
     const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
@@ -1469,11 +1476,15 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         fj_cell = __ldg(s.cell[1] + j);
         fj_face = __ldg(s.face[1] + j);
         fj1_face = __ldg(s.face[1] + j + 1);
-        fkc01 = make_float2(__ldg(s.cell[2] + k0), __ldg(s.cell[2] + k0 + 1));
-        fkc23 = make_float2(__ldg(s.cell[2] + k0 + 2), __ldg(s.cell[2] + k0 + 3));
-        fkf01 = make_float2(__ldg(s.face[2] + k0), __ldg(s.face[2] + k0 + 1));
-        fkf23 = make_float2(__ldg(s.face[2] + k0 + 2), __ldg(s.face[2] + k0 + 3));
-        fkf4 = __ldg(s.face[2] + k0 + 4);
+        // padding lanes take the last cell's and the top face's factors, as fused_column does
+        const int c_last = s.nz - 1, f_last = s.nz;
+        auto kc = [&](int e) { return __ldg(s.cell[2] + (ALIGNED ? k0 + e : min(k0 + e, c_last))); };
+        auto kf = [&](int e) { return __ldg(s.face[2] + (ALIGNED ? k0 + e : min(k0 + e, f_last))); };
+        fkc01 = make_float2(kc(0), kc(1));
+        fkc23 = make_float2(kc(2), kc(3));
+        fkf01 = make_float2(kf(0), kf(1));
+        fkf23 = make_float2(kf(2), kf(3));
+        fkf4 = kf(4);
         damp_y = fj_cell != 1.f || fj_face != 1.f || fj1_face != 1.f;
         damp_z = fkc01.x != 1.f || fkc01.y != 1.f || fkc23.x != 1.f || fkc23.y != 1.f ||
                  fkf01.x != 1.f || fkf01.y != 1.f || fkf23.x != 1.f || fkf23.y != 1.f || fkf4 != 1.f;
@@ -1534,7 +1545,8 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         const float4 VZ = __ldg(reinterpret_cast<const float4 *>(s.vz + base));
         const float p_below = z_lo ? __ldg(s.p + base - 1) : 0.f;
         const float p_above = z_hi ? __ldg(s.p + base + kVec) : 0.f;
-        const float vz_above = __ldg(s.vz + base + kVec);   // face k0 + 4 <= nz: inside the row
+        // face k0 + 4: inside the row when k0 + 4 <= nz (always when ALIGNED)
+        const float vz_above = (ALIGNED || !tail) ? __ldg(s.vz + base + kVec) : 0.f;
         float4 S[NR > 0 ? NR : 1];
 #pragma unroll
         for (int r = 0; r < NR; r++) S[r] = *reinterpret_cast<const float4 *>(s.psi + r * s.field + base);
@@ -1564,6 +1576,11 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         float2 ZL01 = sub2(lo2(VZ), mul2(cv2, sub2(P01, make_float2(p_below, P.x))));
         float2 ZL23 = sub2(hi2(VZ), mul2(cv2, sub2(P23, make_float2(P.y, P.z))));
         if (!z_lo) ZL01.x = VZ.x;                 // face k = 0: a boundary, never updated
+        if (tail) {                               // faces k >= nz: the top face and padding
+            if (real <= 1) ZL01.y = VZ.y;
+            if (real <= 2) ZL23.x = VZ.z;
+            ZL23.y = VZ.w;
+        }
         float ZH3 = vz_above;
         if (z_hi) ZH3 = ZH3 - cv * (p_above - P.w);
         if (LAYER) {   // x, y, z order; an axis whose factors here are all 1 is skipped
@@ -1608,7 +1625,13 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
             const float2 n23 = sub2(t23, mul2(o23, g.pairs[kPairNegDecay + r]));
             pe01 = sub2(pe01, mul2(o01, g.pairs[kPairNegMean + r]));
             pe23 = sub2(pe23, mul2(o23, g.pairs[kPairNegMean + r]));
-            S[r] = make_float4(n01.x, n01.y, n23.x, n23.y);
+            float4 next = make_float4(n01.x, n01.y, n23.x, n23.y);
+            if (tail) {                           // padding lanes keep their state
+                if (real <= 1) next.y = S[r].y;
+                if (real <= 2) next.z = S[r].z;
+                next.w = S[r].w;
+            }
+            S[r] = next;
         }
         if (NR > 0) {
             pe01 = sub2(pe01, mul2(d01, g.pairs[kPairNegRelaxScale]));
@@ -1625,7 +1648,8 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
 #pragma unroll
             for (int e = 0; e < kVec; e++) {
                 float fu, fp;
-                if (wall_pair(s, i, j, k0 + e, fu, fp)) Pn[e] = Pn[e] * fu - Po[e] * fp;
+                if ((ALIGNED || e < real) && wall_pair(s, i, j, k0 + e, fu, fp))
+                    Pn[e] = Pn[e] * fu - Po[e] * fp;
             }
         }
         if (LAYER) {
@@ -1644,18 +1668,29 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
                 Pn[3] = Pn[3] * fkc23.y;
             }
         }
+        if (tail) {                               // padding lanes keep p
+            if (real <= 1) Pn[1] = P.y;
+            if (real <= 2) Pn[2] = P.z;
+            Pn[3] = P.w;
+        }
         if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
 
         // ---- stores: p, the three lower faces, the far boundary faces, psi in place
         *reinterpret_cast<float4 *>(f.np + base) = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
         *reinterpret_cast<float4 *>(f.nvx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
         *reinterpret_cast<float4 *>(f.nvy + base) = make_float4(YL01.x, YL01.y, YL23.x, YL23.y);
-        *reinterpret_cast<float4 *>(f.nvz + base) = make_float4(ZL01.x, ZL01.y, ZL23.x, ZL23.y);
+        float4 ZS = make_float4(ZL01.x, ZL01.y, ZL23.x, ZL23.y);
+        if (tail) {                               // faces past the top one are padding
+            if (real <= 0) ZS.y = VZ.y;           // (never: real >= 1)
+            if (real <= 1) ZS.z = VZ.z;
+            if (real <= 2) ZS.w = VZ.w;
+        }
+        *reinterpret_cast<float4 *>(f.nvz + base) = ZS;
         if (!x_inner)
             *reinterpret_cast<float4 *>(f.nvx + base + s.plane) = make_float4(XH01.x, XH01.y, XH23.x, XH23.y);
         if (!y_hi)
             *reinterpret_cast<float4 *>(f.nvy + base + s.pz) = make_float4(YH01.x, YH01.y, YH23.x, YH23.y);
-        if (!z_hi) f.nvz[base + kVec] = ZH3;
+        if (!z_hi && (ALIGNED || !tail)) f.nvz[base + kVec] = ZH3;
 #pragma unroll
         for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(s.psi + r * s.field + base) = S[r];
         if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
@@ -1666,15 +1701,69 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
     report_nonfinite(s.status, bad2.x != bad2.x || bad2.y != bad2.y);
 }
 
-template <bool LAYER, bool WALLS, int NR>
-__global__ void __launch_bounds__(256, ACF_FUSED_MIN_BLOCKS(float, LAYER, NR)) lean_sweep(const LeanParams g) {
+// Resident blocks of 256 threads: 80 registers (3 blocks) unless there is neither a layer nor a
+// relaxation state (64 registers, 4 blocks); below 80 the relaxation states spill.
+#ifndef ACF_LEAN_MIN_BLOCKS
+#define ACF_LEAN_MIN_BLOCKS(LAYER, NR) ((LAYER) || (NR) > 0 ? 3 : 4)
+#endif
+
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED>
+__device__ __forceinline__ void lean_sweep_body(const LeanParams &g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (c >= g.f.room.nchunks || j >= g.f.room.ny) return;
     const bool any_point = (g.f.room.n_src | g.f.room.n_rec) != 0;
     const int64_t step = any_point ? (*g.f.step_base + g.f.local_step) : 0;
     const int i_begin = blockIdx.z * g.f.planes;
-    lean_column<LAYER, WALLS, NR>(g, i_begin, min(g.f.room.nx, i_begin + g.f.planes), j, c, step);
+    lean_column<LAYER, WALLS, NR, ALIGNED>(g, i_begin, min(g.f.room.nx, i_begin + g.f.planes), j, c, step);
+}
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR)) lean_sweep(const LeanParams g) {
+    lean_sweep_body<LAYER, WALLS, NR, true>(g);
+}
+
+// Rows with padding: the fix-ups keep a few more values live, so 96 registers (fewer spills).
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __maxnreg__(96) lean_sweep_padded(const LeanParams g) {
+    lean_sweep_body<LAYER, WALLS, NR, false>(g);
+}
+
+// The lean fused step over a batch's tile table (fused_batch's schedule), every room's
+// description (with its packed coefficients) staged in shared memory by the CTA.
+struct LeanBatchParams {
+    const LeanParams *rooms;        // one per room, for the current parity
+    const Tile *tiles;
+    int32_t n_tiles;
+    int32_t local_step;
+    const int64_t *step_base;
+};
+
+// 128 registers: at 96 the batch loop's context spills 30-150 bytes per thread.
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __maxnreg__(128) lean_batch(const LeanBatchParams b) {
+    __shared__ __align__(16) unsigned char raw[sizeof(LeanParams)];
+    LeanParams *room = reinterpret_cast<LeanParams *>(raw);
+    static_assert(sizeof(LeanParams) % sizeof(int) == 0, "LeanParams must be a whole number of words");
+    const int64_t step = *b.step_base + b.local_step;
+    int staged = -1;
+    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
+        const Tile tile = b.tiles[t];
+        if (tile.room != staged) {
+            __syncthreads();
+            const int *from = reinterpret_cast<const int *>(b.rooms + tile.room);
+            int *to = reinterpret_cast<int *>(raw);
+            for (int w = threadIdx.x; w < (int)(sizeof(LeanParams) / sizeof(int)); w += blockDim.x)
+                to[w] = __ldg(from + w);
+            __syncthreads();
+            staged = tile.room;
+        }
+        if ((int)threadIdx.x < tile.count) {
+            const int pair = tile.first + threadIdx.x;
+            lean_column<LAYER, WALLS, NR, false>(*room, tile.i_begin, tile.i_end, pair / room->f.room.nchunks,
+                                                 pair % room->f.room.nchunks, step);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1716,7 +1805,7 @@ __device__ __forceinline__ T fma_t(T a, T b, T c) {
 }
 
 template <typename T, bool WALLS, bool FIRST>
-__device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T> &g, int i_begin,
+__device__ __forceinline__ void pressure_only_column_simple(const PressureOnlyParams<T> &g, int i_begin,
                                                      int i_end, int j, int c, int64_t step) {
     const Room<T> &s = g.room;
     const int k0 = c * kVec;
@@ -1830,6 +1919,116 @@ __device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T>
     report_nonfinite(s.status, bad != bad);
 }
 
+
+// The same update with each plane's inputs loaded one plane ahead (into registers, while the
+// current plane computes), so a thread keeps two planes of loads in flight: the steady-state
+// step (not the first one, which also reads the velocities).
+template <typename T, bool WALLS>
+struct PoInputs {
+    T Pp[kVec], Ym[kVec], Yp[kVec], Q[kVec];
+    T zb, za;
+};
+
+template <typename T, bool WALLS>
+__device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T> &g, int i_begin,
+                                                     int i_end, int j, int c, int64_t step) {
+    const Room<T> &s = g.room;
+    const T *__restrict__ cur = g.cur;
+    T *__restrict__ nxt = g.next;
+    const int k0 = c * kVec;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
+    const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+    const bool wall_column = !y_lo || !y_hi || !z_lo || k0 + kVec >= s.nz;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    bool all_points = false;
+    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const T lam2 = g.lam2;
+    T bad = T(0);
+
+    // Inputs of plane i: p of plane i + 1 (own row), rows j -+ 1 and the row's z neighbours
+    // at plane i, p^{n-1} at plane i. Missing neighbours are replaced by p when used.
+    auto load = [&](int i, PoInputs<T, WALLS> &in) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        if (i + 1 < s.nx) Vec4<T>::ldg(cur + base + s.plane, in.Pp);
+        if (y_lo) Vec4<T>::ldg(cur + base - s.pz, in.Ym);
+        if (y_hi) Vec4<T>::ldg(cur + base + s.pz, in.Yp);
+        in.zb = z_lo ? __ldg(cur + base - 1) : T(0);
+        in.za = z_hi ? __ldg(cur + base + kVec) : T(0);
+        Vec4<T>::load(nxt + base, in.Q);
+    };
+
+    T Pm[kVec] = {T(0), T(0), T(0), T(0)}, P[kVec];
+    Vec4<T>::ldg(cur + (int64_t)i_begin * s.plane + column, P);
+    if (i_begin > 0) Vec4<T>::ldg(cur + (int64_t)(i_begin - 1) * s.plane + column, Pm);
+    PoInputs<T, WALLS> in;
+    load(i_begin, in);
+
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        PoInputs<T, WALLS> ahead;
+        if (i + 1 < i_end) {
+            if (s.prefetch && i + 2 < i_end) {   // two planes ahead into L2
+                if (i + 3 < s.nx) prefetch_l2(cur + base + 3 * s.plane);
+                prefetch_l2(nxt + base + 2 * s.plane);
+            }
+            load(i + 1, ahead);
+        }
+        const bool x_lo = i > 0, x_hi = i + 1 < s.nx;
+        const bool wall_plane = WALLS && (wall_column || !x_lo || !x_hi);
+        T Pn[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            const int k = k0 + e;
+            const T p = P[e];
+            if (k >= s.nz) {          // padding
+                Pn[e] = p;
+                continue;
+            }
+            const T xm = x_lo ? Pm[e] : p, xp = x_hi ? in.Pp[e] : p;
+            const T ym = y_lo ? in.Ym[e] : p, yp = y_hi ? in.Yp[e] : p;
+            const T zm = e == 0 ? (z_lo ? in.zb : p) : P[e - 1];
+            const T zp = k + 1 < s.nz ? (e + 1 < kVec ? P[e + 1] : in.za) : p;
+            const T lap = ((xm - p) + (xp - p)) + ((ym - p) + (yp - p)) + ((zm - p) + (zp - p));
+            const T q = fma_t(lam2, lap, p + p);
+            T fu = T(1), fp = T(0);
+            if (wall_plane && wall_pair(s, i, j, k, fu, fp)) Pn[e] = fu * q - (fu - fp) * in.Q[e];
+            else Pn[e] = q - in.Q[e];
+        }
+        if (any_mine) {
+            // - S^{n-1} (added by the previous step), then + S^n, in the order added
+            uint32_t m = all_points ? 0u : source_bits(points, s.n_src);
+            for (int q = all_points ? 0 : -1; all_points ? q < s.n_src : m != 0; q++) {
+                if (!all_points) {
+                    q = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.src_off[q] - base;
+                if (d < 0 || d >= kVec || k0 + d >= s.nz) continue;
+#pragma unroll
+                for (int e = 0; e < kVec; e++) {
+                    if (e != d) continue;
+                    if (step >= 1 && step - 1 < s.src_len[q])
+                        Pn[e] = Pn[e] - s.cs * s.src_sig[q * s.src_stride + step - 1];
+                    if (step < s.src_len[q]) Pn[e] = Pn[e] + s.cs * s.src_sig[q * s.src_stride + step];
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < kVec; e++) bad = finite_acc(bad, Pn[e]);
+        Vec4<T>::store(nxt + base, Pn);
+        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            Pm[e] = P[e];
+            P[e] = in.Pp[e];
+        }
+        in = ahead;
+    }
+    report_nonfinite(s.status, bad != bad);
+}
+
 template <typename T, bool WALLS, bool FIRST>
 __global__ void __launch_bounds__(256) pressure_only_sweep(const PressureOnlyParams<T> g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1838,7 +2037,10 @@ __global__ void __launch_bounds__(256) pressure_only_sweep(const PressureOnlyPar
     const bool any_point = (g.room.n_src | g.room.n_rec) != 0;
     const int64_t step = any_point ? (*g.step_base + g.local_step) : 0;
     const int i_begin = blockIdx.z * g.planes;
-    pressure_only_column<T, WALLS, FIRST>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
+    if constexpr (FIRST)
+        pressure_only_column_simple<T, WALLS, true>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
+    else
+        pressure_only_column<T, WALLS>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
 }
 
 // The two sums of the pressure-only scheme's conserved energy after a step, with cur = p^{n+1}
@@ -2870,6 +3072,7 @@ struct acf_batch {
     size_t state_bytes = 0;
     void *room_table = nullptr;      // device array of Room<T>, one per room
     void *fused_table = nullptr;     // fused scheme on a batch: 2 x rooms FusedParams<T>, by parity
+    void *lean_table = nullptr;      // the same in single precision: 2 x rooms LeanParams
     bool room_table_dirty = true;
     Tile *tiles = nullptr;
     int32_t n_tiles = 0;
@@ -3066,6 +3269,8 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     return s;
 }
 
+void fill_pairs(float2 *pairs, const RoomHost &h);
+
 template <typename T>
 int upload_room_table(acf_batch *b) {
     std::vector<Room<T>> table(b->rooms.size());
@@ -3093,6 +3298,17 @@ int upload_room_table(acf_batch *b) {
         if (!b->fused_table) ACF_CUDA(cudaMalloc(&b->fused_table, fused.size() * sizeof(FusedParams<T>)));
         ACF_CUDA(cudaMemcpy(b->fused_table, fused.data(), fused.size() * sizeof(FusedParams<T>),
                             cudaMemcpyHostToDevice));
+        if constexpr (sizeof(T) == 4) {
+            std::vector<LeanParams> lean(fused.size());
+            for (size_t q = 0; q < fused.size(); q++) {
+                lean[q] = LeanParams{};
+                lean[q].f = fused[q];
+                fill_pairs(lean[q].pairs, b->rooms[q % n]);
+            }
+            if (!b->lean_table) ACF_CUDA(cudaMalloc(&b->lean_table, lean.size() * sizeof(LeanParams)));
+            ACF_CUDA(cudaMemcpy(b->lean_table, lean.data(), lean.size() * sizeof(LeanParams),
+                                cudaMemcpyHostToDevice));
+        }
     }
     b->room_table_dirty = false;
     return ACF_OK;
@@ -3194,6 +3410,20 @@ struct LeanStep {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct LeanStepPadded {
+    static void launch(const LeanParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_sweep_padded<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
+struct LeanBatch {
+    static void launch(const LeanBatchParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_batch<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
 // The packed coefficients of the single-precision kernels: each rounded to float once, the
 // negated slots negated after that rounding, so each is exactly minus the scalar's value.
 void fill_pairs(float2 *pairs, const RoomHost &h) {
@@ -3282,14 +3512,24 @@ template <typename T>
 void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
     if (events) cudaEventRecord(events[0], st);
     if (b->rooms.size() > 1 && b->fused()) {
-        FusedBatchParams<T> p{};
-        p.rooms = (const FusedParams<T> *)b->fused_table + (b->rooms[0].cur ? b->rooms.size() : 0);
-        p.tiles = b->tiles;
-        p.n_tiles = b->n_tiles;
-        p.local_step = local;
-        p.step_base = b->step_base;
         const dim3 grid(b->batch_ctas), block(b->block_threads);
-        dispatch_pressure<T, BatchFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        if constexpr (sizeof(T) == 4) {   // the lean single-precision column
+            LeanBatchParams p{};
+            p.rooms = (const LeanParams *)b->lean_table + (b->rooms[0].cur ? b->rooms.size() : 0);
+            p.tiles = b->tiles;
+            p.n_tiles = b->n_tiles;
+            p.local_step = local;
+            p.step_base = b->step_base;
+            dispatch_pressure<float, LeanBatch>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        } else {
+            FusedBatchParams<T> p{};
+            p.rooms = (const FusedParams<T> *)b->fused_table + (b->rooms[0].cur ? b->rooms.size() : 0);
+            p.tiles = b->tiles;
+            p.n_tiles = b->n_tiles;
+            p.local_step = local;
+            p.step_base = b->step_base;
+            dispatch_pressure<T, BatchFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
+        }
         for (RoomHost &h : b->rooms) h.cur ^= 1;
         if (events) {
             cudaEventRecord(events[1], st);
@@ -3358,19 +3598,18 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
             dispatch_pressure<T, StagedStep>(h.has_layer, h.has_walls, h.n_relax, g, grid, block, st);
         } else {
             const LaunchShape L = single_shape(b);
-            bool lean = false;
-            if constexpr (sizeof(T) == 4) {
-                if (h.nz % kVec == 0) {   // the lean single-precision column (no padding lanes)
-                    LeanParams g{};
-                    g.f = f;
-                    fill_pairs(g.pairs, h);
-                    dispatch_pressure<float, LeanStep>(h.has_layer, h.has_walls, h.n_relax, g, L.grid,
-                                                       L.block, st);
-                    lean = true;
-                }
-            }
-            if (!lean)
+            if constexpr (sizeof(T) == 4) {   // the lean single-precision column
+                LeanParams g{};
+                g.f = f;
+                fill_pairs(g.pairs, h);
+                if (h.nz % kVec == 0)
+                    dispatch_pressure<float, LeanStep>(h.has_layer, h.has_walls, h.n_relax, g, L.grid, L.block, st);
+                else
+                    dispatch_pressure<float, LeanStepPadded>(h.has_layer, h.has_walls, h.n_relax, g, L.grid,
+                                                             L.block, st);
+            } else {
                 dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f, L.grid, L.block, st);
+            }
         }
         h.cur ^= 1;
         if (events) {
@@ -3618,6 +3857,7 @@ void free_batch(acf_batch *b) {
     cudaFree(b->state);
     cudaFree(b->room_table);
     cudaFree(b->fused_table);
+    cudaFree(b->lean_table);
     cudaFree(b->tiles);
     cudaFree(b->step_base);
     cudaFree(b->energy_scratch);

@@ -156,7 +156,8 @@ class ImpulseResponse:
     def decay_metrics(self, device: bool = True) -> dict:
         """T20, T30, EDT (seconds), C50 and C80 (dB) of every receiver's response, computed in
         FP64 on the GPU (``ac_fdtd_b200.postprocess``) or, with ``device=False``, on the host
-        in the reference's arithmetic. A response too short for a fit gives NaN there."""
+        in the reference's arithmetic. A response too short for a fit, or for a clarity split,
+        gives NaN there (the reference's functions raise for it)."""
         if device:
             from . import postprocess as where
         else:
@@ -172,7 +173,11 @@ class ImpulseResponse:
                 except ValueError:
                     values.append(float("nan"))
             out[name] = np.array(values)
+        n = self.signals.shape[-1]
         for name, split in (("c50", 0.05), ("c80", 0.08)):
+            if not 0 < int(round(split * self.sample_rate)) < n:   # no early or no late part
+                out[name] = np.full(len(self.signals), np.nan)
+                continue
             out[name] = np.array([float(where.clarity(signal, self.sample_rate, split))
                                   for signal in self.signals])
         return out

@@ -344,8 +344,9 @@ def test_an_explicit_device_gives_the_same_results():
 
 @pytest.mark.parametrize("faces", [None, ((0, 0), (0, 1)), ((1, 1), (2, 0))])
 def test_lean_single_precision_fused_column_matches_the_oracle(faces):
-    """Single precision with nz a multiple of 4 runs the fused step through the lean column
-    (packed arithmetic, damping skipped where the profile is exactly 1). Grids with one chunk,
+    """Single precision runs the fused step through the lean column (packed arithmetic, damping
+    skipped where the profile is exactly 1; rows of a multiple of 4 cells without padding
+    lanes, others with fix-ups in their last chunk). Grids with one chunk,
     one row, one plane, sponges on every face or on some only (so rows, chunks and planes
     with and without damping meet in one warp), walls, air, points on the edges: the
     oracle's float32 bits, with the L2 prefetch off and on."""
@@ -355,7 +356,8 @@ def test_lean_single_precision_fused_column_matches_the_oracle(faces):
     configuration = dict(walls=WallAdmittances(0.4, 0.1, 0.0, 0.7, 0.2, 0.05),
                          absorbing_layer=layer, air_absorption=AirAbsorption())
     for shape in ((13, 11, 24), (1, 1, 4), (6, 1, 8), (2, 9, 4), (9, 10, 40), (5, 3, 12),
-                  (4, 37, 132)):
+                  (4, 37, 132), (13, 11, 23), (6, 1, 5), (2, 9, 1), (1, 1, 2), (5, 3, 7),
+                  (4, 37, 133), (7, 6, 6)):
         grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
         initial = np.random.default_rng(sum(shape)).standard_normal(shape).astype(np.float32)
         corner = tuple((n - 0.5) * 0.02 for n in shape)

@@ -36,10 +36,10 @@ WALLS = {
 }
 
 
-def close_to_peak(got, want, tol):
+def close_to_peak(got, want, tol, scale=None):
     got = np.asarray(got, dtype=np.float64)
     want = np.asarray(want, dtype=np.float64)
-    peak = np.max(np.abs(want))
+    peak = np.max(np.abs(want)) if scale is None else scale
     assert peak > 0
     err = np.max(np.abs(got - want))
     assert err <= tol * peak, f"{err / peak:.2e} of the peak"
@@ -88,10 +88,11 @@ def test_single_precision_is_within_the_references_float32_bound():
 def test_odd_and_degenerate_grids(shape):
     grid = Grid(dx=0.02, nx=shape[0], ny=shape[1], nz=shape[2])
     oracle, cuda = pair(grid, WALLS["all different"], seed=sum(shape))
+    scale = np.max(np.abs(oracle.p))       # the initial field: tiny rooms lose most of it
     oracle.run(60)
     cuda.run(60)
-    close_to_peak(cuda.recorded_pressure, oracle.recorded_pressure, 1e-12)
-    close_to_peak(cuda.p, oracle.p, 1e-12)
+    close_to_peak(cuda.recorded_pressure, oracle.recorded_pressure, 1e-12, scale)
+    close_to_peak(cuda.p, oracle.p, 1e-12, scale)
 
 
 def test_entering_the_scheme_mid_run():

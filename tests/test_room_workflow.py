@@ -98,5 +98,5 @@ def test_workflow_with_device_postprocessing_matches_the_reference(impulse):
     assert metrics["t20"][0] == pytest.approx(f["t20"], rel=1e-12)
     assert metrics["edt"][0] == pytest.approx(f["edt"], rel=1e-12)
     host = ir.decay_metrics(device=False)
-    for name in ("t20", "edt", "c50", "c80"):
-        np.testing.assert_allclose(metrics[name], host[name], rtol=1e-12)
+    for name in ("t20", "t30", "edt", "c50", "c80"):
+        np.testing.assert_allclose(metrics[name], host[name], rtol=1e-12)   # NaN where both are
