@@ -393,22 +393,36 @@ class DistributedSlabRoom(_SlabSet):
         return len(self._receivers) - 1
 
     def exchange(self) -> None:
+        """Refresh both ghost planes from the neighbours. With NCCL nothing waits on the host:
+        the solver and NCCL's calls are ordered on the device (the solver runs on the legacy
+        default stream, torch's current stream, which NCCL's stream waits for before the
+        transfer and which waits for the transfer before the next step). Other backends move
+        host-visible data, so the device is synchronised around them."""
         import torch
+        import torch.distributed as dist
 
+        if self.world == 1:
+            return
         s = self.slab
-        s.solver.synchronize()
+        on_device = dist.get_backend(self.group) == "nccl" and s.solver._stream.value in (None, 0)
+        if not on_device:
+            s.solver.synchronize()
         # Views over the current copy of p (the fused schemes alternate between two copies).
         planes = (s.plane_view(s.first_owned), s.plane_view(s.last_owned),
                   s.plane_view(s.left_ghost) if s.has_left else None,
                   s.plane_view(s.right_ghost) if s.has_right else None)
         exchange_ghosts(*planes, self.rank, self.world, self.group)
-        torch.cuda.synchronize(s.solver.device)
+        if not on_device:
+            torch.cuda.synchronize(s.solver.device)
 
     def run(self, n_steps: int) -> None:
         n_steps = int(n_steps)
         if n_steps <= 0:
             return
         self.slab.solver.flush()
+        if self.world == 1:              # no cut: the whole room, in CUDA graphs
+            self.slab.solver.run(n_steps)
+            return
         self.exchange()
         for _ in range(n_steps):
             self.slab.solver.run(1)
