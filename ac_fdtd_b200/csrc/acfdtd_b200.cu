@@ -1739,9 +1739,17 @@ struct LeanBatchParams {
     const int64_t *step_base;
 };
 
-// 128 registers: at 96 the batch loop's context spills 30-150 bytes per thread.
+// Registers per thread of the lean batch kernel (at 96 the batch loop's context spills 30-150
+// bytes per thread), and whether single-precision batches use it (else fused_batch).
+#ifndef ACF_LEAN_BATCH_REGS
+#define ACF_LEAN_BATCH_REGS 128
+#endif
+#ifndef ACF_BATCH_LEAN
+#define ACF_BATCH_LEAN 1
+#endif
+
 template <bool LAYER, bool WALLS, int NR>
-__global__ void __maxnreg__(128) lean_batch(const LeanBatchParams b) {
+__global__ void __maxnreg__(ACF_LEAN_BATCH_REGS) lean_batch(const LeanBatchParams b) {
     __shared__ __align__(16) unsigned char raw[sizeof(LeanParams)];
     LeanParams *room = reinterpret_cast<LeanParams *>(raw);
     static_assert(sizeof(LeanParams) % sizeof(int) == 0, "LeanParams must be a whole number of words");
@@ -1920,16 +1928,12 @@ __device__ __forceinline__ void pressure_only_column_simple(const PressureOnlyPa
 }
 
 
-// The same update with each plane's inputs loaded one plane ahead (into registers, while the
-// current plane computes), so a thread keeps two planes of loads in flight: the steady-state
-// step (not the first one, which also reads the velocities).
-template <typename T, bool WALLS>
-struct PoInputs {
-    T Pp[kVec], Ym[kVec], Yp[kVec], Q[kVec];
-    T zb, za;
-};
-
-template <typename T, bool WALLS>
+// The steady-state step, lean in instructions. The Laplacian is formed as the neighbour sum
+// minus 6p (a neighbour missing at a rigid face is replaced by p, which is the same Neumann
+// operator), and 2 p + lam2 L p as (2 - 6 lam2) p + lam2 (neighbour sum): two fused
+// multiply-adds per cell after five additions. The pressures then differ from the p-v scheme's
+// by rounding only, like the first form. ALIGNED: nz is a multiple of 4 (no padding lanes).
+template <typename T, bool WALLS, bool ALIGNED>
 __device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T> &g, int i_begin,
                                                      int i_end, int j, int c, int64_t step) {
     const Room<T> &s = g.room;
@@ -1940,61 +1944,71 @@ __device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T>
     const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
     const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
     const bool wall_column = !y_lo || !y_hi || !z_lo || k0 + kVec >= s.nz;
+    const int real = ALIGNED ? kVec : min(kVec, s.nz - k0);   // cells of the chunk in the room
     const bool any_point = (s.n_src | s.n_rec) != 0;
     bool all_points = false;
     const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
     const bool any_mine = points != 0 || all_points;
-    const T lam2 = g.lam2;
+    const T lam2 = g.lam2, centre = T(2) - T(6) * g.lam2;
     T bad = T(0);
 
-    // Inputs of plane i: p of plane i + 1 (own row), rows j -+ 1 and the row's z neighbours
-    // at plane i, p^{n-1} at plane i. Missing neighbours are replaced by p when used.
-    auto load = [&](int i, PoInputs<T, WALLS> &in) {
-        const int64_t base = (int64_t)i * s.plane + column;
-        if (i + 1 < s.nx) Vec4<T>::ldg(cur + base + s.plane, in.Pp);
-        if (y_lo) Vec4<T>::ldg(cur + base - s.pz, in.Ym);
-        if (y_hi) Vec4<T>::ldg(cur + base + s.pz, in.Yp);
-        in.zb = z_lo ? __ldg(cur + base - 1) : T(0);
-        in.za = z_hi ? __ldg(cur + base + kVec) : T(0);
-        Vec4<T>::load(nxt + base, in.Q);
-    };
-
-    T Pm[kVec] = {T(0), T(0), T(0), T(0)}, P[kVec];
+    T Pm[kVec], P[kVec];
     Vec4<T>::ldg(cur + (int64_t)i_begin * s.plane + column, P);
     if (i_begin > 0) Vec4<T>::ldg(cur + (int64_t)(i_begin - 1) * s.plane + column, Pm);
-    PoInputs<T, WALLS> in;
-    load(i_begin, in);
+    else {
+#pragma unroll
+        for (int e = 0; e < kVec; e++) Pm[e] = P[e];
+    }
 
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
-        PoInputs<T, WALLS> ahead;
-        if (i + 1 < i_end) {
-            if (s.prefetch && i + 2 < i_end) {   // two planes ahead into L2
-                if (i + 3 < s.nx) prefetch_l2(cur + base + 3 * s.plane);
-                prefetch_l2(nxt + base + 2 * s.plane);
-            }
-            load(i + 1, ahead);
+        if (s.prefetch && i + 1 < i_end) {   // the next plane's own-row inputs into L2
+            if (i + 2 < s.nx) prefetch_l2(cur + base + 2 * s.plane);
+            prefetch_l2(nxt + base + s.plane);
         }
-        const bool x_lo = i > 0, x_hi = i + 1 < s.nx;
-        const bool wall_plane = WALLS && (wall_column || !x_lo || !x_hi);
+        T Pp[kVec], Ym[kVec], Yp[kVec], Q[kVec];
+        if (i + 1 < s.nx) Vec4<T>::ldg(cur + base + s.plane, Pp);
+        else {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) Pp[e] = P[e];
+        }
+        if (y_lo) Vec4<T>::ldg(cur + base - s.pz, Ym);
+        else {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) Ym[e] = P[e];
+        }
+        if (y_hi) Vec4<T>::ldg(cur + base + s.pz, Yp);
+        else {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) Yp[e] = P[e];
+        }
+        const T zb = z_lo ? __ldg(cur + base - 1) : P[0];
+        T za = z_hi ? __ldg(cur + base + kVec) : P[kVec - 1];
+        Vec4<T>::load(nxt + base, Q);
+
         T Pn[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
-            const int k = k0 + e;
-            const T p = P[e];
-            if (k >= s.nz) {          // padding
-                Pn[e] = p;
-                continue;
+            T zp = e + 1 < kVec ? P[e + 1] : za;
+            if (!ALIGNED && real < kVec && e + 1 == real) zp = P[e];   // top cell, padded row
+            const T zm = e == 0 ? zb : P[e - 1];
+            const T sum = ((Pm[e] + Pp[e]) + (Ym[e] + Yp[e])) + (zm + zp);
+            Pn[e] = fma_t(lam2, sum, fma_t(centre, P[e], -Q[e]));
+        }
+        if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                T fu, fp;
+                if ((ALIGNED || e < real) && wall_pair(s, i, j, k0 + e, fu, fp)) {
+                    const T q = Pn[e] + Q[e];              // 2 p + lam2 L p, back from Pn
+                    Pn[e] = fu * q - (fu - fp) * Q[e];
+                }
             }
-            const T xm = x_lo ? Pm[e] : p, xp = x_hi ? in.Pp[e] : p;
-            const T ym = y_lo ? in.Ym[e] : p, yp = y_hi ? in.Yp[e] : p;
-            const T zm = e == 0 ? (z_lo ? in.zb : p) : P[e - 1];
-            const T zp = k + 1 < s.nz ? (e + 1 < kVec ? P[e + 1] : in.za) : p;
-            const T lap = ((xm - p) + (xp - p)) + ((ym - p) + (yp - p)) + ((zm - p) + (zp - p));
-            const T q = fma_t(lam2, lap, p + p);
-            T fu = T(1), fp = T(0);
-            if (wall_plane && wall_pair(s, i, j, k, fu, fp)) Pn[e] = fu * q - (fu - fp) * in.Q[e];
-            else Pn[e] = q - in.Q[e];
+        }
+        if (!ALIGNED) {
+#pragma unroll
+            for (int e = 0; e < kVec; e++)
+                if (e >= real) Pn[e] = P[e];               // padding lanes keep their value
         }
         if (any_mine) {
             // - S^{n-1} (added by the previous step), then + S^n, in the order added
@@ -2022,14 +2036,14 @@ __device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T>
 #pragma unroll
         for (int e = 0; e < kVec; e++) {
             Pm[e] = P[e];
-            P[e] = in.Pp[e];
+            P[e] = Pp[e];
         }
-        in = ahead;
     }
     report_nonfinite(s.status, bad != bad);
 }
 
-template <typename T, bool WALLS, bool FIRST>
+// FIRST: the step from the p-v state; otherwise the steady-state step, ALIGNED or padded.
+template <typename T, bool WALLS, bool FIRST, bool ALIGNED = false>
 __global__ void __launch_bounds__(256) pressure_only_sweep(const PressureOnlyParams<T> g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -2040,7 +2054,7 @@ __global__ void __launch_bounds__(256) pressure_only_sweep(const PressureOnlyPar
     if constexpr (FIRST)
         pressure_only_column_simple<T, WALLS, true>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
     else
-        pressure_only_column<T, WALLS>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
+        pressure_only_column<T, WALLS, ALIGNED>(g, i_begin, min(g.room.nx, i_begin + g.planes), j, c, step);
 }
 
 // The two sums of the pressure-only scheme's conserved energy after a step, with cur = p^{n+1}
@@ -3513,7 +3527,7 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
     if (events) cudaEventRecord(events[0], st);
     if (b->rooms.size() > 1 && b->fused()) {
         const dim3 grid(b->batch_ctas), block(b->block_threads);
-        if constexpr (sizeof(T) == 4) {   // the lean single-precision column
+        if constexpr (sizeof(T) == 4 && ACF_BATCH_LEAN) {   // the lean single-precision column
             LeanBatchParams p{};
             p.rooms = (const LeanParams *)b->lean_table + (b->rooms[0].cur ? b->rooms.size() : 0);
             p.tiles = b->tiles;
@@ -3554,9 +3568,12 @@ void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *even
         if (first) {
             if (h.has_walls) pressure_only_sweep<T, true, true><<<L.grid, L.block, 0, st>>>(g);
             else pressure_only_sweep<T, false, true><<<L.grid, L.block, 0, st>>>(g);
+        } else if (h.nz % kVec == 0) {
+            if (h.has_walls) pressure_only_sweep<T, true, false, true><<<L.grid, L.block, 0, st>>>(g);
+            else pressure_only_sweep<T, false, false, true><<<L.grid, L.block, 0, st>>>(g);
         } else {
-            if (h.has_walls) pressure_only_sweep<T, true, false><<<L.grid, L.block, 0, st>>>(g);
-            else pressure_only_sweep<T, false, false><<<L.grid, L.block, 0, st>>>(g);
+            if (h.has_walls) pressure_only_sweep<T, true, false, false><<<L.grid, L.block, 0, st>>>(g);
+            else pressure_only_sweep<T, false, false, false><<<L.grid, L.block, 0, st>>>(g);
         }
         h.cur ^= 1;
         if (events) {
