@@ -367,6 +367,36 @@ __device__ __forceinline__ bool wall_pair(const Room<T> &s, int i, int j, int k,
     return fp != T(0) || fu != T(1);
 }
 
+// The wall closed form for the cells of one column chunk at plane i: on an x-face plane or a
+// y-face row (both uniform across a warp) every cell is tested; elsewhere only the chunk's
+// k = 0 and k = nz - 1 cells can lie on a face -- a z face, the first in FACES order for them --
+// so the thread reads just those pairs instead of searching four cells. `apply(e, fu, fp)` is
+// called for each cell e (< real) with an absorbing pair.
+template <typename T, typename Apply>
+__device__ __forceinline__ void column_walls(const Room<T> &s, int i, int j, int k0, int real,
+                                             Apply apply) {
+    if (i == 0 || i == s.nx - 1 || j == 0 || j == s.ny - 1) {
+#pragma unroll
+        for (int e = 0; e < kVec; e++) {
+            T fu, fp;
+            if (e < real && wall_pair(s, i, j, k0 + e, fu, fp)) apply(e, fu, fp);
+        }
+        return;
+    }
+    const bool bottom = k0 == 0, top_chunk = k0 + kVec >= s.nz;
+    if (!bottom && !top_chunk) return;
+    const int64_t at = 2 * ((int64_t)i * s.ny + j);
+    if (bottom) {
+        const T fu = __ldg(s.shell[4] + at), fp = __ldg(s.shell[4] + at + 1);
+        if (fp != T(0) || fu != T(1)) apply(0, fu, fp);
+    }
+    const int top = s.nz - 1 - k0;
+    if (top_chunk && (top > 0 || k0 > 0)) {     // k = nz - 1 is not also k = 0
+        const T fu = __ldg(s.shell[5] + at), fp = __ldg(s.shell[5] + at + 1);
+        if (fp != T(0) || fu != T(1)) apply(top, fu, fp);
+    }
+}
+
 // Sources (bit q) and receivers (bit n_src + r) that lie in one (row j, chunk at k0) column,
 // found once per column so that the march visits them only at their own plane instead of
 // scanning every point at every plane. Beyond 32 points `all` is set and every point is
@@ -1645,12 +1675,11 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         float Pn[kVec] = {pe01.x, pe01.y, pe23.x, pe23.y};
         if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
             const float Po[kVec] = {P.x, P.y, P.z, P.w};
+            column_walls(s, i, j, k0, real, [&](int e, float fu, float fp) {
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                float fu, fp;
-                if ((ALIGNED || e < real) && wall_pair(s, i, j, k0 + e, fu, fp))
-                    Pn[e] = Pn[e] * fu - Po[e] * fp;
-            }
+                for (int q = 0; q < kVec; q++)
+                    if (q == e) Pn[q] = Pn[q] * fu - Po[q] * fp;
+            });
         }
         if (LAYER) {
             if (fi_cell != 1.f) {
@@ -1727,51 +1756,6 @@ __global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR)) lean_swee
 template <bool LAYER, bool WALLS, int NR>
 __global__ void __maxnreg__(96) lean_sweep_padded(const LeanParams g) {
     lean_sweep_body<LAYER, WALLS, NR, false>(g);
-}
-
-// The lean fused step over a batch's tile table (fused_batch's schedule), every room's
-// description (with its packed coefficients) staged in shared memory by the CTA.
-struct LeanBatchParams {
-    const LeanParams *rooms;        // one per room, for the current parity
-    const Tile *tiles;
-    int32_t n_tiles;
-    int32_t local_step;
-    const int64_t *step_base;
-};
-
-// Registers per thread of the lean batch kernel (at 96 the batch loop's context spills 30-150
-// bytes per thread), and whether single-precision batches use it (else fused_batch).
-#ifndef ACF_LEAN_BATCH_REGS
-#define ACF_LEAN_BATCH_REGS 128
-#endif
-#ifndef ACF_BATCH_LEAN
-#define ACF_BATCH_LEAN 1
-#endif
-
-template <bool LAYER, bool WALLS, int NR>
-__global__ void __maxnreg__(ACF_LEAN_BATCH_REGS) lean_batch(const LeanBatchParams b) {
-    __shared__ __align__(16) unsigned char raw[sizeof(LeanParams)];
-    LeanParams *room = reinterpret_cast<LeanParams *>(raw);
-    static_assert(sizeof(LeanParams) % sizeof(int) == 0, "LeanParams must be a whole number of words");
-    const int64_t step = *b.step_base + b.local_step;
-    int staged = -1;
-    for (int t = blockIdx.x; t < b.n_tiles; t += gridDim.x) {
-        const Tile tile = b.tiles[t];
-        if (tile.room != staged) {
-            __syncthreads();
-            const int *from = reinterpret_cast<const int *>(b.rooms + tile.room);
-            int *to = reinterpret_cast<int *>(raw);
-            for (int w = threadIdx.x; w < (int)(sizeof(LeanParams) / sizeof(int)); w += blockDim.x)
-                to[w] = __ldg(from + w);
-            __syncthreads();
-            staged = tile.room;
-        }
-        if ((int)threadIdx.x < tile.count) {
-            const int pair = tile.first + threadIdx.x;
-            lean_column<LAYER, WALLS, NR, false>(*room, tile.i_begin, tile.i_end, pair / room->f.room.nchunks,
-                                                 pair % room->f.room.nchunks, step);
-        }
-    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1996,14 +1980,14 @@ __device__ __forceinline__ void pressure_only_column(const PressureOnlyParams<T>
             Pn[e] = fma_t(lam2, sum, fma_t(centre, P[e], -Q[e]));
         }
         if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
+            column_walls(s, i, j, k0, real, [&](int e, T fu, T fp) {
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
-                T fu, fp;
-                if ((ALIGNED || e < real) && wall_pair(s, i, j, k0 + e, fu, fp)) {
-                    const T q = Pn[e] + Q[e];              // 2 p + lam2 L p, back from Pn
-                    Pn[e] = fu * q - (fu - fp) * Q[e];
-                }
-            }
+                for (int q = 0; q < kVec; q++)
+                    if (q == e) {
+                        const T two_p = Pn[q] + Q[q];      // 2 p + lam2 L p, back from Pn
+                        Pn[q] = fu * two_p - (fu - fp) * Q[q];
+                    }
+            });
         }
         if (!ALIGNED) {
 #pragma unroll
@@ -3086,7 +3070,6 @@ struct acf_batch {
     size_t state_bytes = 0;
     void *room_table = nullptr;      // device array of Room<T>, one per room
     void *fused_table = nullptr;     // fused scheme on a batch: 2 x rooms FusedParams<T>, by parity
-    void *lean_table = nullptr;      // the same in single precision: 2 x rooms LeanParams
     bool room_table_dirty = true;
     Tile *tiles = nullptr;
     int32_t n_tiles = 0;
@@ -3283,8 +3266,6 @@ Room<T> make_room(const acf_batch *b, int r, const void *state = nullptr) {
     return s;
 }
 
-void fill_pairs(float2 *pairs, const RoomHost &h);
-
 template <typename T>
 int upload_room_table(acf_batch *b) {
     std::vector<Room<T>> table(b->rooms.size());
@@ -3312,17 +3293,6 @@ int upload_room_table(acf_batch *b) {
         if (!b->fused_table) ACF_CUDA(cudaMalloc(&b->fused_table, fused.size() * sizeof(FusedParams<T>)));
         ACF_CUDA(cudaMemcpy(b->fused_table, fused.data(), fused.size() * sizeof(FusedParams<T>),
                             cudaMemcpyHostToDevice));
-        if constexpr (sizeof(T) == 4) {
-            std::vector<LeanParams> lean(fused.size());
-            for (size_t q = 0; q < fused.size(); q++) {
-                lean[q] = LeanParams{};
-                lean[q].f = fused[q];
-                fill_pairs(lean[q].pairs, b->rooms[q % n]);
-            }
-            if (!b->lean_table) ACF_CUDA(cudaMalloc(&b->lean_table, lean.size() * sizeof(LeanParams)));
-            ACF_CUDA(cudaMemcpy(b->lean_table, lean.data(), lean.size() * sizeof(LeanParams),
-                                cudaMemcpyHostToDevice));
-        }
     }
     b->room_table_dirty = false;
     return ACF_OK;
@@ -3431,12 +3401,6 @@ struct LeanStepPadded {
     }
 };
 
-template <typename T, bool L, bool W, int NR>
-struct LeanBatch {
-    static void launch(const LeanBatchParams &p, dim3 g, dim3 b, cudaStream_t st) {
-        lean_batch<L, W, NR><<<g, b, 0, st>>>(p);
-    }
-};
 
 // The packed coefficients of the single-precision kernels: each rounded to float once, the
 // negated slots negated after that rounding, so each is exactly minus the scalar's value.
@@ -3526,24 +3490,16 @@ template <typename T>
 void launch_step(acf_batch *b, int32_t local, cudaStream_t st, cudaEvent_t *events) {
     if (events) cudaEventRecord(events[0], st);
     if (b->rooms.size() > 1 && b->fused()) {
+        // The tile-table launch keeps the generic column: the lean column there measured 82-89
+        // Gcell-updates/s on the 64 uneven rooms against 94 (its registers cost warps per SM).
         const dim3 grid(b->batch_ctas), block(b->block_threads);
-        if constexpr (sizeof(T) == 4 && ACF_BATCH_LEAN) {   // the lean single-precision column
-            LeanBatchParams p{};
-            p.rooms = (const LeanParams *)b->lean_table + (b->rooms[0].cur ? b->rooms.size() : 0);
-            p.tiles = b->tiles;
-            p.n_tiles = b->n_tiles;
-            p.local_step = local;
-            p.step_base = b->step_base;
-            dispatch_pressure<float, LeanBatch>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
-        } else {
-            FusedBatchParams<T> p{};
-            p.rooms = (const FusedParams<T> *)b->fused_table + (b->rooms[0].cur ? b->rooms.size() : 0);
-            p.tiles = b->tiles;
-            p.n_tiles = b->n_tiles;
-            p.local_step = local;
-            p.step_base = b->step_base;
-            dispatch_pressure<T, BatchFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
-        }
+        FusedBatchParams<T> p{};
+        p.rooms = (const FusedParams<T> *)b->fused_table + (b->rooms[0].cur ? b->rooms.size() : 0);
+        p.tiles = b->tiles;
+        p.n_tiles = b->n_tiles;
+        p.local_step = local;
+        p.step_base = b->step_base;
+        dispatch_pressure<T, BatchFused>(b->any_layer, b->any_walls, b->n_relax, p, grid, block, st);
         for (RoomHost &h : b->rooms) h.cur ^= 1;
         if (events) {
             cudaEventRecord(events[1], st);
@@ -3874,7 +3830,6 @@ void free_batch(acf_batch *b) {
     cudaFree(b->state);
     cudaFree(b->room_table);
     cudaFree(b->fused_table);
-    cudaFree(b->lean_table);
     cudaFree(b->tiles);
     cudaFree(b->step_base);
     cudaFree(b->energy_scratch);

@@ -158,19 +158,24 @@ def test_refusals_and_what_the_scheme_does_not_keep():
     cuda.close()
 
 
-def test_large_room_single_precision_agrees_with_the_fused_pv_scheme():
-    """256^3 fp32 with walls (the L2 plane prefetch on at this size): the pressure-only scheme
-    against the fused p-v scheme over 400 steps from a source, to the float32 bound."""
+def test_large_room_single_precision_against_double():
+    """256^3 fp32 with walls (the L2 plane prefetch on at this size), 400 steps from a source:
+    the pressure-only scheme and the fused p-v scheme in fp32, each against the p-v scheme in
+    fp64. The second-order form carries p^{n-1} rather than a velocity, so its float32 rounding
+    accumulates faster than the p-v form's: it is held to 3e-4 of the peak, the p-v form to 3e-5."""
     grid = Grid(dx=343.2 / 40000.0, nx=256, ny=256, nz=256)
     walls = WallAdmittances(0.11, 0.05, 0.2, 0.31, 0.07, 0.4)
     out = {}
-    for scheme in ("fused", "pressure_only"):
-        s = CudaAcousticFDTD(grid, dtype=np.float32, walls=walls, scheme=scheme)
+    for scheme, dtype in (("fused", np.float64), ("fused", np.float32), ("pressure_only", np.float32)):
+        s = CudaAcousticFDTD(grid, dtype=dtype, walls=walls, scheme=scheme)
         s.add_volume_source((0.4, 0.5, 0.6), np.hanning(40))
         for point in ((1.1, 1.2, 0.9), (0.3, 1.9, 1.7)):
             s.add_pressure_receiver(point)
         s.run(400)
-        out[scheme] = (s.recorded_pressure.astype(np.float64), s.p.astype(np.float64))
+        out[(scheme, np.dtype(dtype).name)] = (s.recorded_pressure.astype(np.float64),
+                                               s.p.astype(np.float64))
         s.close()
-    close_to_peak(out["pressure_only"][0], out["fused"][0], 1e-4)
-    close_to_peak(out["pressure_only"][1], out["fused"][1], 1e-4)
+    double = out[("fused", "float64")]
+    for key, tol in ((("fused", "float32"), 3e-5), (("pressure_only", "float32"), 3e-4)):
+        close_to_peak(out[key][0], double[0], tol)
+        close_to_peak(out[key][1], double[1], tol)
