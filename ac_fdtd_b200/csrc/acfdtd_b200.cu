@@ -797,7 +797,11 @@ __device__ __forceinline__ void fused_column(const FusedParams<T> &f, int i_begi
         T ZS[kVec];
 #pragma unroll
         for (int e = 0; e < kVec; e++) ZS[e] = k0 + e <= s.nz ? ZL[e] : VZ[e];
-        Vec4<T>::store(f.np + base, Pn);
+        // A slab's ghost planes get their p from the neighbours' sweeps, never from their own;
+        // its boundary planes also go to the neighbours' ghost planes (in their next copies).
+        if (i >= s.own_lo && i < s.own_hi) Vec4<T>::store(f.np + base, Pn);
+        if (s.ghost_lo != nullptr && i == s.own_lo) Vec4<T>::store(s.ghost_lo + column, Pn);
+        if (s.ghost_hi != nullptr && i == s.own_hi - 1) Vec4<T>::store(s.ghost_hi + column, Pn);
         Vec4<T>::store(f.nvx + base, XL);
         Vec4<T>::store(f.nvy + base, YL);
         Vec4<T>::store(f.nvz + base, ZS);
@@ -1705,7 +1709,12 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
 
         // ---- stores: p, the three lower faces, the far boundary faces, psi in place
-        *reinterpret_cast<float4 *>(f.np + base) = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
+        // A slab's ghost planes get their p from the neighbours' sweeps, never from their own;
+        // its boundary planes also go to the neighbours' ghost planes (in their next copies).
+        const float4 pn4 = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
+        if (i >= s.own_lo && i < s.own_hi) *reinterpret_cast<float4 *>(f.np + base) = pn4;
+        if (s.ghost_lo != nullptr && i == s.own_lo) *reinterpret_cast<float4 *>(s.ghost_lo + column) = pn4;
+        if (s.ghost_hi != nullptr && i == s.own_hi - 1) *reinterpret_cast<float4 *>(s.ghost_hi + column) = pn4;
         *reinterpret_cast<float4 *>(f.nvx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
         *reinterpret_cast<float4 *>(f.nvy + base) = make_float4(YL01.x, YL01.y, YL23.x, YL23.y);
         float4 ZS = make_float4(ZL01.x, ZL01.y, ZL23.x, ZL23.y);
@@ -4191,6 +4200,130 @@ int run_batch(acf_batch *b, int64_t n_steps, int64_t step_offset, acf_stream str
 // kernel: a velocity sweep waits for the neighbours' pressure sweeps of the previous step
 // (they wrote its ghost planes), a pressure sweep for the neighbours' velocity sweeps of the
 // same step (they read the ghost planes it overwrites).
+// The fused step of every part of a slab group, for the parity the parts are at: each part
+// reads its current copy and writes its next one; its p store skips the ghost planes, and its
+// first and last own planes also go to the neighbours' ghost planes in the neighbours' NEXT
+// copies (what they read at the following step). All parameters are formed before any part's
+// copy flips; `after(q)` runs after part q's launch (an event record across GPUs).
+template <typename T, typename After>
+void fused_slab_step(acf_batch *const *parts, int n, const int32_t *own_lo, const int32_t *own_hi,
+                     int32_t local, const std::vector<cudaStream_t> &streams, After after) {
+    std::vector<FusedParams<T>> f((size_t)n);
+    for (int q = 0; q < n; q++) {
+        acf_batch *b = parts[q];
+        FusedParams<T> &x = f[q];
+        x = FusedParams<T>{};
+        x.room = make_room<T>(b, 0);
+        x.room.own_lo = own_lo[q];
+        x.room.own_hi = own_hi[q];
+        if (q > 0)
+            x.room.ghost_lo = (T *)parts[q - 1]->other_ptr(0, ACF_FIELD_P) + (int64_t)own_hi[q - 1] * x.room.plane;
+        if (q + 1 < n)
+            x.room.ghost_hi = (T *)parts[q + 1]->other_ptr(0, ACF_FIELD_P) +
+                              (int64_t)(own_lo[q + 1] - 1) * x.room.plane;
+        x.np = (T *)b->other_ptr(0, ACF_FIELD_P);
+        x.nvx = (T *)b->other_ptr(0, ACF_FIELD_VX);
+        x.nvy = (T *)b->other_ptr(0, ACF_FIELD_VY);
+        x.nvz = (T *)b->other_ptr(0, ACF_FIELD_VZ);
+        x.step_base = b->step_base;
+        x.local_step = local;
+        x.planes = b->planes;
+    }
+    for (int q = 0; q < n; q++) {
+        DeviceGuard g(parts[q]->device);
+        const RoomHost &h = parts[q]->rooms[0];
+        const LaunchShape L = single_shape(parts[q]);
+        if constexpr (sizeof(T) == 4) {
+            LeanParams lp{};
+            lp.f = f[q];
+            fill_pairs(lp.pairs, h);
+            if (h.nz % kVec == 0)
+                dispatch_pressure<float, LeanStep>(h.has_layer, h.has_walls, h.n_relax, lp, L.grid, L.block, streams[q]);
+            else
+                dispatch_pressure<float, LeanStepPadded>(h.has_layer, h.has_walls, h.n_relax, lp, L.grid,
+                                                         L.block, streams[q]);
+        } else {
+            dispatch_pressure<T, FusedStep>(h.has_layer, h.has_walls, h.n_relax, f[q], L.grid, L.block, streams[q]);
+        }
+        parts[q]->launches += 1;
+        after(q);
+    }
+    for (int q = 0; q < n; q++) parts[q]->rooms[0].cur ^= 1;
+}
+
+// Slab groups on the fused scheme: one launch per part and step. On one GPU the steps replay
+// from a CUDA graph of an even number of steps (the copies come back to the same parity);
+// across GPUs each part's step waits, by events, for its neighbours' previous step (which wrote
+// its ghost planes and read the copy it now writes into theirs).
+template <typename T>
+int run_fused_slabs(acf_batch *const *parts, int n, const int32_t *own_lo, const int32_t *own_hi,
+                    int64_t n_steps, int64_t step_offset, cudaStream_t st, bool one_device) {
+    std::vector<cudaStream_t> streams((size_t)n, one_device ? st : (cudaStream_t)0);
+    for (int q = 0; q < n; q++) {
+        DeviceGuard g(parts[q]->device);
+        set_step_base<<<1, 1, 0, streams[q]>>>(parts[q]->step_base, step_offset);
+        parts[q]->launches += 1;
+    }
+    int64_t done = 0;
+    if (one_device) {
+        const int64_t G = 64;
+        if (n_steps >= G) {
+            cudaStream_t cap = nullptr;
+            ACF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            std::vector<cudaStream_t> cs((size_t)n, cap);
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            cudaError_t err = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (err == cudaSuccess) {
+                for (int64_t t = 0; t < G; t++) fused_slab_step<T>(parts, n, own_lo, own_hi, (int32_t)t, cs, [](int) {});
+                for (int q = 0; q < n; q++) bump_step_base<<<1, 1, 0, cap>>>(parts[q]->step_base, G);
+                err = cudaStreamEndCapture(cap, &graph);
+            }
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            for (; err == cudaSuccess && done + G <= n_steps; done += G) {
+                err = cudaGraphLaunch(exec, st);
+                for (int q = 0; q < n; q++) parts[q]->launches += G + 1;
+            }
+            if (exec) cudaGraphExecDestroy(exec);
+            cudaStreamDestroy(cap);
+            if (err != cudaSuccess) return fail(ACF_ERR_CUDA, "slab graph: %s", cudaGetErrorString(err));
+        }
+        for (int64_t t = 0; done + t < n_steps; t++)
+            fused_slab_step<T>(parts, n, own_lo, own_hi, (int32_t)t, streams, [](int) {});
+        ACF_CUDA(cudaGetLastError());
+        return ACF_OK;
+    }
+    std::vector<cudaEvent_t> done_ev((size_t)n, nullptr);
+    auto release = [&]() {
+        for (int q = 0; q < n; q++) {
+            DeviceGuard g(parts[q]->device);
+            if (done_ev[q]) cudaEventDestroy(done_ev[q]);
+        }
+    };
+    for (int q = 0; q < n; q++) {
+        DeviceGuard g(parts[q]->device);
+        if (cudaEventCreateWithFlags(&done_ev[q], cudaEventDisableTiming) != cudaSuccess) {
+            release();
+            return fail(ACF_ERR_CUDA, "event creation failed");
+        }
+    }
+    for (int64_t t = 0; t < n_steps; t++) {
+        if (t > 0)
+            for (int q = 0; q < n; q++) {
+                DeviceGuard g(parts[q]->device);
+                for (int r : {q - 1, q + 1})
+                    if (r >= 0 && r < n) cudaStreamWaitEvent(streams[q], done_ev[r], 0);
+            }
+        fused_slab_step<T>(parts, n, own_lo, own_hi, (int32_t)t, streams,
+                           [&](int q) { cudaEventRecord(done_ev[q], streams[q]); });
+    }
+    const cudaError_t e = cudaGetLastError();
+    release();
+    if (e != cudaSuccess) return fail(ACF_ERR_CUDA, "slab step: %s", cudaGetErrorString(e));
+    return ACF_OK;
+}
+
 template <typename T>
 int run_slabs_impl(acf_batch *const *parts, int n, const int32_t *own_lo, const int32_t *own_hi,
                    int64_t n_steps, int64_t step_offset, cudaStream_t st) {
@@ -4293,8 +4426,12 @@ int run_slabs(acf_solver *const *parts, int32_t n, const int32_t *own_lo, const 
         if (!b) return fail(ACF_ERR_ARGUMENT, "null part %d", q);
         const RoomHost &h = b->rooms[0];
         const RoomHost &h0 = parts[0]->rooms[0];
-        if (b->scheme != ACF_SCHEME_TWO_SWEEPS)
-            return fail(ACF_ERR_STATE, "part %d: slabs step with the two-sweep scheme", q);
+        if (b->scheme != parts[0]->scheme ||
+            (b->scheme != ACF_SCHEME_TWO_SWEEPS && b->scheme != ACF_SCHEME_FUSED))
+            return fail(ACF_ERR_STATE, "part %d: slabs step with the two-sweep or the fused scheme, "
+                        "the same for every part", q);
+        if (b->rooms[0].cur != parts[0]->rooms[0].cur)
+            return fail(ACF_ERR_STATE, "part %d: the fused copies of the parts are out of step", q);
         if (b->precision != parts[0]->precision || h.ny != h0.ny || h.nz != h0.nz)
             return fail(ACF_ERR_ARGUMENT, "part %d differs in precision, ny or nz", q);
         const bool left = q > 0, right = q + 1 < n;
@@ -4317,6 +4454,10 @@ int run_slabs(acf_solver *const *parts, int32_t n, const int32_t *own_lo, const 
     }
     DeviceGuard guard(parts[0]->device);
     acf_batch *const *b = (acf_batch *const *)parts;
+    if (parts[0]->scheme == ACF_SCHEME_FUSED)
+        return parts[0]->precision == 8
+                   ? run_fused_slabs<double>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream, one_device)
+                   : run_fused_slabs<float>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream, one_device);
     return parts[0]->precision == 8
                ? run_slabs_impl<double>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream)
                : run_slabs_impl<float>(b, n, own_lo, own_hi, n_steps, step_offset, (cudaStream_t)stream);

@@ -17,11 +17,11 @@ overwrites them before the next step.
 
 Two ways to run the parts:
 
-* ``SlabGroup`` -- every part in this process (one GPU or several). With the two-sweep scheme
-  the exchange is fused into the pressure sweep: each part's sweep stores its first and last
-  own planes straight into the neighbours' ghost planes (peer stores across GPUs,
-  ``acf_run_slabs``), and the steps are ordered so that no kernel waits on another; the other
-  schemes copy the ghost planes after each step (``acf_copy_plane``);
+* ``SlabGroup`` -- every part in this process (one GPU or several). With the two-sweep and the
+  fused schemes the exchange is part of the step: each part's pressure update stores its first
+  and last own planes straight into the neighbours' ghost planes (peer stores across GPUs,
+  ``acf_run_slabs``), and the steps are ordered so that no kernel waits on another; the staged
+  scheme copies the ghost planes after each step (``acf_copy_plane``);
 * ``DistributedSlabRoom`` -- this rank's part, one process per GPU, planes exchanged by
   ``exchange_ghosts`` over ``torch.distributed`` (NCCL between GPUs; gloo in the CPU tests).
 
@@ -265,16 +265,18 @@ class SlabGroup(_SlabSet):
                 s.solver.synchronize()
 
     def run(self, n_steps: int) -> None:
-        """Advance every part. With the two-sweep scheme each pressure sweep also stores its
-        boundary planes into the neighbours' ghost planes (``acf_run_slabs``: no exchange step);
-        the other schemes step part by part and copy the ghost planes after each step."""
+        """Advance every part. With the two-sweep or the fused scheme each step's pressure update
+        also stores the boundary planes into the neighbours' ghost planes (``acf_run_slabs``: no
+        exchange step; the fused steps replay from a CUDA graph on one GPU); the staged scheme
+        steps part by part and copies the ghost planes after each step."""
         n_steps = int(n_steps)
         if n_steps <= 0:
             return
         for s in self.slabs:
             s.solver.flush()      # state written on the host reaches the device first
         self.exchange()           # ghost planes from the current state
-        if all(s.solver.scheme == "two_sweeps" for s in self.slabs):
+        if all(s.solver.scheme in ("two_sweeps", "fused") for s in self.slabs) and \
+                len({s.solver.scheme for s in self.slabs}) == 1:
             n = len(self.slabs)
             for s in self.slabs:
                 s.solver.prepare_points()

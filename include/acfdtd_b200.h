@@ -304,8 +304,11 @@ int acf_solver_device(const acf_solver *solver);
  * velocity sweep, then every part's pressure sweep, which updates its own planes and also stores
  * its first and last own planes of p into the neighbours' ghost planes (peer stores across
  * GPUs; peer access is enabled as needed). The ghost planes must hold the neighbours' p before
- * the first step (acf_copy_plane). Two-sweep scheme, single rooms of equal precision, ny and
- * nz. Parts on one GPU run on `stream`; parts on several GPUs on each device's default stream,
+ * the first step (acf_copy_plane). With the fused scheme (every part on it, copies in step)
+ * each step is one launch per part: it writes its own planes of the next copy and stores its
+ * first and last own planes into the neighbours' ghost planes of their next copies; on one GPU
+ * the steps replay from a CUDA graph. Single rooms of equal scheme, precision, ny and nz. Parts
+ * on one GPU run on `stream`; parts on several GPUs on each device's default stream,
  * ordered by events, and `stream` must then be null (ACF_ERR_ARGUMENT otherwise: a stream
  * belongs to one device). Asynchronous. No counterpart in the reference. */
 int acf_run_slabs(acf_solver *const *parts, int32_t n_parts, const int32_t *own_lo,
