@@ -402,7 +402,8 @@ __device__ __forceinline__ void column_walls(const Room<T> &s, int i, int j, int
 // scanning every point at every plane. Beyond 32 points `all` is set and every point is
 // scanned, as before.
 template <typename T>
-__device__ __forceinline__ uint32_t column_points(const Room<T> &s, int j, int k0, bool &all) {
+__device__ __forceinline__ uint32_t column_points(const Room<T> &s, int j, int k0, bool &all,
+                                                 int width = kVec) {
     const int total = s.n_src + s.n_rec;
     all = total > 32;
     uint32_t mask = 0;
@@ -410,7 +411,7 @@ __device__ __forceinline__ uint32_t column_points(const Room<T> &s, int j, int k
     const int64_t first = (int64_t)j * s.pz + k0;
     for (int q = 0; q < total; q++) {
         const int64_t col = q < s.n_src ? s.src_col[q] : s.rec_col[q - s.n_src];
-        if (col >= first && col < first + kVec) mask |= 1u << q;
+        if (col >= first && col < first + width) mask |= 1u << q;
     }
     return mask;
 }
@@ -988,6 +989,7 @@ struct VecW;
 template <typename T>
 struct VecW<T, 4> {
     __device__ __forceinline__ static void ldg(const T *__restrict__ a, T v[4]) { Vec4<T>::ldg(a, v); }
+    __device__ __forceinline__ static void load(const T *a, T v[4]) { Vec4<T>::load(a, v); }
     __device__ __forceinline__ static void store(T *__restrict__ a, const T v[4]) { Vec4<T>::store(a, v); }
     __device__ __forceinline__ static void lds(const T *a, T v[4]) { lds4<T>(a, v); }
 };
@@ -996,6 +998,10 @@ template <>
 struct VecW<float, 2> {
     __device__ __forceinline__ static void ldg(const float *__restrict__ a, float v[2]) {
         const float2 t = __ldg(reinterpret_cast<const float2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void load(const float *a, float v[2]) {
+        const float2 t = *reinterpret_cast<const float2 *>(a);
         v[0] = t.x; v[1] = t.y;
     }
     __device__ __forceinline__ static void store(float *__restrict__ a, const float v[2]) {
@@ -1011,6 +1017,10 @@ template <>
 struct VecW<double, 2> {
     __device__ __forceinline__ static void ldg(const double *__restrict__ a, double v[2]) {
         const double2 t = __ldg(reinterpret_cast<const double2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void load(const double *a, double v[2]) {
+        const double2 t = *reinterpret_cast<const double2 *>(a);
         v[0] = t.x; v[1] = t.y;
     }
     __device__ __forceinline__ static void store(double *__restrict__ a, const double v[2]) {
@@ -2285,44 +2295,44 @@ __device__ __forceinline__ T adjoint_face(T lv, T d_lower, T d_upper, T ga, T gb
 // (stored, with the far boundary faces) and its three upper faces (recomputed exactly as their
 // owners compute them) -- and writes lambda_D^n to out_d. Per cell and step this moves (10 + 2R)
 // elements instead of the two sweeps' (13 + 2R), with the same results.
-template <typename T, bool LAYER, bool WALLS, int NR, bool AIR, bool FUSED = false>
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR, bool FUSED = false, int VW = kVec>
 __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &a, int i_begin,
                                                         int i_end, int j, int c, int64_t step,
                                                         T *air_acc) {
     const Room<T> &s = a.room;
-    const int k0 = c * kVec;
+    const int k0 = c * VW;
     const int64_t column = (int64_t)j * s.pz + k0;
-    const bool has_above = k0 + kVec <= s.nz;
+    const bool has_above = k0 + VW <= s.nz;
     const T scp = s.relax_scale - s.cp;
     bool all_points = false;
-    const uint32_t points = (s.n_src | s.n_rec) != 0 ? column_points(s, j, k0, all_points) : 0u;
+    const uint32_t points = (s.n_src | s.n_rec) != 0 ? column_points(s, j, k0, all_points, VW) : 0u;
     const bool any_mine = points != 0 || all_points;
-    const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + kVec >= s.nz;
-    T XL[kVec];
+    const bool wall_column = j == 0 || j == s.ny - 1 || k0 == 0 || k0 + VW >= s.nz;
+    T XL[VW];
     // FUSED: lambda_D^{n+1} of the current cell and of the cell below in x, carried along x
-    T Dc[kVec], Dm[kVec];
+    T Dc[VW], Dm[VW];
     T fj_cell = T(1), fj_face = T(1), fj1_face = T(1);
     if (FUSED) {
         const int64_t b0 = (int64_t)i_begin * s.plane + column;
-        Vec4<T>::ldg(a.ld + b0, Dc);
+        VecW<T, VW>::ldg(a.ld + b0, Dc);
 #pragma unroll
-        for (int e = 0; e < kVec; e++) Dm[e] = T(0);
-        if (i_begin > 0) Vec4<T>::ldg(a.ld + b0 - s.plane, Dm);
+        for (int e = 0; e < VW; e++) Dm[e] = T(0);
+        if (i_begin > 0) VecW<T, VW>::ldg(a.ld + b0 - s.plane, Dm);
         if (LAYER) {
             fj_cell = __ldg(s.cell[1] + j);
             fj_face = __ldg(s.face[1] + j);
             fj1_face = __ldg(s.face[1] + j + 1);
         }
-        T V[kVec];
-        Vec4<T>::ldg(a.lvx + b0, V);
+        T V[VW];
+        VecW<T, VW>::ldg(a.lvx + b0, V);
         const T fi_face = LAYER ? __ldg(s.face[0] + i_begin) : T(1);
 #pragma unroll
-        for (int e = 0; e < kVec; e++)
+        for (int e = 0; e < VW; e++)
             XL[e] = k0 + e < s.nz ? adjoint_face<T, LAYER>(V[e], Dm[e], Dc[e], fi_face, fj_cell,
                                                            LAYER ? __ldg(s.cell[2] + k0 + e) : T(1))
                                   : V[e];
     } else {
-        Vec4<T>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
+        VecW<T, VW>::ldg(a.lvx + (int64_t)i_begin * s.plane + column, XL);
     }
     for (int i = i_begin; i < i_end; i++) {
         const int64_t base = (int64_t)i * s.plane + column;
@@ -2342,34 +2352,34 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
                 for (int r = 0; r <= NR; r++) prefetch_l2(h + r * s.field);
             }
         }
-        T XH[kVec], YL[kVec], YH[kVec], Z[kVec], L[kVec], LS[NR > 0 ? NR : 1][kVec];
+        T XH[VW], YL[VW], YH[VW], Z[VW], L[VW], LS[NR > 0 ? NR : 1][VW];
         T above;
-        T Dxp[kVec];   // FUSED: lambda_D^{n+1} of the next plane
+        T Dxp[VW];   // FUSED: lambda_D^{n+1} of the next plane
         if (FUSED) {
-            T Dy[kVec], Dyp[kVec], VXp[kVec], VY[kVec], VYp[kVec], VZ[kVec];
+            T Dy[VW], Dyp[VW], VXp[VW], VY[VW], VYp[VW], VZ[VW];
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
+            for (int e = 0; e < VW; e++) {
                 Dxp[e] = T(0);
                 Dy[e] = T(0);
                 Dyp[e] = T(0);
             }
-            if (i + 1 < s.nx) Vec4<T>::ldg(a.ld + base + s.plane, Dxp);
-            if (j > 0) Vec4<T>::ldg(a.ld + base - s.pz, Dy);
-            if (j + 1 < s.ny) Vec4<T>::ldg(a.ld + base + s.pz, Dyp);
+            if (i + 1 < s.nx) VecW<T, VW>::ldg(a.ld + base + s.plane, Dxp);
+            if (j > 0) VecW<T, VW>::ldg(a.ld + base - s.pz, Dy);
+            if (j + 1 < s.ny) VecW<T, VW>::ldg(a.ld + base + s.pz, Dyp);
             const T d_below = k0 > 0 ? __ldg(a.ld + base - 1) : T(0);
-            const T d_above = k0 + kVec < s.nz ? __ldg(a.ld + base + kVec) : T(0);
-            Vec4<T>::ldg(a.lvx + base + s.plane, VXp);
-            Vec4<T>::ldg(a.lvy + base, VY);
-            Vec4<T>::ldg(a.lvy + base + s.pz, VYp);
-            Vec4<T>::ldg(a.lvz + base, VZ);
-            const T vz_above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+            const T d_above = k0 + VW < s.nz ? __ldg(a.ld + base + VW) : T(0);
+            VecW<T, VW>::ldg(a.lvx + base + s.plane, VXp);
+            VecW<T, VW>::ldg(a.lvy + base, VY);
+            VecW<T, VW>::ldg(a.lvy + base + s.pz, VYp);
+            VecW<T, VW>::ldg(a.lvz + base, VZ);
+            const T vz_above = has_above ? __ldg(a.lvz + base + VW) : T(0);
             T fi_cell = T(1), fi1_face = T(1);
             if (LAYER) {
                 fi_cell = __ldg(s.cell[0] + i);
                 fi1_face = __ldg(s.face[0] + i + 1);
             }
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
+            for (int e = 0; e < VW; e++) {
                 const int k = k0 + e;
                 const T gk_cell = LAYER ? __ldg(s.cell[2] + min(k, s.nz - 1)) : T(1);
                 if (k < s.nz) {
@@ -2393,26 +2403,26 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
             }
             above = T(0);
             if (has_above)
-                above = adjoint_face<T, LAYER>(vz_above, Dc[kVec - 1], d_above, fi_cell, fj_cell,
-                                               LAYER ? __ldg(s.face[2] + k0 + kVec) : T(1));
+                above = adjoint_face<T, LAYER>(vz_above, Dc[VW - 1], d_above, fi_cell, fj_cell,
+                                               LAYER ? __ldg(s.face[2] + k0 + VW) : T(1));
         } else {
-            Vec4<T>::ldg(a.lvx + base + s.plane, XH);
-            Vec4<T>::ldg(a.lvy + base, YL);
-            Vec4<T>::ldg(a.lvy + base + s.pz, YH);
-            Vec4<T>::ldg(a.lvz + base, Z);
-            above = has_above ? __ldg(a.lvz + base + kVec) : T(0);
+            VecW<T, VW>::ldg(a.lvx + base + s.plane, XH);
+            VecW<T, VW>::ldg(a.lvy + base, YL);
+            VecW<T, VW>::ldg(a.lvy + base + s.pz, YH);
+            VecW<T, VW>::ldg(a.lvz + base, Z);
+            above = has_above ? __ldg(a.lvz + base + VW) : T(0);
         }
-        Vec4<T>::load(a.lp + base, L);
+        VecW<T, VW>::load(a.lp + base, L);
 #pragma unroll
-        for (int r = 0; r < NR; r++) Vec4<T>::load(a.lpsi + r * s.field + base, LS[r]);
-        T HD[kVec], HS[NR > 0 ? NR : 1][kVec];
+        for (int r = 0; r < NR; r++) VecW<T, VW>::load(a.lpsi + r * s.field + base, LS[r]);
+        T HD[VW], HS[NR > 0 ? NR : 1][VW];
         constexpr bool air = AIR && NR > 0;
         if (air) {
             const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
             const T *h = a.hist.fields + slot * (1 + NR) * s.field + base;
-            Vec4<T>::ldg(h, HD);
+            VecW<T, VW>::ldg(h, HD);
 #pragma unroll
-            for (int r = 0; r < NR; r++) Vec4<T>::ldg(h + (1 + r) * s.field, HS[r]);
+            for (int r = 0; r < NR; r++) VecW<T, VW>::ldg(h + (1 + r) * s.field, HS[r]);
         }
         T fi = T(1), fj = T(1);
         if (LAYER) {
@@ -2420,11 +2430,11 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
             fj = __ldg(s.cell[1] + j);
         }
         // lambda(p^{n+1}): the interior-face divergence of mu^{n+1}, plus dL/drec[n]
-        T LPn[kVec];
+        T LPn[VW];
 #pragma unroll
-        for (int e = 0; e < kVec; e++) {
+        for (int e = 0; e < VW; e++) {
             const int k = k0 + e;
-            const T up = e + 1 < kVec ? Z[e + 1] : above;
+            const T up = e + 1 < VW ? Z[e + 1] : above;
             T dmu = (i + 1 < s.nx ? XH[e] : T(0)) - (i > 0 ? XL[e] : T(0));
             dmu = dmu + ((j + 1 < s.ny ? YH[e] : T(0)) - (j > 0 ? YL[e] : T(0)));
             dmu = dmu + ((k + 1 < s.nz ? up : T(0)) - (k > 0 ? Z[e] : T(0)));
@@ -2438,10 +2448,10 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
                     m &= m - 1;
                 }
                 const int64_t d = s.rec_off[r] - base;
-                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                if (d >= 0 && d < VW && step >= s.rec_start[r]) {
                     const T g = (T)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
 #pragma unroll
-                    for (int e = 0; e < kVec; e++)
+                    for (int e = 0; e < VW; e++)
                         if (e == d) LPn[e] = LPn[e] + g;
                 }
             }
@@ -2452,19 +2462,19 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
                     m &= m - 1;
                 }
                 const int64_t d = s.src_off[q] - base;
-                if (d >= 0 && d < kVec && step < s.src_len[q]) {
+                if (d >= 0 && d < VW && step < s.src_len[q]) {
                     T v = LPn[0];
 #pragma unroll
-                    for (int e = 1; e < kVec; e++)
+                    for (int e = 1; e < VW; e++)
                         if (e == d) v = LPn[e];
                     a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
                 }
             }
         }
         const bool boundary = wall_column || i == 0 || i == s.nx - 1;
-        T LD[kVec];
+        T LD[VW];
 #pragma unroll
-        for (int e = 0; e < kVec; e++) {
+        for (int e = 0; e < VW; e++) {
             const int k = k0 + e;
             LD[e] = T(0);
             if (k >= s.nz) continue;
@@ -2511,32 +2521,34 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
             L[e] = lpart;
             LD[e] = ld;
         }
-        Vec4<T>::store(a.lp + base, L);
+        VecW<T, VW>::store(a.lp + base, L);
 #pragma unroll
-        for (int r = 0; r < NR; r++) Vec4<T>::store(a.lpsi + r * s.field + base, LS[r]);
+        for (int r = 0; r < NR; r++) VecW<T, VW>::store(a.lpsi + r * s.field + base, LS[r]);
         if (FUSED) {
-            Vec4<T>::store(a.out_d + base, LD);
-            Vec4<T>::store(a.out_vx + base, XL);
-            Vec4<T>::store(a.out_vy + base, YL);
-            Vec4<T>::store(a.out_vz + base, Z);
-            if (i == s.nx - 1) Vec4<T>::store(a.out_vx + base + s.plane, XH);
-            if (j == s.ny - 1) Vec4<T>::store(a.out_vy + base + s.pz, YH);
-            if (k0 + kVec == s.nz) a.out_vz[base + kVec] = above;
+            VecW<T, VW>::store(a.out_d + base, LD);
+            VecW<T, VW>::store(a.out_vx + base, XL);
+            VecW<T, VW>::store(a.out_vy + base, YL);
+            VecW<T, VW>::store(a.out_vz + base, Z);
+            if (i == s.nx - 1) VecW<T, VW>::store(a.out_vx + base + s.plane, XH);
+            if (j == s.ny - 1) VecW<T, VW>::store(a.out_vy + base + s.pz, YH);
+            if (k0 + VW == s.nz) a.out_vz[base + VW] = above;
 #pragma unroll
-            for (int e = 0; e < kVec; e++) {
+            for (int e = 0; e < VW; e++) {
                 Dm[e] = Dc[e];
                 Dc[e] = Dxp[e];
             }
         } else {
-            Vec4<T>::store(a.ld + base, LD);
+            VecW<T, VW>::store(a.ld + base, LD);
         }
 #pragma unroll
-        for (int e = 0; e < kVec; e++) XL[e] = XH[e];
+        for (int e = 0; e < VW; e++) XL[e] = XH[e];
     }
 }
 
-template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
-__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 2 : 4)))
+// VW: z elements per thread (4, or 2 for the air-gradient variants: their per-thread arrays and
+// sums otherwise hold the SM to 16 warps, and the step waits on its loads).
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR, int VW = kVec>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR && VW == kVec ? 1 : 2) : (AIR && VW == kVec ? 2 : 4)))
     adjoint_pressure_sweep(const AdjointParams<T> a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -2546,10 +2558,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 
     T air_acc[NA];
 #pragma unroll
     for (int t = 0; t < NA; t++) air_acc[t] = T(0);
-    if (c < a.room.nchunks && j < a.room.ny) {
+    if (c < (a.room.nz + VW - 1) / VW && j < a.room.ny) {
         const int i_begin = blockIdx.z * a.planes;
-        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR>(a, i_begin, min(a.room.nx, i_begin + a.planes),
-                                                          j, c, *a.step_base + a.local_step, air_acc);
+        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR, false, VW>(a, i_begin, min(a.room.nx, i_begin + a.planes),
+                                                                     j, c, *a.step_base + a.local_step, air_acc);
     }
     if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
         __shared__ double red[NA][8];
@@ -2573,8 +2585,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 
 }
 
 // The face sweep of forward step n + 1 and the cell sweep of step n in one launch (FUSED above).
-template <typename T, bool LAYER, bool WALLS, int NR, bool AIR>
-__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 2 : 3)))
+template <typename T, bool LAYER, bool WALLS, int NR, bool AIR, int VW = kVec>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR && VW == kVec ? 1 : 2) : (AIR && VW == kVec ? 2 : 3)))
     adjoint_fused_sweep(const AdjointParams<T> a) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -2584,10 +2596,10 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR ? 1 : 2) : (AIR ? 
     T air_acc[NA];
 #pragma unroll
     for (int t = 0; t < NA; t++) air_acc[t] = T(0);
-    if (c < a.room.nchunks && j < a.room.ny) {
+    if (c < (a.room.nz + VW - 1) / VW && j < a.room.ny) {
         const int i_begin = blockIdx.z * a.planes;
-        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR, true>(a, i_begin, min(a.room.nx, i_begin + a.planes),
-                                                          j, c, *a.step_base + a.local_step, air_acc);
+        adjoint_pressure_column<T, LAYER, WALLS, NR, AIR, true, VW>(a, i_begin, min(a.room.nx, i_begin + a.planes),
+                                                                    j, c, *a.step_base + a.local_step, air_acc);
     }
     if (AIR && NR > 0) {  // uniform per launch: every thread reaches the barrier
         __shared__ double red[NA][8];
@@ -3343,9 +3355,9 @@ struct LaunchShape {
     dim3 grid, block;
 };
 
-LaunchShape single_shape(const acf_batch *b) {
+LaunchShape single_shape(const acf_batch *b, int width = kVec) {
     const RoomHost &h = b->rooms[0];
-    const int nchunks = (int)((h.nz + kVec - 1) / kVec);
+    const int nchunks = (int)((h.nz + width - 1) / width);
     int bx = 1;
     while (bx < nchunks && bx < 32) bx <<= 1;
     int by = std::max(1, std::min<int>(h.ny, b->block_threads / bx));
@@ -4639,11 +4651,12 @@ struct AdjPressure {
     }
 };
 
+// The air-gradient launches use two z elements per thread (launch shape single_shape_w(b, 2)).
 template <typename T, bool L, bool W, int NR>
 struct AdjPressureAir {
     static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
-        if (NR > 0) adjoint_pressure_sweep<T, L, W, NR, NR != 0><<<g, b, 0, st>>>(p);
-        else adjoint_pressure_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
+        if (NR > 0) adjoint_pressure_sweep<T, L, W, NR, NR != 0, 2><<<g, b, 0, st>>>(p);
+        else adjoint_pressure_sweep<T, L, W, NR, false, 2><<<g, b, 0, st>>>(p);
     }
 };
 
@@ -4657,8 +4670,8 @@ struct AdjFused {
 template <typename T, bool L, bool W, int NR>
 struct AdjFusedAir {
     static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
-        if (NR > 0) adjoint_fused_sweep<T, L, W, NR, NR != 0><<<g, b, 0, st>>>(p);
-        else adjoint_fused_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
+        if (NR > 0) adjoint_fused_sweep<T, L, W, NR, NR != 0, 2><<<g, b, 0, st>>>(p);
+        else adjoint_fused_sweep<T, L, W, NR, false, 2><<<g, b, 0, st>>>(p);
     }
 };
 
@@ -4822,7 +4835,8 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     ACF_CUDA(cudaMemsetAsync(A.fields, 0, adj_bytes, st));
     if (A.grad_shell) ACF_CUDA(cudaMemsetAsync(A.grad_shell, 0, A.shell_total * sizeof(double), st));
     const LaunchShape L = single_shape(b);
-    const int64_t blocks = (int64_t)L.grid.x * L.grid.y * L.grid.z;
+    const LaunchShape LA = air ? single_shape(b, 2) : L;   // the air launches: 2 z elements each
+    const int64_t blocks = (int64_t)LA.grid.x * LA.grid.y * LA.grid.z;
     const int NA = 3 * h.n_relax + 1;
     if (air) {
         if (A.air_blocks < blocks) {
@@ -4887,7 +4901,7 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     auto fused_unit = [&](int32_t local, cudaStream_t s, int par) {
         AdjointParams<T> q = par ? a1 : a0;
         q.local_step = local;
-        if (air) dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        if (air) dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, s);
         else dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
     };
     // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter),
@@ -4900,7 +4914,7 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
             set_step_base<<<1, 1, 0, st>>>(b->step_base, end - 1);
             AdjointParams<T> q = a0;
             q.local_step = 0;
-            if (air) dispatch_pressure<T, AdjPressureAir>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, st);
+            if (air) dispatch_pressure<T, AdjPressureAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, st);
             else dispatch_pressure<T, AdjPressure>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, st);
             b->launches += 2;
             end -= 1;
