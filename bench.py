@@ -38,22 +38,27 @@ METRIC = "Gcell-updates/s"
 N_RECEIVERS = 4
 
 
-def workload(size: int, seed: int = 2):
+def workload(size: int, seed: int = 2, walls_only: bool = False):
+    """The headline room; ``walls_only`` keeps its walls, source and receivers and drops the
+    sponge and the air (the room the pressure-only scheme can run)."""
     from ac_fdtd_b200.workloads import plain_room_large
 
     grid, objects, source, receivers = plain_room_large(size, seed, N_RECEIVERS)
+    if walls_only:
+        objects = dict(walls=objects["walls"])
     return grid, objects, [source, *receivers]
 
 
 def config_dict(args, grid) -> dict:
+    physics = ("" if getattr(args, "walls_only", False) else
+               "16-cell sponge on 2 x faces, ISO air 20C/50%RH (3 relaxation states), ")
     return {
-        "workload": f"plain-method room {grid.nx}^3 fp32, 6 walls alpha~U(0.05,0.5), "
-                    f"16-cell sponge on 2 x faces, ISO air 20C/50%RH (3 relaxation states), "
+        "workload": f"plain-method room {grid.nx}^3 fp32, 6 walls alpha~U(0.05,0.5), {physics}"
                     f"gaussian pulse 4 kHz, {N_RECEIVERS} receivers, {args.time_steps} steps "
                     f"per bench step",
         "cells": grid.n_cells,
         "time_steps_per_bench_step": args.time_steps,
-        "relaxation_states": 3,
+        "relaxation_states": 0 if getattr(args, "walls_only", False) else 3,
         "dtype": "float32",
         "l2": "inputs larger than L2 (fields 2.5 GB at 384^3); no flush",
         "parallelism": f"replicas x{args.gpus}",
@@ -324,7 +329,7 @@ def run_ours(args) -> None:
     from ac_fdtd_b200.autotune import _apply as apply_geometry
     from ac_fdtd_b200.autotune import apply_tuned
 
-    grid, objects, points = workload(args.size)
+    grid, objects, points = workload(args.size, walls_only=args.walls_only)
     solver = CudaAcousticFDTD(grid, dtype=np.float32, **objects)
     if args.launch:
         parts = args.launch.split(",")
@@ -373,21 +378,35 @@ def run_ours(args) -> None:
     cell_updates = grid.n_cells * T * args.steps * world
     value = cell_updates / (elapsed_ms * 1e-3) / 1e9
 
-    # ---- roofline of the dominant kernel: the fused step, or the pressure sweep
-    R = 3
+    # ---- roofline of the dominant kernel: the fused step, the pressure-only step, or the
+    # pressure sweep
+    R = 0 if args.walls_only else 3
     itemsize = 4
+    layer = "nolayer" if args.walls_only else "layer"
     peak, peak_kind = measured_peak_hbm()
     peak_source = (f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                    else "fallback 6650 GB/s")
     vel_avg = vel_ms / max(timed_steps, 1)
     pres_avg = pres_ms / max(timed_steps, 1)
-    if geometry[0] in ("fused", "staged"):
+    if geometry[0] == "pressure_only":
+        step_bytes = grid.n_cells * 3 * itemsize
+        step_avg = vel_avg + pres_avg          # one kernel; its time is in the first slot
+        achieved = step_bytes / (step_avg * 1e-3) / 1e9
+        traffic_per_cell = ncu_traffic_per_cell("pressure_only_sweep")
+        roofline = {
+            "bound": "hbm", "kernel": "pressure_only_sweep<float,walls>",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_source, "algorithmic_bytes_per_launch": step_bytes,
+            "bytes_per_cell": 3 * itemsize, "avg_launch_ms": step_avg,
+            "traffic": None if traffic_per_cell is None else traffic_per_cell * grid.n_cells,
+        }
+    elif geometry[0] in ("fused", "staged"):
         if geometry[0] == "staged":
-            kernel, label = "fused_staged_sweep", "fused_staged_sweep<float,layer,walls,3>"
+            kernel, label = "fused_staged_sweep", f"fused_staged_sweep<float,{layer},walls,{R}>"
         else:                      # single precision: the lean column
             kernel = "lean_sweep"
-            label = ("lean_sweep<layer,walls,3>" if grid.nz % 4 == 0
-                     else "lean_sweep_padded<layer,walls,3>")
+            label = (f"lean_sweep<{layer},walls,{R}>" if grid.nz % 4 == 0
+                     else f"lean_sweep_padded<{layer},walls,{R}>")
         step_bytes = grid.n_cells * (8 + 2 * R) * itemsize
         step_avg = vel_avg + pres_avg          # one kernel; its time is in the first slot
         achieved = step_bytes / (step_avg * 1e-3) / 1e9
@@ -435,6 +454,8 @@ def run_ours(args) -> None:
         # stream, torch's current one); set_state and get_state return after their copies.
         solver.step_index = 0
         marks[0].record()
+        if geometry[0] == "pressure_only":
+            solver.reset_state()          # its velocities are only taken before the first step
         h2d = solver.set_state(p=p0, velocity=v0, relaxation=psi0)
         marks[1].record()
         solver.run(T)
@@ -1114,6 +1135,9 @@ def main() -> None:
     parser.add_argument("--skip-extras", action="store_true",
                         help="skip the batched-room and adjoint-cost measurements")
     parser.add_argument("--batch-steps", type=int, default=3000)
+    parser.add_argument("--walls-only", action="store_true",
+                        help="the headline room without its sponge and air (for the "
+                             "pressure-only scheme, --launch pressure_only,128,8)")
     parser.add_argument("--launch", default="",
                         help="fixed geometry instead of the autotuner: 'two_sweeps|fused,threads,planes' "
                              "or 'staged,rows,stages,planes,vector'")
