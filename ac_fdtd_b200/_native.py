@@ -37,13 +37,15 @@ EXPORTED_SYMBOLS = (
     "acf_batch_energy_terms", "acf_batch_profile_enable", "acf_batch_profile_read",
     "acf_batch_launch_count", "acf_set_coefficients", "acf_adjoint_prepare",
     "acf_adjoint_shell_size", "acf_forward_record", "acf_adjoint_run", "acf_adjoint_download",
-    "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status", "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval", "acf_set_device",
+    "acf_reset_state", "acf_set_scheme", "acf_get_scheme", "acf_set_staging", "acf_device_status",
+    "acf_batch_set_scheme", "acf_adjoint_checkpoint_interval", "acf_set_device",
     "acf_batch_adjoint_prepare", "acf_batch_adjoint_shell_size", "acf_batch_forward_record",
     "acf_batch_adjoint_run", "acf_batch_reset_state", "acf_batch_set_coefficients",
     "acf_set_prefetch", "acf_get_prefetch", "acf_batch_set_prefetch", "acf_copy_plane",
     "acf_solver_device", "acf_energy_terms_planes", "acf_run_slabs", "acf_batch_device_status",
     "acf_set_wait_test", "acf_schroeder_decay", "acf_decay_fit", "acf_clarity",
-    "acf_spectral_divide", "acf_pressure_only_energy_terms",
+    "acf_spectral_divide", "acf_pressure_only_energy_terms", "acf_set_time_blocking",
+    "acf_get_time_blocking",
 )
 
 SCHEME_TWO_SWEEPS, SCHEME_FUSED, SCHEME_FUSED_STAGED, SCHEME_PRESSURE_ONLY = 0, 1, 2, 3
@@ -157,6 +159,8 @@ _SIGNATURES = {
     "acf_batch_set_coefficients": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(AcfConfig)]),
     "acf_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_get_prefetch": (ctypes.c_int, [_P]),
+    "acf_set_time_blocking": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "acf_get_time_blocking": (ctypes.c_int, [_P]),
     "acf_batch_set_prefetch": (ctypes.c_int, [_P, ctypes.c_int32]),
     "acf_copy_plane": (ctypes.c_int, [_P, _I64, _P, _I64, ctypes.c_int, _P]),
     "acf_solver_device": (ctypes.c_int, [_P]),

@@ -1489,50 +1489,300 @@ struct LeanParams {
 __device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
+// The per-column constants of a lean column: its place, its edges, its sources and receivers and
+// the y and z layer factors of its cells and faces.
+struct LeanColumn {
+    int j, k0, real;
+    int64_t column;                 // j * pz + k0
+    bool y_lo, y_hi, z_lo, z_hi;
+    bool tail;                      // a padding chunk (rows with nz not a multiple of 4)
+    bool wall_column, all_points, any_mine, damp_y, damp_z;
+    uint32_t points;
+    float fj_cell, fj_face, fj1_face, fkf4;
+    float2 fkc01, fkc23, fkf01, fkf23;
+};
+
 // ALIGNED: nz is a multiple of 4. Otherwise the last chunk of every row holds padding elements
 // (k >= nz), which this column leaves as they are, and the top face k = nz, which it damps
 // without a gradient update -- exactly as fused_column does -- with per-thread fix-ups that only
 // the threads of those chunks take.
-template <bool LAYER, bool WALLS, int NR, bool ALIGNED = true>
-__device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, int i_end, int j, int c,
-                                            int64_t step) {
-    const FusedParams<float> &f = g.f;
-    const Room<float> &s = f.room;
-    const int k0 = c * kVec;
-    const int64_t column = (int64_t)j * s.pz + k0;
-    const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
-    const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+template <bool LAYER, bool ALIGNED>
+__device__ __forceinline__ LeanColumn lean_setup(const Room<float> &s, int j, int c) {
+    LeanColumn col;
+    col.j = j;
+    col.k0 = c * kVec;
+    const int k0 = col.k0;
+    col.column = (int64_t)j * s.pz + k0;
+    col.y_lo = j > 0;
+    col.y_hi = j + 1 < s.ny;
+    col.z_lo = k0 > 0;
+    col.z_hi = k0 + kVec < s.nz;
     // Padding chunk: `real` elements (1..3) lie inside the room, the next one is the top face.
-    const bool tail = !ALIGNED && k0 + kVec > s.nz;
-    const int real = tail ? s.nz - k0 : kVec;
+    col.tail = !ALIGNED && k0 + kVec > s.nz;
+    col.real = col.tail ? s.nz - k0 : kVec;
     const bool any_point = (s.n_src | s.n_rec) != 0;
-    bool all_points = false;
-    const uint32_t points = any_point ? column_points(s, j, k0, all_points) : 0u;
-    const bool any_mine = points != 0 || all_points;
-    const bool wall_column = !y_lo || !y_hi || !z_lo || !z_hi;
-    const float2 cv2 = g.pairs[kPairCv], cp2 = g.pairs[kPairCp];
-    const float cv = cv2.x;
-
-    float fj_cell = 1.f, fj_face = 1.f, fj1_face = 1.f, fkf4 = 1.f;
-    float2 fkc01 = dup2(1.f), fkc23 = dup2(1.f), fkf01 = dup2(1.f), fkf23 = dup2(1.f);
-    bool damp_y = false, damp_z = false;
+    col.all_points = false;
+    col.points = any_point ? column_points(s, j, k0, col.all_points) : 0u;
+    col.any_mine = col.points != 0 || col.all_points;
+    col.wall_column = !col.y_lo || !col.y_hi || !col.z_lo || !col.z_hi;
+    col.fj_cell = col.fj_face = col.fj1_face = col.fkf4 = 1.f;
+    col.fkc01 = col.fkc23 = col.fkf01 = col.fkf23 = dup2(1.f);
+    col.damp_y = col.damp_z = false;
     if (LAYER) {
-        fj_cell = __ldg(s.cell[1] + j);
-        fj_face = __ldg(s.face[1] + j);
-        fj1_face = __ldg(s.face[1] + j + 1);
+        col.fj_cell = __ldg(s.cell[1] + j);
+        col.fj_face = __ldg(s.face[1] + j);
+        col.fj1_face = __ldg(s.face[1] + j + 1);
         // padding lanes take the last cell's and the top face's factors, as fused_column does
         const int c_last = s.nz - 1, f_last = s.nz;
         auto kc = [&](int e) { return __ldg(s.cell[2] + (ALIGNED ? k0 + e : min(k0 + e, c_last))); };
         auto kf = [&](int e) { return __ldg(s.face[2] + (ALIGNED ? k0 + e : min(k0 + e, f_last))); };
-        fkc01 = make_float2(kc(0), kc(1));
-        fkc23 = make_float2(kc(2), kc(3));
-        fkf01 = make_float2(kf(0), kf(1));
-        fkf23 = make_float2(kf(2), kf(3));
-        fkf4 = kf(4);
-        damp_y = fj_cell != 1.f || fj_face != 1.f || fj1_face != 1.f;
-        damp_z = fkc01.x != 1.f || fkc01.y != 1.f || fkc23.x != 1.f || fkc23.y != 1.f ||
-                 fkf01.x != 1.f || fkf01.y != 1.f || fkf23.x != 1.f || fkf23.y != 1.f || fkf4 != 1.f;
+        col.fkc01 = make_float2(kc(0), kc(1));
+        col.fkc23 = make_float2(kc(2), kc(3));
+        col.fkf01 = make_float2(kf(0), kf(1));
+        col.fkf23 = make_float2(kf(2), kf(3));
+        col.fkf4 = kf(4);
+        col.damp_y = col.fj_cell != 1.f || col.fj_face != 1.f || col.fj1_face != 1.f;
+        col.damp_z = col.fkc01.x != 1.f || col.fkc01.y != 1.f || col.fkc23.x != 1.f ||
+                     col.fkc23.y != 1.f || col.fkf01.x != 1.f || col.fkf01.y != 1.f ||
+                     col.fkf23.x != 1.f || col.fkf23.y != 1.f || col.fkf4 != 1.f;
     }
+    return col;
+}
+
+// The updated x face below the first plane i of a march: the face's velocity V moved by the
+// pressures P (plane i) and Q (plane i - 1, when i > 0), then damped.
+template <bool LAYER>
+__device__ __forceinline__ void lean_lower_face(const LeanParams &g, const LeanColumn &col, int i,
+                                                float4 V, float4 P, float4 Q, float2 &XL01,
+                                                float2 &XL23) {
+    const Room<float> &s = g.f.room;
+    const float2 cv2 = g.pairs[kPairCv];
+    XL01 = lo2(V);
+    XL23 = hi2(V);
+    if (i > 0) {
+        XL01 = sub2(XL01, mul2(cv2, sub2(lo2(P), lo2(Q))));
+        XL23 = sub2(XL23, mul2(cv2, sub2(hi2(P), hi2(Q))));
+    }
+    if (LAYER) {
+        const float fi_face = __ldg(s.face[0] + i);
+        if (fi_face != 1.f) {
+            XL01 = mul2(XL01, dup2(fi_face));
+            XL23 = mul2(XL23, dup2(fi_face));
+        }
+        if (col.damp_y) {
+            XL01 = mul2(XL01, dup2(col.fj_cell));
+            XL23 = mul2(XL23, dup2(col.fj_cell));
+        }
+        if (col.damp_z) {
+            XL01 = mul2(XL01, col.fkc01);
+            XL23 = mul2(XL23, col.fkc23);
+        }
+    }
+}
+
+// The state around one chunk at plane i before a step: its pressures P, the pressures next to it
+// (x + 1, y -+ 1, z below and above), and the velocities of its faces (x upper, y lower and
+// upper, z lower and the one above the chunk).
+struct LeanInputs {
+    float4 P, PX, PYm, PYp, VXo, VY, VYp, VZ;
+    float p_below, p_above, vz_above;
+};
+
+// The chunk's updated faces after the step: x upper, y lower and upper, z lower and above.
+struct LeanFaces {
+    float2 XH01, XH23, YL01, YL23, YH01, YH23, ZL01, ZL23;
+    float ZH3;
+};
+
+// One step of one chunk at plane i: from the state around it (`in`, the updated lower x face
+// XL and the relaxation states S, which it advances in place) to its updated faces and its next
+// pressures Pn, with walls, the sponge and the sources of `step`. `bad2` turns NaN once a
+// pressure produced is not finite.
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED>
+__device__ __forceinline__ void lean_update(const LeanParams &g, const LeanColumn &col, int i,
+                                            int64_t base, int64_t step, const LeanInputs &in,
+                                            float2 XL01, float2 XL23, float4 (&S)[NR > 0 ? NR : 1],
+                                            LeanFaces &o, float (&Pn)[kVec], float2 &bad2) {
+    const Room<float> &s = g.f.room;
+    const bool x_inner = i + 1 < s.nx;
+    const float2 cv2 = g.pairs[kPairCv], cp2 = g.pairs[kPairCp];
+    const float cv = cv2.x;
+    const bool tail = col.tail;
+    const int real = col.real;
+    float fi_cell = 1.f, fi1_face = 1.f;
+    if (LAYER) {
+        fi_cell = __ldg(s.cell[0] + i);
+        fi1_face = __ldg(s.face[0] + i + 1);
+    }
+
+    // ---- updated faces: x upper (carried on), y lower and upper, z lower and upper
+    const float4 P = in.P;
+    const float2 P01 = lo2(P), P23 = hi2(P);
+    float2 XH01 = lo2(in.VXo), XH23 = hi2(in.VXo);
+    if (x_inner) {
+        XH01 = sub2(XH01, mul2(cv2, sub2(lo2(in.PX), P01)));
+        XH23 = sub2(XH23, mul2(cv2, sub2(hi2(in.PX), P23)));
+    }
+    float2 YL01 = lo2(in.VY), YL23 = hi2(in.VY);
+    if (col.y_lo) {
+        YL01 = sub2(YL01, mul2(cv2, sub2(P01, lo2(in.PYm))));
+        YL23 = sub2(YL23, mul2(cv2, sub2(P23, hi2(in.PYm))));
+    }
+    float2 YH01 = lo2(in.VYp), YH23 = hi2(in.VYp);
+    if (col.y_hi) {
+        YH01 = sub2(YH01, mul2(cv2, sub2(lo2(in.PYp), P01)));
+        YH23 = sub2(YH23, mul2(cv2, sub2(hi2(in.PYp), P23)));
+    }
+    const float4 VZ = in.VZ;
+    float2 ZL01 = sub2(lo2(VZ), mul2(cv2, sub2(P01, make_float2(in.p_below, P.x))));
+    float2 ZL23 = sub2(hi2(VZ), mul2(cv2, sub2(P23, make_float2(P.y, P.z))));
+    if (!col.z_lo) ZL01.x = VZ.x;             // face k = 0: a boundary, never updated
+    if (tail) {                               // faces k >= nz: the top face and padding
+        if (real <= 1) ZL01.y = VZ.y;
+        if (real <= 2) ZL23.x = VZ.z;
+        ZL23.y = VZ.w;
+    }
+    float ZH3 = in.vz_above;
+    if (col.z_hi) ZH3 = ZH3 - cv * (in.p_above - P.w);
+    if (LAYER) {   // x, y, z order; an axis whose factors here are all 1 is skipped
+        if (fi_cell != 1.f || fi1_face != 1.f) {
+            const float2 a = dup2(fi1_face), b = dup2(fi_cell);
+            XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
+            YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
+            YH01 = mul2(YH01, b); YH23 = mul2(YH23, b);
+            ZL01 = mul2(ZL01, b); ZL23 = mul2(ZL23, b);
+            ZH3 = ZH3 * fi_cell;
+        }
+        if (col.damp_y) {
+            const float2 a = dup2(col.fj_cell), b = dup2(col.fj_face), e = dup2(col.fj1_face);
+            XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
+            YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
+            YH01 = mul2(YH01, e); YH23 = mul2(YH23, e);
+            ZL01 = mul2(ZL01, a); ZL23 = mul2(ZL23, a);
+            ZH3 = ZH3 * col.fj_cell;
+        }
+        if (col.damp_z) {
+            XH01 = mul2(XH01, col.fkc01); XH23 = mul2(XH23, col.fkc23);
+            YL01 = mul2(YL01, col.fkc01); YL23 = mul2(YL23, col.fkc23);
+            YH01 = mul2(YH01, col.fkc01); YH23 = mul2(YH23, col.fkc23);
+            ZL01 = mul2(ZL01, col.fkf01); ZL23 = mul2(ZL23, col.fkf23);
+            ZH3 = ZH3 * col.fkf4;
+        }
+    }
+
+    // ---- pressure, as the pressure sweep computes it
+    float2 d01 = sub2(XH01, XL01), d23 = sub2(XH23, XL23);
+    d01 = add2(d01, sub2(YH01, YL01));
+    d23 = add2(d23, sub2(YH23, YL23));
+    d01 = add2(d01, sub2(make_float2(ZL01.y, ZL23.x), ZL01));
+    d23 = add2(d23, sub2(make_float2(ZL23.y, ZH3), ZL23));
+    float2 pe01 = P01, pe23 = P23;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const float2 t01 = mul2(d01, g.pairs[kPairGain + r]), t23 = mul2(d23, g.pairs[kPairGain + r]);
+        const float2 o01 = sub2(lo2(S[r]), t01), o23 = sub2(hi2(S[r]), t23);
+        // offset * decay + target, and pe + offset * mean, as minus the negated products
+        const float2 n01 = sub2(t01, mul2(o01, g.pairs[kPairNegDecay + r]));
+        const float2 n23 = sub2(t23, mul2(o23, g.pairs[kPairNegDecay + r]));
+        pe01 = sub2(pe01, mul2(o01, g.pairs[kPairNegMean + r]));
+        pe23 = sub2(pe23, mul2(o23, g.pairs[kPairNegMean + r]));
+        float4 next = make_float4(n01.x, n01.y, n23.x, n23.y);
+        if (tail) {                           // padding lanes keep their state
+            if (real <= 1) next.y = S[r].y;
+            if (real <= 2) next.z = S[r].z;
+            next.w = S[r].w;
+        }
+        S[r] = next;
+    }
+    if (NR > 0) {
+        pe01 = sub2(pe01, mul2(d01, g.pairs[kPairNegRelaxScale]));
+        pe23 = sub2(pe23, mul2(d23, g.pairs[kPairNegRelaxScale]));
+    }
+    pe01 = sub2(pe01, mul2(d01, cp2));
+    pe23 = sub2(pe23, mul2(d23, cp2));
+    // Any non-finite p, v or psi reaches pe here; walls, damping and sources are finite.
+    bad2 = __ffma2_rn(pe01, dup2(0.f), bad2);
+    bad2 = __ffma2_rn(pe23, dup2(0.f), bad2);
+    Pn[0] = pe01.x;
+    Pn[1] = pe01.y;
+    Pn[2] = pe23.x;
+    Pn[3] = pe23.y;
+    if (WALLS && (col.wall_column || i == 0 || i == s.nx - 1)) {
+        const float Po[kVec] = {P.x, P.y, P.z, P.w};
+        column_walls(s, i, col.j, col.k0, real, [&](int e, float fu, float fp) {
+#pragma unroll
+            for (int q = 0; q < kVec; q++)
+                if (q == e) Pn[q] = Pn[q] * fu - Po[q] * fp;
+        });
+    }
+    if (LAYER) {
+        if (fi_cell != 1.f) {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * fi_cell;
+        }
+        if (col.damp_y) {
+#pragma unroll
+            for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * col.fj_cell;
+        }
+        if (col.damp_z) {
+            Pn[0] = Pn[0] * col.fkc01.x;
+            Pn[1] = Pn[1] * col.fkc01.y;
+            Pn[2] = Pn[2] * col.fkc23.x;
+            Pn[3] = Pn[3] * col.fkc23.y;
+        }
+    }
+    if (tail) {                               // padding lanes keep p
+        if (real <= 1) Pn[1] = P.y;
+        if (real <= 2) Pn[2] = P.z;
+        Pn[3] = P.w;
+    }
+    if (col.any_mine) add_sources(s, col.points, col.all_points, base, col.k0, step, Pn);
+    o.XH01 = XH01; o.XH23 = XH23;
+    o.YL01 = YL01; o.YL23 = YL23;
+    o.YH01 = YH01; o.YH23 = YH23;
+    o.ZL01 = ZL01; o.ZL23 = ZL23;
+    o.ZH3 = ZH3;
+}
+
+// The stores of one chunk's step at plane i: p, the three lower faces, the far boundary faces
+// and the relaxation states (to `psi`, n_relax fields of `field` elements). A slab's ghost planes
+// get their p from the neighbours' sweeps, never from their own; its boundary planes also go to
+// the neighbours' ghost planes (in their next copies).
+template <int NR, bool ALIGNED>
+__device__ __forceinline__ void lean_store(const LeanParams &g, const LeanColumn &col, int i,
+                                           int64_t base, const float (&Pn)[kVec], float2 XL01,
+                                           float2 XL23, const LeanFaces &o, float4 VZ,
+                                           const float4 (&S)[NR > 0 ? NR : 1], float *psi) {
+    const FusedParams<float> &f = g.f;
+    const Room<float> &s = f.room;
+    const float4 pn4 = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
+    if (i >= s.own_lo && i < s.own_hi) *reinterpret_cast<float4 *>(f.np + base) = pn4;
+    if (s.ghost_lo != nullptr && i == s.own_lo) *reinterpret_cast<float4 *>(s.ghost_lo + col.column) = pn4;
+    if (s.ghost_hi != nullptr && i == s.own_hi - 1) *reinterpret_cast<float4 *>(s.ghost_hi + col.column) = pn4;
+    *reinterpret_cast<float4 *>(f.nvx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
+    *reinterpret_cast<float4 *>(f.nvy + base) = make_float4(o.YL01.x, o.YL01.y, o.YL23.x, o.YL23.y);
+    float4 ZS = make_float4(o.ZL01.x, o.ZL01.y, o.ZL23.x, o.ZL23.y);
+    if (col.tail) {                           // faces past the top one are padding
+        if (col.real <= 0) ZS.y = VZ.y;       // (never: real >= 1)
+        if (col.real <= 1) ZS.z = VZ.z;
+        if (col.real <= 2) ZS.w = VZ.w;
+    }
+    *reinterpret_cast<float4 *>(f.nvz + base) = ZS;
+    if (i + 1 >= s.nx)
+        *reinterpret_cast<float4 *>(f.nvx + base + s.plane) = make_float4(o.XH01.x, o.XH01.y, o.XH23.x, o.XH23.y);
+    if (!col.y_hi)
+        *reinterpret_cast<float4 *>(f.nvy + base + s.pz) = make_float4(o.YH01.x, o.YH01.y, o.YH23.x, o.YH23.y);
+    if (!col.z_hi && (ALIGNED || !col.tail)) f.nvz[base + kVec] = o.ZH3;
+#pragma unroll
+    for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(psi + r * s.field + base) = S[r];
+}
+
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED = true>
+__device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, int i_end, int j, int c,
+                                            int64_t step) {
+    const Room<float> &s = g.f.room;
+    const LeanColumn col = lean_setup<LAYER, ALIGNED>(s, j, c);
+    const int64_t column = col.column;
 
     // Carried from plane to plane: p(i) and the updated vx on face i.
     float4 P;
@@ -1542,28 +1792,9 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         const int64_t base = (int64_t)i_begin * s.plane + column;
         P = __ldg(reinterpret_cast<const float4 *>(s.p + base));
         const float4 V = __ldg(reinterpret_cast<const float4 *>(s.vx + base));
-        XL01 = lo2(V);
-        XL23 = hi2(V);
-        if (i_begin > 0) {
-            const float4 Q = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.plane));
-            XL01 = sub2(XL01, mul2(cv2, sub2(lo2(P), lo2(Q))));
-            XL23 = sub2(XL23, mul2(cv2, sub2(hi2(P), hi2(Q))));
-        }
-        if (LAYER) {
-            const float fi_face = __ldg(s.face[0] + i_begin);
-            if (fi_face != 1.f) {
-                XL01 = mul2(XL01, dup2(fi_face));
-                XL23 = mul2(XL23, dup2(fi_face));
-            }
-            if (damp_y) {
-                XL01 = mul2(XL01, dup2(fj_cell));
-                XL23 = mul2(XL23, dup2(fj_cell));
-            }
-            if (damp_z) {
-                XL01 = mul2(XL01, fkc01);
-                XL23 = mul2(XL23, fkc23);
-            }
-        }
+        float4 Q = P;
+        if (i_begin > 0) Q = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.plane));
+        lean_lower_face<LAYER>(g, col, i_begin, V, P, Q, XL01, XL23);
     }
 
     for (int i = i_begin; i < i_end; i++) {
@@ -1579,172 +1810,32 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
             for (int r = 0; r < NR; r++) prefetch_l2(s.psi + r * s.field + next);
         }
         // ---- loads (all read-only: the next state goes to the other buffer)
-        float4 PX = P, PYm = P, PYp = P;
-        if (x_inner) PX = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.plane));
-        const float4 VXo = __ldg(reinterpret_cast<const float4 *>(s.vx + base + s.plane));
-        if (y_lo) PYm = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.pz));
-        if (y_hi) PYp = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.pz));
-        const float4 VY = __ldg(reinterpret_cast<const float4 *>(s.vy + base));
-        const float4 VYp = __ldg(reinterpret_cast<const float4 *>(s.vy + base + s.pz));
-        const float4 VZ = __ldg(reinterpret_cast<const float4 *>(s.vz + base));
-        const float p_below = z_lo ? __ldg(s.p + base - 1) : 0.f;
-        const float p_above = z_hi ? __ldg(s.p + base + kVec) : 0.f;
+        LeanInputs in;
+        in.P = P;
+        in.PX = in.PYm = in.PYp = P;
+        if (x_inner) in.PX = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.plane));
+        in.VXo = __ldg(reinterpret_cast<const float4 *>(s.vx + base + s.plane));
+        if (col.y_lo) in.PYm = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.pz));
+        if (col.y_hi) in.PYp = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.pz));
+        in.VY = __ldg(reinterpret_cast<const float4 *>(s.vy + base));
+        in.VYp = __ldg(reinterpret_cast<const float4 *>(s.vy + base + s.pz));
+        in.VZ = __ldg(reinterpret_cast<const float4 *>(s.vz + base));
+        in.p_below = col.z_lo ? __ldg(s.p + base - 1) : 0.f;
+        in.p_above = col.z_hi ? __ldg(s.p + base + kVec) : 0.f;
         // face k0 + 4: inside the row when k0 + 4 <= nz (always when ALIGNED)
-        const float vz_above = (ALIGNED || !tail) ? __ldg(s.vz + base + kVec) : 0.f;
+        in.vz_above = (ALIGNED || !col.tail) ? __ldg(s.vz + base + kVec) : 0.f;
         float4 S[NR > 0 ? NR : 1];
 #pragma unroll
         for (int r = 0; r < NR; r++) S[r] = *reinterpret_cast<const float4 *>(s.psi + r * s.field + base);
-        float fi_cell = 1.f, fi1_face = 1.f;
-        if (LAYER) {
-            fi_cell = __ldg(s.cell[0] + i);
-            fi1_face = __ldg(s.face[0] + i + 1);
-        }
 
-        // ---- updated faces: x upper (carried on), y lower and upper, z lower and upper
-        const float2 P01 = lo2(P), P23 = hi2(P);
-        float2 XH01 = lo2(VXo), XH23 = hi2(VXo);
-        if (x_inner) {
-            XH01 = sub2(XH01, mul2(cv2, sub2(lo2(PX), P01)));
-            XH23 = sub2(XH23, mul2(cv2, sub2(hi2(PX), P23)));
-        }
-        float2 YL01 = lo2(VY), YL23 = hi2(VY);
-        if (y_lo) {
-            YL01 = sub2(YL01, mul2(cv2, sub2(P01, lo2(PYm))));
-            YL23 = sub2(YL23, mul2(cv2, sub2(P23, hi2(PYm))));
-        }
-        float2 YH01 = lo2(VYp), YH23 = hi2(VYp);
-        if (y_hi) {
-            YH01 = sub2(YH01, mul2(cv2, sub2(lo2(PYp), P01)));
-            YH23 = sub2(YH23, mul2(cv2, sub2(hi2(PYp), P23)));
-        }
-        float2 ZL01 = sub2(lo2(VZ), mul2(cv2, sub2(P01, make_float2(p_below, P.x))));
-        float2 ZL23 = sub2(hi2(VZ), mul2(cv2, sub2(P23, make_float2(P.y, P.z))));
-        if (!z_lo) ZL01.x = VZ.x;                 // face k = 0: a boundary, never updated
-        if (tail) {                               // faces k >= nz: the top face and padding
-            if (real <= 1) ZL01.y = VZ.y;
-            if (real <= 2) ZL23.x = VZ.z;
-            ZL23.y = VZ.w;
-        }
-        float ZH3 = vz_above;
-        if (z_hi) ZH3 = ZH3 - cv * (p_above - P.w);
-        if (LAYER) {   // x, y, z order; an axis whose factors here are all 1 is skipped
-            if (fi_cell != 1.f || fi1_face != 1.f) {
-                const float2 a = dup2(fi1_face), b = dup2(fi_cell);
-                XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
-                YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
-                YH01 = mul2(YH01, b); YH23 = mul2(YH23, b);
-                ZL01 = mul2(ZL01, b); ZL23 = mul2(ZL23, b);
-                ZH3 = ZH3 * fi_cell;
-            }
-            if (damp_y) {
-                const float2 a = dup2(fj_cell), b = dup2(fj_face), e = dup2(fj1_face);
-                XH01 = mul2(XH01, a); XH23 = mul2(XH23, a);
-                YL01 = mul2(YL01, b); YL23 = mul2(YL23, b);
-                YH01 = mul2(YH01, e); YH23 = mul2(YH23, e);
-                ZL01 = mul2(ZL01, a); ZL23 = mul2(ZL23, a);
-                ZH3 = ZH3 * fj_cell;
-            }
-            if (damp_z) {
-                XH01 = mul2(XH01, fkc01); XH23 = mul2(XH23, fkc23);
-                YL01 = mul2(YL01, fkc01); YL23 = mul2(YL23, fkc23);
-                YH01 = mul2(YH01, fkc01); YH23 = mul2(YH23, fkc23);
-                ZL01 = mul2(ZL01, fkf01); ZL23 = mul2(ZL23, fkf23);
-                ZH3 = ZH3 * fkf4;
-            }
-        }
-
-        // ---- pressure, as the pressure sweep computes it
-        float2 d01 = sub2(XH01, XL01), d23 = sub2(XH23, XL23);
-        d01 = add2(d01, sub2(YH01, YL01));
-        d23 = add2(d23, sub2(YH23, YL23));
-        d01 = add2(d01, sub2(make_float2(ZL01.y, ZL23.x), ZL01));
-        d23 = add2(d23, sub2(make_float2(ZL23.y, ZH3), ZL23));
-        float2 pe01 = P01, pe23 = P23;
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-            const float2 t01 = mul2(d01, g.pairs[kPairGain + r]), t23 = mul2(d23, g.pairs[kPairGain + r]);
-            const float2 o01 = sub2(lo2(S[r]), t01), o23 = sub2(hi2(S[r]), t23);
-            // offset * decay + target, and pe + offset * mean, as minus the negated products
-            const float2 n01 = sub2(t01, mul2(o01, g.pairs[kPairNegDecay + r]));
-            const float2 n23 = sub2(t23, mul2(o23, g.pairs[kPairNegDecay + r]));
-            pe01 = sub2(pe01, mul2(o01, g.pairs[kPairNegMean + r]));
-            pe23 = sub2(pe23, mul2(o23, g.pairs[kPairNegMean + r]));
-            float4 next = make_float4(n01.x, n01.y, n23.x, n23.y);
-            if (tail) {                           // padding lanes keep their state
-                if (real <= 1) next.y = S[r].y;
-                if (real <= 2) next.z = S[r].z;
-                next.w = S[r].w;
-            }
-            S[r] = next;
-        }
-        if (NR > 0) {
-            pe01 = sub2(pe01, mul2(d01, g.pairs[kPairNegRelaxScale]));
-            pe23 = sub2(pe23, mul2(d23, g.pairs[kPairNegRelaxScale]));
-        }
-        pe01 = sub2(pe01, mul2(d01, cp2));
-        pe23 = sub2(pe23, mul2(d23, cp2));
-        // Any non-finite p, v or psi reaches pe here; walls, damping and sources are finite.
-        bad2 = __ffma2_rn(pe01, dup2(0.f), bad2);
-        bad2 = __ffma2_rn(pe23, dup2(0.f), bad2);
-        float Pn[kVec] = {pe01.x, pe01.y, pe23.x, pe23.y};
-        if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
-            const float Po[kVec] = {P.x, P.y, P.z, P.w};
-            column_walls(s, i, j, k0, real, [&](int e, float fu, float fp) {
-#pragma unroll
-                for (int q = 0; q < kVec; q++)
-                    if (q == e) Pn[q] = Pn[q] * fu - Po[q] * fp;
-            });
-        }
-        if (LAYER) {
-            if (fi_cell != 1.f) {
-#pragma unroll
-                for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * fi_cell;
-            }
-            if (damp_y) {
-#pragma unroll
-                for (int e = 0; e < kVec; e++) Pn[e] = Pn[e] * fj_cell;
-            }
-            if (damp_z) {
-                Pn[0] = Pn[0] * fkc01.x;
-                Pn[1] = Pn[1] * fkc01.y;
-                Pn[2] = Pn[2] * fkc23.x;
-                Pn[3] = Pn[3] * fkc23.y;
-            }
-        }
-        if (tail) {                               // padding lanes keep p
-            if (real <= 1) Pn[1] = P.y;
-            if (real <= 2) Pn[2] = P.z;
-            Pn[3] = P.w;
-        }
-        if (any_mine) add_sources(s, points, all_points, base, k0, step, Pn);
-
-        // ---- stores: p, the three lower faces, the far boundary faces, psi in place
-        // A slab's ghost planes get their p from the neighbours' sweeps, never from their own;
-        // its boundary planes also go to the neighbours' ghost planes (in their next copies).
-        const float4 pn4 = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
-        if (i >= s.own_lo && i < s.own_hi) *reinterpret_cast<float4 *>(f.np + base) = pn4;
-        if (s.ghost_lo != nullptr && i == s.own_lo) *reinterpret_cast<float4 *>(s.ghost_lo + column) = pn4;
-        if (s.ghost_hi != nullptr && i == s.own_hi - 1) *reinterpret_cast<float4 *>(s.ghost_hi + column) = pn4;
-        *reinterpret_cast<float4 *>(f.nvx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
-        *reinterpret_cast<float4 *>(f.nvy + base) = make_float4(YL01.x, YL01.y, YL23.x, YL23.y);
-        float4 ZS = make_float4(ZL01.x, ZL01.y, ZL23.x, ZL23.y);
-        if (tail) {                               // faces past the top one are padding
-            if (real <= 0) ZS.y = VZ.y;           // (never: real >= 1)
-            if (real <= 1) ZS.z = VZ.z;
-            if (real <= 2) ZS.w = VZ.w;
-        }
-        *reinterpret_cast<float4 *>(f.nvz + base) = ZS;
-        if (!x_inner)
-            *reinterpret_cast<float4 *>(f.nvx + base + s.plane) = make_float4(XH01.x, XH01.y, XH23.x, XH23.y);
-        if (!y_hi)
-            *reinterpret_cast<float4 *>(f.nvy + base + s.pz) = make_float4(YH01.x, YH01.y, YH23.x, YH23.y);
-        if (!z_hi && (ALIGNED || !tail)) f.nvz[base + kVec] = ZH3;
-#pragma unroll
-        for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(s.psi + r * s.field + base) = S[r];
-        if (any_mine) record_receivers(s, points, all_points, base, step, Pn);
-        XL01 = XH01;
-        XL23 = XH23;
-        P = PX;
+        LeanFaces o;
+        float Pn[kVec];
+        lean_update<LAYER, WALLS, NR, ALIGNED>(g, col, i, base, step, in, XL01, XL23, S, o, Pn, bad2);
+        lean_store<NR, ALIGNED>(g, col, i, base, Pn, XL01, XL23, o, in.VZ, S, s.psi);
+        if (col.any_mine) record_receivers(s, col.points, col.all_points, base, step, Pn);
+        XL01 = o.XH01;
+        XL23 = o.XH23;
+        P = in.PX;
     }
     report_nonfinite(s.status, bad2.x != bad2.x || bad2.y != bad2.y);
 }
@@ -1775,6 +1866,212 @@ __global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR)) lean_swee
 template <bool LAYER, bool WALLS, int NR>
 __global__ void __maxnreg__(96) lean_sweep_padded(const LeanParams g) {
     lean_sweep_body<LAYER, WALLS, NR, false>(g);
+}
+
+// ------------------------------------------------------------------------------------------
+// Two steps per launch: temporal blocking of the lean column (the step after the fused sweep
+// that the reference's C backend names as its next one, c/acfdtd.c:12-14).
+//
+// One sweep reads the state of step n once and writes the state of step n + 2 once, so a cell
+// moves (8 + 2R) elements per two steps instead of per step. Each thread marches its column
+// through x and, at plane t, takes the first step at plane t and the second step at plane t - 1.
+// The second step needs the first step's pressures of the four neighbouring columns at plane
+// t - 1; every other input of it is the thread's own first-step result, kept in registers (the
+// updated faces, which every cell computes for all six of its faces), or the relaxation states,
+// parked in the output field (the only thread that touches that element is this one).
+//
+// The neighbours' first-step pressures travel through a ring of kPairRing x planes in global
+// memory (L2-resident: four planes of the room per x group). A CTA publishes "first step done
+// through plane t" with a release store after a block barrier; before its second step at plane
+// t - 1, four threads of warp 0 acquire the four neighbour CTAs' counters (y -+ 1, z -+ 1).
+// Counters only grow; the second step at t - 1 waits for plane t - 1 of the neighbours; the ring
+// slot written at plane t was last read by the neighbours' second step at t - 4, which precedes
+// their publication of plane t - 2, awaited at t - 1. So four slots suffice and no wait depends
+// on a later plane. The launch is cooperative (every CTA resident), and every wait is bounded:
+// one that runs out raises kStatusWaitTimeout in the room's status word and the thread stops
+// waiting; the kernel returns.
+//
+// The x range is cut into groups of planes, as the lean sweep's is; a group also takes the
+// first step at the plane before and the plane after its range (redundantly, without
+// publishing it), so that groups never wait on one another. Inputs come only from the read copy
+// of p and v and from the input relaxation states, outputs go only to the other copy and the
+// output states, so the redundant planes read nothing another group writes.
+//
+// Every value is produced by the lean column's own update, in the same order: two launches of
+// two steps equal four lean steps bit for bit.
+
+constexpr int kPairRing = 4;
+constexpr int kPairThreads = 128;
+
+struct PairParams {
+    LeanParams g;           // g.f.room: step n (p, v of the read copy; psi: the input states);
+                            // g.f.np, nvx, nvy, nvz: the copy that receives step n + 2
+    float *psi_out;         // relaxation states after the two steps
+    float *ring;            // first-step p: groups x kPairRing planes of the room's geometry
+    int32_t *progress;      // one counter per CTA, zero at launch
+    uint64_t wait_limit_ns;
+    // Test hook, neutral (-1) by default: the first CTA stops publishing from this plane on, so
+    // that its neighbours' bounded waits run out and the kernel returns with kStatusWaitTimeout.
+    int32_t stop_plane;
+    int32_t reserved;
+};
+
+__device__ __forceinline__ int32_t load_acquire(const int32_t *p) {
+    int32_t v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void store_release(int32_t *p, int32_t v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait for a counter to reach `target`: false when it did not within `limit_ns` nor
+// within kWaitLimitIterations polls.
+__device__ __forceinline__ bool wait_counter(const int32_t *counter, int32_t target, uint64_t limit_ns) {
+    if (load_acquire(counter) >= target) return true;
+    const uint64_t start = global_ns();
+    for (int it = 0; it < kWaitLimitIterations; it++) {
+        __nanosleep(32);
+        if (load_acquire(counter) >= target) return true;
+        if (global_ns() - start > limit_ns) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float4 f4(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(kPairThreads, 4) lean_pair_sweep(const PairParams q) {
+    const LeanParams &g = q.g;
+    const Room<float> &s = g.f.room;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool active = c < s.nchunks && j < s.ny;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int s0 = blockIdx.z * g.f.planes;              // second step: planes [s0, e0)
+    const int e0 = min(s.nx, s0 + g.f.planes);
+    const int a_lo = max(0, s0 - 1), a_hi = min(s.nx, e0 + 1);   // first step: [a_lo, a_hi)
+    float *ring = q.ring + (int64_t)blockIdx.z * kPairRing * s.plane;
+    const int cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    int watch = -1;                                      // the neighbour CTA this thread watches
+    if (tid == 0 && blockIdx.y > 0) watch = cta - (int)gridDim.x;
+    if (tid == 1 && blockIdx.y + 1 < gridDim.y) watch = cta + (int)gridDim.x;
+    if (tid == 2 && blockIdx.x > 0) watch = cta - 1;
+    if (tid == 3 && blockIdx.x + 1 < gridDim.x) watch = cta + 1;
+    bool waiting = watch >= 0;
+    const bool any_point = (s.n_src | s.n_rec) != 0;
+    const int64_t step = any_point ? (*g.f.step_base + g.f.local_step) : 0;
+
+    LeanColumn col{};
+    float4 P = make_float4(0.f, 0.f, 0.f, 0.f);          // p^n at plane t
+    float4 PA = P;                                       // p^{n+1} at plane t - 1
+    float2 XA01 = dup2(0.f), XA23 = XA01;                // v^{n+1/2} on the x face below plane t
+    float2 XB01 = XA01, XB23 = XA01;                     // v^{n+3/2} on the x face below plane t - 1
+    LeanFaces A{};                                       // the first step's faces at plane t - 1
+    float2 bad2 = dup2(0.f);
+    if (active) {
+        col = lean_setup<LAYER, true>(s, j, c);
+        const int64_t base = (int64_t)a_lo * s.plane + col.column;
+        P = __ldg(reinterpret_cast<const float4 *>(s.p + base));
+        const float4 V = __ldg(reinterpret_cast<const float4 *>(s.vx + base));
+        float4 Q = P;
+        if (a_lo > 0) Q = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.plane));
+        lean_lower_face<LAYER>(g, col, a_lo, V, P, Q, XA01, XA23);
+    }
+
+    for (int t = a_lo; t <= e0; t++) {
+        const bool first = t < a_hi, second = t - 1 >= s0;
+        // (1) the neighbours' first step through plane t - 1
+        if (second && waiting && !wait_counter(q.progress + watch, t, q.wait_limit_ns)) {
+            atomicOr(s.status, kStatusWaitTimeout);
+            waiting = false;
+        }
+        // (2) the first step at plane t
+        const float2 XO01 = XA01, XO23 = XA23;           // v^{n+1/2} below plane t
+        float4 PN = P;                                   // p^{n+1} at plane t
+        LeanFaces An{};
+        if (active && first) {
+            const int64_t base = (int64_t)t * s.plane + col.column;
+            const bool x_inner = t + 1 < s.nx;
+            if (s.prefetch && t + 1 < a_hi) {
+                const int64_t next = base + s.plane;
+                if (t + 2 < s.nx) prefetch_l2(s.p + next + s.plane);
+                prefetch_l2(s.vx + next + s.plane);
+                prefetch_l2(s.vy + next);
+                prefetch_l2(s.vz + next);
+#pragma unroll
+                for (int r = 0; r < NR; r++) prefetch_l2(s.psi + r * s.field + next);
+            }
+            LeanInputs in;
+            in.P = P;
+            in.PX = in.PYm = in.PYp = P;
+            if (x_inner) in.PX = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.plane));
+            in.VXo = __ldg(reinterpret_cast<const float4 *>(s.vx + base + s.plane));
+            if (col.y_lo) in.PYm = __ldg(reinterpret_cast<const float4 *>(s.p + base - s.pz));
+            if (col.y_hi) in.PYp = __ldg(reinterpret_cast<const float4 *>(s.p + base + s.pz));
+            in.VY = __ldg(reinterpret_cast<const float4 *>(s.vy + base));
+            in.VYp = __ldg(reinterpret_cast<const float4 *>(s.vy + base + s.pz));
+            in.VZ = __ldg(reinterpret_cast<const float4 *>(s.vz + base));
+            in.p_below = col.z_lo ? __ldg(s.p + base - 1) : 0.f;
+            in.p_above = col.z_hi ? __ldg(s.p + base + kVec) : 0.f;
+            in.vz_above = __ldg(s.vz + base + kVec);
+            float4 S[NR > 0 ? NR : 1];
+#pragma unroll
+            for (int r = 0; r < NR; r++) S[r] = __ldg(reinterpret_cast<const float4 *>(s.psi + r * s.field + base));
+            float Pn[kVec];
+            lean_update<LAYER, WALLS, NR, true>(g, col, t, base, step, in, XA01, XA23, S, An, Pn, bad2);
+            PN = make_float4(Pn[0], Pn[1], Pn[2], Pn[3]);
+            if (t >= s0 && t < e0) {                     // planes the second step visits
+                __stcg(reinterpret_cast<float4 *>(ring + (t % kPairRing) * s.plane + col.column), PN);
+#pragma unroll
+                for (int r = 0; r < NR; r++)
+                    *reinterpret_cast<float4 *>(q.psi_out + r * s.field + base) = S[r];
+                if (col.any_mine) record_receivers(s, col.points, col.all_points, base, step, Pn);
+            }
+            if (t == s0)                                 // the second step's x face below s0
+                lean_lower_face<LAYER>(g, col, s0, f4(XO01, XO23), PN, PA, XB01, XB23);
+            XA01 = An.XH01;
+            XA23 = An.XH23;
+            P = in.PX;
+        }
+        __syncthreads();
+        if (tid == 0 && first && !(cta == 0 && q.stop_plane >= 0 && t >= q.stop_plane)) {
+            __threadfence();
+            store_release(q.progress + cta, t + 1);
+        }
+        // (3) the second step at plane t - 1
+        if (active && second) {
+            const int i = t - 1;
+            const int64_t base = (int64_t)i * s.plane + col.column;
+            const float *slot = ring + (i % kPairRing) * s.plane + col.column;
+            LeanInputs in;
+            in.P = PA;
+            in.PX = i + 1 < s.nx ? PN : PA;
+            in.PYm = col.y_lo ? __ldcg(reinterpret_cast<const float4 *>(slot - s.pz)) : PA;
+            in.PYp = col.y_hi ? __ldcg(reinterpret_cast<const float4 *>(slot + s.pz)) : PA;
+            in.VXo = f4(XO01, XO23);
+            in.VY = f4(A.YL01, A.YL23);
+            in.VYp = f4(A.YH01, A.YH23);
+            in.VZ = f4(A.ZL01, A.ZL23);
+            in.p_below = col.z_lo ? __ldcg(slot - 1) : 0.f;
+            in.p_above = col.z_hi ? __ldcg(slot + kVec) : 0.f;
+            in.vz_above = A.ZH3;
+            float4 S[NR > 0 ? NR : 1];
+#pragma unroll
+            for (int r = 0; r < NR; r++) S[r] = *reinterpret_cast<const float4 *>(q.psi_out + r * s.field + base);
+            LeanFaces B;
+            float Pn[kVec];
+            lean_update<LAYER, WALLS, NR, true>(g, col, i, base, step + 1, in, XB01, XB23, S, B, Pn, bad2);
+            lean_store<NR, true>(g, col, i, base, Pn, XB01, XB23, B, in.VZ, S, q.psi_out);
+            if (col.any_mine) record_receivers(s, col.points, col.all_points, base, step + 1, Pn);
+            XB01 = B.XH01;
+            XB23 = B.XH23;
+        }
+        A = An;
+        PA = PN;
+    }
+    report_nonfinite(s.status, bad2.x != bad2.x || bad2.y != bad2.y);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -3139,6 +3436,16 @@ struct acf_batch {
     // Test hooks of the staged sweep (acf_set_wait_test): 0 / -1 leave it as built.
     uint64_t test_wait_limit_ns = 0;
     int32_t test_skip_plane = -1;
+    // Steps per launch of the fused single-precision scheme (acf_set_time_blocking): 1, or 2 for
+    // the two-step sweep, with its launch and buffers -- the first-step pressure ring, the CTA
+    // counters and the second copy of the relaxation states -- allocated when it is selected.
+    int32_t time_block = 1;
+    dim3 pair_grid, pair_block;
+    int32_t pair_planes = 0;
+    float *pair_ring = nullptr;
+    int32_t *pair_progress = nullptr;
+    size_t pair_counters = 0;
+    float *psi2 = nullptr;
 
     // CUDA graphs of the adjoint path: forward record, recompute, adjoint steps
     struct Graph {
@@ -3505,6 +3812,120 @@ struct StagedStep {
     }
 };
 
+// The two-step sweep: a cooperative launch, so that every CTA is resident (CTAs wait for their
+// neighbours' counters) or the launch fails with an error instead.
+template <typename T, bool L, bool W, int NR>
+struct PairStep {
+    static void launch(const PairParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = g;
+        cfg.blockDim = b;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, lean_pair_sweep<L, W, NR>, p);
+    }
+};
+
+const void *pair_kernel(bool layer, bool walls, int nr) {
+#define ACF_PAIR_NR(L, W)                                                  \
+    switch (nr) {                                                           \
+        case 0: return (const void *)lean_pair_sweep<L, W, 0>;              \
+        case 1: return (const void *)lean_pair_sweep<L, W, 1>;              \
+        case 2: return (const void *)lean_pair_sweep<L, W, 2>;              \
+        case 3: return (const void *)lean_pair_sweep<L, W, 3>;              \
+        default: return (const void *)lean_pair_sweep<L, W, 4>;             \
+    }
+    if (layer) {
+        if (walls) { ACF_PAIR_NR(true, true) } else { ACF_PAIR_NR(true, false) }
+    } else {
+        if (walls) { ACF_PAIR_NR(false, true) } else { ACF_PAIR_NR(false, false) }
+    }
+#undef ACF_PAIR_NR
+}
+
+// Select 1 or 2 steps per launch. Two need one single-precision room with nz a multiple of 4
+// whose CTAs (128 threads over 32 chunks and 4 rows, or fewer chunks and more rows) all fit on
+// the device at once for one group of x planes; as many groups are used as fit, at least 8
+// planes each.
+int set_time_blocking(acf_batch *b, int32_t steps) {
+    if (!b) return fail(ACF_ERR_ARGUMENT, "null solver");
+    if (steps != 1 && steps != 2) return fail(ACF_ERR_ARGUMENT, "steps per launch must be 1 or 2, got %d", steps);
+    if (steps == 1) {
+        b->time_block = 1;
+        return ACF_OK;
+    }
+    if (b->precision != 4 || b->rooms.size() != 1)
+        return fail(ACF_ERR_ARGUMENT, "two steps per launch need one single-precision room");
+    const RoomHost &h = b->rooms[0];
+    if (h.nz % kVec != 0)
+        return fail(ACF_ERR_ARGUMENT, "two steps per launch need nz to be a multiple of %d, got %d", kVec, h.nz);
+    DeviceGuard guard(b->device);
+    const int nchunks = h.nz / kVec;
+    int bx = 1;
+    while (bx < nchunks && bx < 32) bx <<= 1;
+    const int by = kPairThreads / bx;
+    const int gx = (nchunks + bx - 1) / bx, gy = (h.ny + by - 1) / by;
+    int per_sm = 0;
+    ACF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel(h.has_layer, h.has_walls, h.n_relax),
+                                                           kPairThreads, 0));
+    const int64_t resident = (int64_t)per_sm * b->sms, per_group = (int64_t)gx * gy;
+    if (per_group > resident)
+        return fail(ACF_ERR_ARGUMENT, "two steps per launch: a y-z plane needs %lld CTAs, the device holds %lld",
+                    (long long)per_group, (long long)resident);
+    int64_t groups = std::min<int64_t>(resident / per_group, std::max<int64_t>(1, h.nx / 8));
+    const int planes = (int)((h.nx + groups - 1) / groups);
+    groups = (h.nx + planes - 1) / planes;
+    const size_t ring_bytes = (size_t)groups * kPairRing * h.plane * sizeof(float);
+    const size_t counters = (size_t)(per_group * groups);
+    cudaFree(b->pair_ring);
+    cudaFree(b->pair_progress);
+    b->pair_ring = nullptr;
+    b->pair_progress = nullptr;
+    ACF_CUDA(cudaMalloc(&b->pair_ring, ring_bytes));
+    ACF_CUDA(cudaMalloc(&b->pair_progress, counters * sizeof(int32_t)));
+    if (h.n_relax > 0 && !b->psi2)
+        ACF_CUDA(cudaMalloc(&b->psi2, (size_t)h.n_relax * h.field * sizeof(float)));
+    b->pair_grid = dim3(gx, gy, (unsigned)groups);
+    b->pair_block = dim3(bx, by, 1);
+    b->pair_planes = planes;
+    b->pair_counters = counters;
+    b->time_block = 2;
+    return ACF_OK;
+}
+
+// Two steps of the fused single-precision scheme in one launch. The relaxation states go from
+// the room's own field to the second copy (`back` false) or back; p and v to the other copy.
+void launch_pair(acf_batch *b, int32_t local, bool back, cudaStream_t st) {
+    RoomHost &h = b->rooms[0];
+    PairParams q{};
+    LeanParams &g = q.g;
+    g.f.room = make_room<float>(b, 0);
+    float *own = g.f.room.psi;
+    g.f.room.psi = back ? b->psi2 : own;
+    q.psi_out = back ? own : b->psi2;
+    g.f.np = (float *)b->other_ptr(0, ACF_FIELD_P);
+    g.f.nvx = (float *)b->other_ptr(0, ACF_FIELD_VX);
+    g.f.nvy = (float *)b->other_ptr(0, ACF_FIELD_VY);
+    g.f.nvz = (float *)b->other_ptr(0, ACF_FIELD_VZ);
+    g.f.step_base = b->step_base;
+    g.f.local_step = local;
+    g.f.planes = b->pair_planes;
+    fill_pairs(g.pairs, h);
+    q.ring = b->pair_ring;
+    q.progress = b->pair_progress;
+    q.wait_limit_ns = b->test_wait_limit_ns ? b->test_wait_limit_ns : kWaitLimitNs;
+    q.stop_plane = b->test_skip_plane;
+    cudaMemsetAsync(b->pair_progress, 0, b->pair_counters * sizeof(int32_t), st);
+    dispatch_pressure<float, PairStep>(h.has_layer, h.has_walls, h.n_relax, q, b->pair_grid, b->pair_block, st);
+    h.cur ^= 1;
+    b->launches += 1;
+}
+
 // Launch one step; the fused scheme flips the room's current buffer, as the kernel will have
 // done by the time anything queued after it runs.
 template <typename T>
@@ -3683,6 +4104,25 @@ int run_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cudaStream_t st
         return ACF_OK;
     }
 
+    if constexpr (sizeof(T) == 4) {
+        if (b->time_block == 2 && b->scheme == ACF_SCHEME_FUSED && b->rooms.size() == 1) {
+            // Units of four steps (two launches) leave the relaxation states in the room's own
+            // field and p, v in the copy that four single steps would; the rest are single steps.
+            // A launch covers two full sweeps, so these are not captured in graphs.
+            int64_t done = 0;
+            for (; done + 4 <= n_steps; done += 4) {
+                launch_pair(b, (int32_t)done, false, st);
+                launch_pair(b, (int32_t)(done + 2), true, st);
+            }
+            for (; done < n_steps; done++) {
+                launch_step<T>(b, (int32_t)done, st, nullptr);
+                b->launches += 1;
+            }
+            ACF_CUDA(cudaGetLastError());
+            return ACF_OK;
+        }
+    }
+
     int64_t done = 0;
     if (b->pressure_only() && b->po_first) {
         // The step from the p-v state is not the repeated one: launch it before any graph.
@@ -3848,6 +4288,9 @@ void free_batch(acf_batch *b) {
         cudaFree(ra.grad_src);
     }
     cudaFree(b->badj_table);
+    cudaFree(b->pair_ring);
+    cudaFree(b->pair_progress);
+    cudaFree(b->psi2);
     cudaFree(b->state);
     cudaFree(b->room_table);
     cudaFree(b->fused_table);
@@ -5764,6 +6207,12 @@ int acf_get_scheme(const acf_solver *h) { return h ? h->scheme : -1; }
 int acf_set_prefetch(acf_solver *h, int32_t mode) { return set_prefetch(h, mode); }
 
 int acf_get_prefetch(const acf_solver *h) { return h ? (prefetch_planes(h) ? 1 : 0) : -1; }
+
+int acf_set_time_blocking(acf_solver *h, int32_t steps_per_launch) {
+    return set_time_blocking(h, steps_per_launch);
+}
+
+int acf_get_time_blocking(const acf_solver *h) { return h ? h->time_block : -1; }
 
 int acf_set_staging(acf_solver *h, int32_t rows, int32_t stages, int32_t vector) {
     if (!h) return fail(ACF_ERR_ARGUMENT, "null solver");

@@ -106,8 +106,9 @@ def raise_for_status(word: int) -> None:
                                   "the state is not valid")
     if word & _native.STATUS_WAIT_TIMEOUT:
         raise _native.NativeError(_native.ERR_STATE, "acf_device_status",
-                                  "a staged sweep timed out waiting for its bulk copies; the "
-                                  "solver state is not valid")
+                                  "a sweep timed out waiting (a staged sweep for its bulk "
+                                  "copies, a two-step sweep for its neighbours); the solver "
+                                  "state is not valid")
 
 
 def pinned_array(shape, dtype=np.float32) -> np.ndarray:
@@ -600,6 +601,20 @@ class CudaAcousticFDTD:
     def prefetch(self) -> bool:
         """Whether the L2 prefetch is in effect for this room."""
         return self._lib.acf_get_prefetch(self._handle) == 1
+
+    def set_time_blocking(self, steps_per_launch: int = 2) -> None:
+        """Steps per launch of the fused single-precision sweep: 2 takes every x plane through
+        two steps in one sweep (temporal blocking: the state is read and written once per two
+        steps), 1 goes back to one step per launch. Results are identical either way. Needs
+        float32 and nz a multiple of 4 (``NativeError`` otherwise); takes effect while the
+        scheme is ``"fused"``."""
+        _native.check(self._lib.acf_set_time_blocking(self._handle, int(steps_per_launch)),
+                      "acf_set_time_blocking")
+
+    @property
+    def time_blocking(self) -> int:
+        """Steps per launch of the fused sweep (1 or 2)."""
+        return self._lib.acf_get_time_blocking(self._handle)
 
     def set_launch(self, block_threads: int = 256, planes: int = 4) -> None:
         """Launch geometry of the sweeps (threads per block, x planes per block)."""

@@ -178,6 +178,19 @@ int acf_get_scheme(const acf_solver *solver);
 int acf_set_prefetch(acf_solver *solver, int32_t mode);
 int acf_get_prefetch(const acf_solver *solver);
 
+/* Steps per launch of the fused scheme in single precision: 1 (the default) or 2, temporal
+ * blocking -- one sweep takes each x plane through two steps, reading the state once and writing
+ * it once per two steps. Runs then go in units of four steps (two launches, after which the
+ * state sits where four single steps leave it) and single steps for the rest; results equal
+ * single steps bit for bit. 2 needs one single-precision room with nz a multiple of 4 whose CTAs
+ * of one x-plane group fit on the device at once (ACF_ERR_ARGUMENT otherwise), allocates four
+ * planes of pressure per group, a counter per CTA and a second copy of the relaxation states,
+ * and takes effect while the scheme is ACF_SCHEME_FUSED. acf_get_time_blocking returns the
+ * setting (-1 for a null solver). The step after the fused sweep that the reference's C backend
+ * names as its next one (c/acfdtd.c:12-14); no counterpart in its API. */
+int acf_set_time_blocking(acf_solver *solver, int32_t steps_per_launch);
+int acf_get_time_blocking(const acf_solver *solver);
+
 /* Geometry of the staged scheme: y rows per CTA (1..16, each a whole padded z row), ring
  * buffers per CTA (2..8; 0 picks three, or two where three do not fit) and z elements per
  * thread (2 or 4). The x planes per CTA come from acf_set_launch. ACF_ERR_ARGUMENT when the
@@ -187,7 +200,8 @@ int acf_get_prefetch(const acf_solver *solver);
 int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages, int32_t vector);
 
 /* The solver's device status word, then cleared: 0 when nothing was reported; bit 1 when a
- * staged sweep gave up waiting for its copies; bit 2 when a sweep produced a non-finite
+ * staged sweep gave up waiting for its copies, or a two-step sweep for its neighbour CTAs'
+ * counters; bit 2 when a sweep produced a non-finite
  * pressure (NaN or infinity: every sweep that writes p checks what it writes). Either way the
  * state is not valid. Synchronizes the solver's device. acf_run and acf_batch_run also read
  * the word copied after the previous run, without waiting for the device, and return
@@ -196,12 +210,14 @@ int acf_set_staging(acf_solver *solver, int32_t rows, int32_t stages, int32_t ve
 int acf_device_status(acf_solver *solver, int32_t *status);
 int acf_batch_device_status(acf_batch *batch, int32_t *status);
 
-/* Test hook of the staged sweep, for exercising its bounded waits without a fault: every wait
- * gives up after `wait_limit_ns` (0: the built-in two seconds; else 1 ms to two seconds), and
- * the producer of the grid's first CTA leaves out the copies of x plane `skip_plane` (-1:
- * none), so that CTA's consumers wait for data that never arrives, run out of time, raise bit
- * 1 of the status word and return; the producer drains the copies it did issue before the CTA
- * exits. No counterpart in the reference. */
+/* Test hook of the staged and two-step sweeps, for exercising their bounded waits without a
+ * fault: every wait gives up after `wait_limit_ns` (0: the built-in two seconds; else 1 ms to
+ * two seconds), and with `skip_plane` >= 0 (-1: none) the grid's first CTA withholds something
+ * its waiters need. In the staged sweep its producer leaves out the copies of x plane
+ * `skip_plane`, so that CTA's consumers wait for data that never arrives, run out of time, raise
+ * bit 1 of the status word and return; the producer drains the copies it did issue before the
+ * CTA exits. In the two-step sweep it stops publishing its progress from that plane on, so its
+ * neighbour CTAs' waits run out, raise bit 1 and stop waiting. No counterpart in the reference. */
 int acf_set_wait_test(acf_solver *solver, int64_t wait_limit_ns, int32_t skip_plane);
 
 /* Use CUDA graphs of `steps_per_graph` steps for runs at least that long (0 disables). */
