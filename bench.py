@@ -488,6 +488,7 @@ def run_ours(args) -> None:
     precision = None if args.skip_extras else precision_check(args)
     slabs = None if args.skip_extras else slab_overhead(args)
     pressure_only = None if args.skip_extras else pressure_only_cost(args)
+    time_blocking = None if args.skip_extras else time_blocking_cost(args)
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -511,6 +512,7 @@ def run_ours(args) -> None:
         "precision": precision,
         "slabs_one_gpu": slabs,
         "pressure_only": pressure_only,
+        "time_blocking": time_blocking,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, budget_s=args.cpu_budget)
@@ -558,6 +560,7 @@ def extras_summary(line: dict) -> dict:
         "pressure_only_gcups": get("pressure_only", "pressure_only", "gcups"),
         "pressure_only_frac": get("pressure_only", "pressure_only", "hbm_frac_of_measured"),
         "pressure_only_speedup": get("pressure_only", "speedup_over_fused"),
+        "time_blocking_speedup": get("time_blocking", "speedup"),
     }
 
 
@@ -787,6 +790,49 @@ def pressure_only_cost(args) -> dict:
     rec = recordings["pressure_only"]
     out["speedup_over_fused"] = out["pressure_only"]["gcups"] / out["fused"]["gcups"]
     out["receivers_vs_fused_fp32"] = _errors(rec, recordings["fused"])
+    return out
+
+
+def time_blocking_cost(args) -> dict:
+    """Two steps per launch (temporal blocking, ``set_time_blocking(2)``) against the one-step
+    lean sweep on the headline room (walls, sponge, air, the source and receivers), 400 steps
+    from rest each, device time from CUDA events around the run; recordings compared bit for
+    bit. Algorithmic DRAM bytes per cell-step: 56 one step at a time, 28 two at a time (plus the
+    first-step pressure ring, which stays in L2)."""
+    import torch
+
+    from ac_fdtd_b200 import CudaAcousticFDTD, gaussian_pulse
+
+    grid, objects, points = workload(args.size)
+    T = 400
+    peak, peak_kind = measured_peak_hbm()
+    out = {"workload": f"the headline room, {args.size}^3 fp32, {T} steps from rest"}
+    recordings = {}
+    for steps_per_launch, bytes_per_cell in ((1, 56), (2, 28)):
+        solver = CudaAcousticFDTD(grid, dtype=np.float32, scheme="fused", **objects)
+        if steps_per_launch == 2:
+            solver.set_time_blocking(2)
+        solver.add_volume_source(points[0], gaussian_pulse(T, solver.dt, 4000.0))
+        for point in points[1:]:
+            solver.add_pressure_receiver(point)
+
+        def run(solver=solver):
+            solver.reset_state()
+            solver.step_index = 0
+            solver.run(T)
+
+        run()
+        run_ms = min(_device_ms(run, torch) for _ in range(2))
+        recordings[steps_per_launch] = solver.recorded_pressure
+        solver.close()
+        gcups = grid.n_cells * T / (run_ms * 1e-3) / 1e9
+        out[f"steps_per_launch_{steps_per_launch}"] = {
+            "gcups": gcups, "bytes_per_cell_step": bytes_per_cell,
+            f"hbm_frac_of_{peak_kind}": gcups * bytes_per_cell / peak,
+            "kernel": "lean_sweep<true,true,3>" if steps_per_launch == 1 else "lean_pair_sweep<true,true,3>",
+        }
+    out["speedup"] = out["steps_per_launch_2"]["gcups"] / out["steps_per_launch_1"]["gcups"]
+    out["recordings_bitwise_equal"] = bool(np.array_equal(recordings[1], recordings[2]))
     return out
 
 
