@@ -490,6 +490,13 @@ def run_ours(args) -> None:
     pressure_only = None if args.skip_extras else pressure_only_cost(args)
     time_blocking = None if args.skip_extras else time_blocking_cost(args)
 
+    clock_record = clocks.summary()
+    if clock_record.get("sm_mhz"):
+        # Launch time in SM clock cycles at the median loaded clock: separates the code's cost
+        # from the clock the power cap allowed (ms x MHz = thousands of cycles).
+        avg_ms = roofline.get("avg_launch_ms") or 0.0
+        roofline["launch_kcycles_at_median_sm_clock"] = avg_ms * clock_record["sm_mhz"]
+        roofline["median_sm_mhz"] = clock_record["sm_mhz"]
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
@@ -505,7 +512,7 @@ def run_ours(args) -> None:
                         "recorded_pressure, get_state (pinned host)",
                 "phases_per_step": phases},
         "gpu_launches": launches,
-        "clocks": clocks.summary(),
+        "clocks": clock_record,
         "batched": batched,
         "adjoint": adjoint,
         "batched_inversion": inversion,
