@@ -1598,11 +1598,12 @@ struct LeanFaces {
 // XL and the relaxation states S, which it advances in place) to its updated faces and its next
 // pressures Pn, with walls, the sponge and the sources of `step`. `bad2` turns NaN once a
 // pressure produced is not finite.
-template <bool LAYER, bool WALLS, int NR, bool ALIGNED>
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED, bool REC = false>
 __device__ __forceinline__ void lean_update(const LeanParams &g, const LeanColumn &col, int i,
                                             int64_t base, int64_t step, const LeanInputs &in,
                                             float2 XL01, float2 XL23, float4 (&S)[NR > 0 ? NR : 1],
-                                            LeanFaces &o, float (&Pn)[kVec], float2 &bad2) {
+                                            LeanFaces &o, float (&Pn)[kVec], float2 &bad2,
+                                            float *PT = nullptr) {
     const Room<float> &s = g.f.room;
     const bool x_inner = i + 1 < s.nx;
     const float2 cv2 = g.pairs[kPairCv], cp2 = g.pairs[kPairCp];
@@ -1707,6 +1708,10 @@ __device__ __forceinline__ void lean_update(const LeanParams &g, const LeanColum
     Pn[1] = pe01.y;
     Pn[2] = pe23.x;
     Pn[3] = pe23.y;
+    if (REC) {                                // p before the wall closed form, for the history
+#pragma unroll
+        for (int e = 0; e < kVec; e++) PT[e] = Pn[e];
+    }
     if (WALLS && (col.wall_column || i == 0 || i == s.nx - 1)) {
         const float Po[kVec] = {P.x, P.y, P.z, P.w};
         column_walls(s, i, col.j, col.k0, real, [&](int e, float fu, float fp) {
@@ -1777,9 +1782,11 @@ __device__ __forceinline__ void lean_store(const LeanParams &g, const LeanColumn
     for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(psi + r * s.field + base) = S[r];
 }
 
-template <bool LAYER, bool WALLS, int NR, bool ALIGNED = true>
+// REC: also write the boundary history of the wall gradients (record_shell), as
+// pressure_sweep_rec does.
+template <bool LAYER, bool WALLS, int NR, bool ALIGNED = true, bool REC = false>
 __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, int i_end, int j, int c,
-                                            int64_t step) {
+                                            int64_t step, const History<float> *hist = nullptr) {
     const Room<float> &s = g.f.room;
     const LeanColumn col = lean_setup<LAYER, ALIGNED>(s, j, c);
     const int64_t column = col.column;
@@ -1829,10 +1836,15 @@ __device__ __forceinline__ void lean_column(const LeanParams &g, int i_begin, in
         for (int r = 0; r < NR; r++) S[r] = *reinterpret_cast<const float4 *>(s.psi + r * s.field + base);
 
         LeanFaces o;
-        float Pn[kVec];
-        lean_update<LAYER, WALLS, NR, ALIGNED>(g, col, i, base, step, in, XL01, XL23, S, o, Pn, bad2);
+        float Pn[kVec], PT[kVec];
+        lean_update<LAYER, WALLS, NR, ALIGNED, REC>(g, col, i, base, step, in, XL01, XL23, S, o, Pn,
+                                                    bad2, PT);
         lean_store<NR, ALIGNED>(g, col, i, base, Pn, XL01, XL23, o, in.VZ, S, s.psi);
         if (col.any_mine) record_receivers(s, col.points, col.all_points, base, step, Pn);
+        if (REC && hist->shell && (col.wall_column || i == 0 || i == s.nx - 1)) {
+            const float Po[kVec] = {in.P.x, in.P.y, in.P.z, in.P.w};
+            record_shell(s, *hist, i, j, col.k0, step, Po, PT);
+        }
         XL01 = o.XH01;
         XL23 = o.XH23;
         P = in.PX;
@@ -1866,6 +1878,24 @@ __global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR)) lean_swee
 template <bool LAYER, bool WALLS, int NR>
 __global__ void __maxnreg__(96) lean_sweep_padded(const LeanParams g) {
     lean_sweep_body<LAYER, WALLS, NR, false>(g);
+}
+
+// The recorded forward step of the wall gradients in single precision (rooms with nz a multiple
+// of 4): the lean step, also writing the boundary history.
+struct LeanRecParams {
+    LeanParams g;
+    History<float> hist;
+};
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR)) lean_sweep_rec(const LeanRecParams q) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= q.g.f.room.nchunks || j >= q.g.f.room.ny) return;
+    const int64_t step = *q.g.f.step_base + q.g.f.local_step;
+    const int i_begin = blockIdx.z * q.g.f.planes;
+    lean_column<LAYER, WALLS, NR, true, true>(q.g, i_begin, min(q.g.f.room.nx, i_begin + q.g.f.planes), j,
+                                              c, step, &q.hist);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -3466,7 +3496,8 @@ struct acf_batch {
         int32_t every = 0;           // checkpoint interval
         int64_t recorded = 0, step0 = 0;
         bool fields_recorded = false;   // the recorded run wrote D and psi of every step itself
-        int direct_mode = -1;        // fields_recorded of the last recorded run (graph validity)
+        int direct_mode = -1;        // how the last recorded run stepped (graph validity): 0 two
+                                     // sweeps, 1 two sweeps writing D and psi, 2 the lean step
         int64_t shell_total = 0;
         int64_t face_off[6] = {};
         void *hist_shell = nullptr;  // capacity x 2 x shell_total values
@@ -5088,6 +5119,13 @@ struct RecPressure {
 };
 
 template <typename T, bool L, bool W, int NR>
+struct LeanRecStep {
+    static void launch(const LeanRecParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_sweep_rec<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
 struct AdjPressure {
     static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
         adjoint_pressure_sweep<T, L, W, NR, false><<<g, b, 0, st>>>(p);
@@ -5162,10 +5200,15 @@ constexpr int64_t kAdjointChunk = 64;
 // Forward steps [s0, s0 + n) on `state` (the room's own fields, or the recompute copy), writing
 // the history in `hist`. Receivers record only when `receivers` is set, so a recompute leaves
 // the caller's recordings alone. With `checkpoints`, the state at every multiple of the
-// checkpoint interval (counted from the recorded run's first step) is copied out first.
+// checkpoint interval (counted from the recorded run's first step) is copied out first. With
+// `lean` (single precision, nz a multiple of 4, the room's own fields current in its primary
+// copy, no D/psi history) each step is one lean step into the other copy, flipping the current
+// copy as the fused scheme does; graphs hold an even number of steps, so a replay leaves it as
+// it found it.
 template <typename T>
 int record_steps(acf_batch *b, acf_batch::Graph &g, const void *state, const History<T> &hist,
-                 int64_t s0, int64_t n, bool receivers, cudaStream_t st, bool checkpoints) {
+                 int64_t s0, int64_t n, bool receivers, cudaStream_t st, bool checkpoints,
+                 bool lean = false) {
     const RoomHost &h = b->rooms[0];
     StepParams<T> p{};
     p.room = make_room<T>(b, 0, state);
@@ -5174,7 +5217,28 @@ int record_steps(acf_batch *b, acf_batch::Graph &g, const void *state, const His
     p.step_base = b->step_base;
     p.planes = b->planes;
     const LaunchShape L = single_shape(b);
+    const int per_step = lean ? 1 : 2;
     auto launch = [&](int32_t local, cudaStream_t s) {
+        if constexpr (sizeof(T) == 4) {
+            if (lean) {
+                RoomHost &hr = b->rooms[0];
+                LeanRecParams q{};
+                q.g.f.room = make_room<float>(b, 0);
+                q.g.f.np = (float *)b->other_ptr(0, ACF_FIELD_P);
+                q.g.f.nvx = (float *)b->other_ptr(0, ACF_FIELD_VX);
+                q.g.f.nvy = (float *)b->other_ptr(0, ACF_FIELD_VY);
+                q.g.f.nvz = (float *)b->other_ptr(0, ACF_FIELD_VZ);
+                q.g.f.step_base = b->step_base;
+                q.g.f.local_step = local;
+                q.g.f.planes = b->planes;
+                fill_pairs(q.g.pairs, hr);
+                q.hist = hist;
+                dispatch_pressure<float, LeanRecStep>(hr.has_layer, hr.has_walls, hr.n_relax, q, L.grid,
+                                                      L.block, s);
+                hr.cur ^= 1;
+                return;
+            }
+        }
         StepParams<T> q = p;
         q.local_step = local;
         if (h.has_layer) velocity_sweep<T, true><<<L.grid, L.block, 0, s>>>(q);
@@ -5195,13 +5259,13 @@ int record_steps(acf_batch *b, acf_batch::Graph &g, const void *state, const His
         if (n - done >= G) {
             int rc = replay(b, g, G, G, 1, st, launch);
             if (rc) return rc;
-            b->launches += 2 * G + 1;
+            b->launches += per_step * G + 1;
             done += G;
         } else {
             // the tail: launch step by step from the counter, then advance it past them
             for (int64_t t = 0; done + t < n; t++) launch((int32_t)t, st);
             bump_step_base<<<1, 1, 0, st>>>(b->step_base, n - done);
-            b->launches += 2 * (n - done) + 1;
+            b->launches += per_step * (n - done) + 1;
             done = n;
         }
     }
@@ -5227,13 +5291,34 @@ int forward_record_impl(acf_batch *b, int64_t n_steps, int64_t step_offset, cuda
         hist.fields_step0 = step_offset;
         hist.fields_slots = A.every;
     }
-    if ((int)A.fields_recorded != A.direct_mode) {
+    // Without air the history is the boundary shell alone, which the lean single-precision step
+    // writes as it goes: one sweep per recorded step instead of two, into the second copy of p
+    // and v (allocated here when the solver's scheme has none; two sweeps if that fails).
+    bool lean = !air && sizeof(T) == 4 && b->rooms.size() == 1 && b->rooms[0].nz % kVec == 0 &&
+                b->rooms[0].cur == 0;
+    if (lean && !b->rooms[0].second) {
+        RoomHost &h = b->rooms[0];
+        const size_t bytes = ((size_t)4 * h.field + (size_t)h.pz) * b->elem();
+        if (cudaMalloc(&h.second, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            h.second = nullptr;
+            lean = false;
+        } else {
+            ACF_CUDA(cudaMemsetAsync(h.second, 0, bytes, st));
+        }
+    }
+    const int mode = A.fields_recorded ? 1 : (lean ? 2 : 0);
+    if (mode != A.direct_mode) {
         b->adj_graphs_dirty = true;           // the record graph holds the history pointers
-        A.direct_mode = (int)A.fields_recorded;
+        A.direct_mode = mode;
     }
     int rc = record_steps<T>(b, b->g_record, b->field_ptr(0, ACF_FIELD_P), hist, step_offset, n_steps,
-                             true, st, air && !A.fields_recorded);
+                             true, st, air && !A.fields_recorded, lean);
     if (rc) return rc;
+    if (lean) {   // an odd number of steps ends in the second copy: bring the state back
+        rc = make_primary(b, st);
+        if (rc) return rc;
+    }
     ACF_CUDA(cudaGetLastError());
     return ACF_OK;
 }

@@ -95,3 +95,47 @@ def test_batched_patch_gradient_matches_central_differences():
         fds.append((lp - lm) / (2 * h))
     got = np.array([grads[2].walls[c] for c in checked])
     assert np.max(np.abs(got - np.array(fds))) <= 1e-6 * np.max(np.abs(grads[2].walls)), (got, fds)
+
+
+def test_single_precision_lean_recorded_rooms_equal_the_batch():
+    """Without air, a single-precision room with nz a multiple of 4 records its forward run with
+    the lean one-sweep step (writing the boundary history as it goes) while a batch records with
+    two sweeps: recordings and wall and source gradients agree bit for bit, over an odd number of
+    steps (the state ends in the second copy and is moved back), and the final pressure equals a
+    plain run's."""
+    from ac_fdtd_b200 import CudaAcousticFDTD
+
+    steps = 71
+    specs = [
+        dict(grid=Grid(dx=0.05, nx=13, ny=11, nz=12), walls=WallAdmittances(0.3, 0.1, 0.45, 0.2, 0.08, 0.27)),
+        dict(grid=Grid(dx=0.05, nx=9, ny=14, nz=16), walls=WallAdmittances(0.2, 0.1, 0.3, 0.05, 0.4, 0.15),
+             absorbing_layer=AbsorbingLayer(thickness=3, faces=((1, 1),))),
+    ]
+    batch = DifferentiableBatch(specs, dtype=np.float32, max_steps=steps)
+    for r, spec in enumerate(specs):
+        pts = points(spec, r)
+        batch.batch.add_volume_source(r, pts[0], gaussian_pulse(steps, batch.batch.dt(r), 2000.0))
+        for p in pts[1:]:
+            batch.batch.add_pressure_receiver(r, p)
+    recs = batch.forward(steps)
+    weights = [np.random.default_rng(40 + r).standard_normal(rec.shape) for r, rec in enumerate(recs)]
+    grads = batch.backward([w * rec.astype(np.float64) for w, rec in zip(weights, recs, strict=True)])
+    for r, spec in enumerate(specs):
+        pts = points(spec, r)
+        room = DifferentiableRoom(spec["grid"], dtype=np.float32, walls=spec["walls"],
+                                  absorbing_layer=spec.get("absorbing_layer"), max_steps=steps)
+        plain = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
+                                 absorbing_layer=spec.get("absorbing_layer"))
+        for s in (room.solver, plain):
+            s.add_volume_source(pts[0], gaussian_pulse(steps, s.dt, 2000.0))
+            for p in pts[1:]:
+                s.add_pressure_receiver(p)
+        rec = room.forward(steps)
+        plain.run(steps)
+        np.testing.assert_array_equal(rec, recs[r])
+        np.testing.assert_array_equal(room.solver.p, plain.p)
+        single = room.backward(weights[r] * rec.astype(np.float64))
+        np.testing.assert_array_equal(grads[r].walls, single.walls)
+        np.testing.assert_array_equal(grads[r].signal, single.signal)
+        room.solver.close()
+        plain.close()
