@@ -847,10 +847,11 @@ def slab_overhead(args) -> dict:
     """The x-slab decomposition's own cost with every part on this GPU: the headline room whole
     and cut into 2 and 4 slabs (300 steps), recordings compared bit for bit. Two sweeps: the
     pressure sweep stores the boundary planes into the neighbours' ghosts (acf_run_slabs);
-    fused scheme: the ghost planes are copied after each step."""
+    fused scheme: one lean step per part and step, storing its boundary planes into the
+    neighbours' next-copy ghosts, the parts' launches replayed from one CUDA graph."""
     out = {"workload": f"the headline room, {args.size}^3 fp32, 300 steps, every part on one GPU"}
     for scheme, path in (("two_sweeps", "exchange fused into the pressure sweep"),
-                         ("fused", "ghost planes copied after each step")):
+                         ("fused", "ghost stores fused into each part's lean step")):
         out[scheme] = {"exchange": path, **_slab_runs(args, scheme)}
     return out
 
