@@ -1880,6 +1880,33 @@ __global__ void __maxnreg__(96) lean_sweep_padded(const LeanParams g) {
     lean_sweep_body<LAYER, WALLS, NR, false>(g);
 }
 
+// The lean step of up to kMaxLeanParts slabs of one room in one launch (slab groups whose parts
+// share a GPU): every part's step reads only its own current copy and writes only the next
+// copies (its own, and its boundary planes into the neighbours' ghost planes), so the parts of
+// one step are independent. blockIdx.z runs over the parts' groups of x planes in turn.
+constexpr int kMaxLeanParts = 8;
+
+struct LeanPartsParams {
+    LeanParams part[kMaxLeanParts];
+    int32_t first_group[kMaxLeanParts + 1];   // part p: blockIdx.z in [first_group[p], first_group[p + 1])
+    int32_t n;
+};
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, ACF_LEAN_MIN_BLOCKS(LAYER, NR))
+lean_parts_sweep(const __grid_constant__ LeanPartsParams q) {
+    int p = 0;
+    while (p + 1 < q.n && (int)blockIdx.z >= q.first_group[p + 1]) p++;
+    const LeanParams &g = q.part[p];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= g.f.room.nchunks || j >= g.f.room.ny) return;
+    const bool any_point = (g.f.room.n_src | g.f.room.n_rec) != 0;
+    const int64_t step = any_point ? (*g.f.step_base + g.f.local_step) : 0;
+    const int i_begin = ((int)blockIdx.z - q.first_group[p]) * g.f.planes;
+    lean_column<LAYER, WALLS, NR, true>(g, i_begin, min(g.f.room.nx, i_begin + g.f.planes), j, c, step);
+}
+
 // The recorded forward step of the wall gradients in single precision (rooms with nz a multiple
 // of 4): the lean step, also writing the boundary history.
 struct LeanRecParams {
@@ -3754,6 +3781,13 @@ struct LeanStep {
 };
 
 template <typename T, bool L, bool W, int NR>
+struct LeanPartsStep {
+    static void launch(const LeanPartsParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_parts_sweep<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+template <typename T, bool L, bool W, int NR>
 struct LeanStepPadded {
     static void launch(const LeanParams &p, dim3 g, dim3 b, cudaStream_t st) {
         lean_sweep_padded<L, W, NR><<<g, b, 0, st>>>(p);
@@ -4714,6 +4748,47 @@ void fused_slab_step(acf_batch *const *parts, int n, const int32_t *own_lo, cons
         x.step_base = b->step_base;
         x.local_step = local;
         x.planes = b->planes;
+    }
+    if constexpr (sizeof(T) == 4) {
+        // Parts on one GPU with the same features and nz a multiple of 4: one launch per
+        // kMaxLeanParts parts instead of one per part.
+        bool combined = true;
+        const RoomHost &h0 = parts[0]->rooms[0];
+        for (int q = 0; q < n; q++) {
+            const RoomHost &h = parts[q]->rooms[0];
+            combined = combined && streams[q] == streams[0] && parts[q]->device == parts[0]->device &&
+                       h.nz % kVec == 0 && h.ny == h0.ny && h.nz == h0.nz && h.has_layer == h0.has_layer &&
+                       h.has_walls == h0.has_walls && h.n_relax == h0.n_relax &&
+                       parts[q]->block_threads == parts[0]->block_threads;
+        }
+        if (combined && n > 1) {
+            DeviceGuard g(parts[0]->device);
+            for (int q0 = 0; q0 < n; q0 += kMaxLeanParts) {
+                const int m = std::min(kMaxLeanParts, n - q0);
+                LeanPartsParams lp{};
+                lp.n = m;
+                LaunchShape L{};
+                int groups = 0;
+                for (int k = 0; k < m; k++) {
+                    const int q = q0 + k;
+                    lp.part[k].f = f[q];
+                    fill_pairs(lp.part[k].pairs, parts[q]->rooms[0]);
+                    L = single_shape(parts[q]);
+                    lp.first_group[k] = groups;
+                    groups += (int)L.grid.z;
+                }
+                lp.first_group[m] = groups;
+                L.grid.z = (unsigned)groups;
+                dispatch_pressure<float, LeanPartsStep>(h0.has_layer, h0.has_walls, h0.n_relax, lp, L.grid,
+                                                        L.block, streams[0]);
+                parts[q0]->launches += 1;
+            }
+            for (int q = 0; q < n; q++) {
+                after(q);
+                parts[q]->rooms[0].cur ^= 1;
+            }
+            return;
+        }
     }
     for (int q = 0; q < n; q++) {
         DeviceGuard g(parts[q]->device);

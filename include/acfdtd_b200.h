@@ -321,9 +321,10 @@ int acf_solver_device(const acf_solver *solver);
  * its first and last own planes of p into the neighbours' ghost planes (peer stores across
  * GPUs; peer access is enabled as needed). The ghost planes must hold the neighbours' p before
  * the first step (acf_copy_plane). With the fused scheme (every part on it, copies in step)
- * each step is one launch per part: it writes its own planes of the next copy and stores its
- * first and last own planes into the neighbours' ghost planes of their next copies; on one GPU
- * the steps replay from a CUDA graph. Single rooms of equal scheme, precision, ny and nz. Parts
+ * each part's step writes its own planes of the next copy and stores its first and last own
+ * planes into the neighbours' ghost planes of their next copies: one launch per part across
+ * GPUs; on one GPU, in single precision with nz a multiple of 4, one launch per step for up to 8
+ * parts, and the steps replay from a CUDA graph. Single rooms of equal scheme, precision, ny and nz. Parts
  * on one GPU run on `stream`; parts on several GPUs on each device's default stream,
  * ordered by events, and `stream` must then be null (ACF_ERR_ARGUMENT otherwise: a stream
  * belongs to one device). Asynchronous. No counterpart in the reference. */
