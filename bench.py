@@ -791,6 +791,8 @@ def pressure_only_cost(args) -> dict:
             "gcups": grid.n_cells * T / (run_ms * 1e-3) / 1e9, "bytes_per_cell": bytes_per_cell,
             "avg_launch_ms": kernel_ms, "achieved_GBps": achieved,
             f"hbm_frac_of_{peak_kind}": achieved / peak,
+            # one kernel per step in both schemes: the whole graph-replayed run over its bytes
+            f"run_hbm_frac_of_{peak_kind}": grid.n_cells * T * bytes_per_cell / (run_ms * 1e-3) / 1e9 / peak,
             "kernel": "lean_sweep<false,walls,0>" if scheme == "fused" else "pressure_only_sweep<float,walls>",
             "launch": launch,
         }
