@@ -2976,6 +2976,271 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? (AIR && VW == kVec ? 1 
     }
 }
 
+// The fused adjoint step in single precision for rooms with nz a multiple of 4 and no air
+// gradients: adjoint_pressure_column<float, ..., FUSED> with the lean forward column's packed
+// arithmetic -- the same operations in the same order, each lane rounded as the scalar operation
+// (sums as a + (+-1) b, "plus a product" as "minus the product by the negated coefficient"),
+// layer factors that are exactly 1 skipped -- so its results are the generic column's bit for bit.
+// Walls, receivers and sources keep the generic column's scalar code on the cells they touch.
+
+enum {
+    kAdjNegCv = 0, kAdjScp = 1,
+    kAdjNegGain = 2, kAdjOneMinusDecay = 6, kAdjMean = 10, kAdjNegMean = 14, kAdjDecay = 18
+};
+
+struct LeanAdjointParams {
+    AdjointParams<float> a;
+    float2 k[22];          // the kAdj* slots, each value in both lanes
+};
+
+template <bool LAYER, bool WALLS, int NR>
+__device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, int i_begin, int i_end,
+                                                    int j, int c, int64_t step) {
+    const AdjointParams<float> &a = g.a;
+    const Room<float> &s = a.room;
+    const int k0 = c * kVec;
+    const int64_t column = (int64_t)j * s.pz + k0;
+    const bool y_lo = j > 0, y_hi = j + 1 < s.ny;
+    const bool z_lo = k0 > 0, z_hi = k0 + kVec < s.nz;
+    bool all_points = false;
+    const uint32_t points = (s.n_src | s.n_rec) != 0 ? column_points(s, j, k0, all_points) : 0u;
+    const bool any_mine = points != 0 || all_points;
+    const bool wall_column = !y_lo || !y_hi || !z_lo || !z_hi;
+    const float2 zero2 = dup2(0.f);
+
+    float fj_cell = 1.f, fj_face = 1.f, fj1_face = 1.f, fkf4 = 1.f;
+    float2 fkc01 = dup2(1.f), fkc23 = dup2(1.f), fkf01 = dup2(1.f), fkf23 = dup2(1.f);
+    bool damp_y = false, damp_z = false;
+    if (LAYER) {
+        fj_cell = __ldg(s.cell[1] + j);
+        fj_face = __ldg(s.face[1] + j);
+        fj1_face = __ldg(s.face[1] + j + 1);
+        fkc01 = make_float2(__ldg(s.cell[2] + k0), __ldg(s.cell[2] + k0 + 1));
+        fkc23 = make_float2(__ldg(s.cell[2] + k0 + 2), __ldg(s.cell[2] + k0 + 3));
+        fkf01 = make_float2(__ldg(s.face[2] + k0), __ldg(s.face[2] + k0 + 1));
+        fkf23 = make_float2(__ldg(s.face[2] + k0 + 2), __ldg(s.face[2] + k0 + 3));
+        fkf4 = __ldg(s.face[2] + k0 + 4);
+        damp_y = fj_cell != 1.f || fj_face != 1.f || fj1_face != 1.f;
+        damp_z = fkc01.x != 1.f || fkc01.y != 1.f || fkc23.x != 1.f || fkc23.y != 1.f ||
+                 fkf01.x != 1.f || fkf01.y != 1.f || fkf23.x != 1.f || fkf23.y != 1.f || fkf4 != 1.f;
+    }
+
+    // Carried along x: lambda_D^{n+1} of this plane and mu^{n+1} on its lower x face.
+    float4 Dc;
+    float2 XL01, XL23;
+    {
+        const int64_t b0 = (int64_t)i_begin * s.plane + column;
+        float4 Dm = make_float4(0.f, 0.f, 0.f, 0.f);
+        Dc = __ldg(reinterpret_cast<const float4 *>(a.ld + b0));
+        if (i_begin > 0) Dm = __ldg(reinterpret_cast<const float4 *>(a.ld + b0 - s.plane));
+        const float4 V = __ldg(reinterpret_cast<const float4 *>(a.lvx + b0));
+        XL01 = add2(lo2(V), sub2(lo2(Dm), lo2(Dc)));
+        XL23 = add2(hi2(V), sub2(hi2(Dm), hi2(Dc)));
+        if (LAYER) {   // (m fi_face) fj_cell gk_cell
+            const float fi_face = __ldg(s.face[0] + i_begin);
+            if (fi_face != 1.f) { XL01 = mul2(XL01, dup2(fi_face)); XL23 = mul2(XL23, dup2(fi_face)); }
+            if (damp_y) { XL01 = mul2(XL01, dup2(fj_cell)); XL23 = mul2(XL23, dup2(fj_cell)); }
+            if (damp_z) { XL01 = mul2(XL01, fkc01); XL23 = mul2(XL23, fkc23); }
+        }
+    }
+
+    for (int i = i_begin; i < i_end; i++) {
+        const int64_t base = (int64_t)i * s.plane + column;
+        const bool x_lo = i > 0, x_hi = i + 1 < s.nx;
+        if (s.prefetch && i + 1 < i_end) {
+            const int64_t next = base + s.plane;
+            if (i + 2 < s.nx) prefetch_l2(a.ld + next + s.plane);
+            prefetch_l2(a.lvx + next + s.plane);
+            prefetch_l2(a.lvy + next);
+            prefetch_l2(a.lvz + next);
+            prefetch_l2(a.lp + next);
+#pragma unroll
+            for (int r = 0; r < NR; r++) prefetch_l2(a.lpsi + r * s.field + next);
+        }
+        // ---- loads
+        float4 Dxp = make_float4(0.f, 0.f, 0.f, 0.f), Dy = Dxp, Dyp = Dxp;
+        if (x_hi) Dxp = __ldg(reinterpret_cast<const float4 *>(a.ld + base + s.plane));
+        if (y_lo) Dy = __ldg(reinterpret_cast<const float4 *>(a.ld + base - s.pz));
+        if (y_hi) Dyp = __ldg(reinterpret_cast<const float4 *>(a.ld + base + s.pz));
+        const float d_below = z_lo ? __ldg(a.ld + base - 1) : 0.f;
+        const float d_above = z_hi ? __ldg(a.ld + base + kVec) : 0.f;
+        const float4 VXp = __ldg(reinterpret_cast<const float4 *>(a.lvx + base + s.plane));
+        const float4 VY = __ldg(reinterpret_cast<const float4 *>(a.lvy + base));
+        const float4 VYp = __ldg(reinterpret_cast<const float4 *>(a.lvy + base + s.pz));
+        const float4 VZ = __ldg(reinterpret_cast<const float4 *>(a.lvz + base));
+        const float vz_above = __ldg(a.lvz + base + kVec);
+        const float4 L = *reinterpret_cast<const float4 *>(a.lp + base);
+        float4 LS[NR > 0 ? NR : 1];
+#pragma unroll
+        for (int r = 0; r < NR; r++) LS[r] = *reinterpret_cast<const float4 *>(a.lpsi + r * s.field + base);
+        float fi_cell = 1.f, fi1_face = 1.f;
+        if (LAYER) {
+            fi_cell = __ldg(s.cell[0] + i);
+            fi1_face = __ldg(s.face[0] + i + 1);
+        }
+
+        // ---- mu^{n+1} on the six faces: LV + (lambda_D[lower] - lambda_D[upper]), damped
+        float2 XH01 = add2(lo2(VXp), sub2(lo2(Dc), lo2(Dxp))), XH23 = add2(hi2(VXp), sub2(hi2(Dc), hi2(Dxp)));
+        float2 YL01 = add2(lo2(VY), sub2(lo2(Dy), lo2(Dc))), YL23 = add2(hi2(VY), sub2(hi2(Dy), hi2(Dc)));
+        float2 YH01 = add2(lo2(VYp), sub2(lo2(Dc), lo2(Dyp))), YH23 = add2(hi2(VYp), sub2(hi2(Dc), hi2(Dyp)));
+        // z face k0 + e lies between cells k0 + e - 1 (below: d_below for e = 0; 0 at k = 0) and k0 + e
+        float2 Z01 = add2(lo2(VZ), sub2(make_float2(d_below, Dc.x), lo2(Dc)));
+        float2 Z23 = add2(hi2(VZ), sub2(make_float2(Dc.y, Dc.z), hi2(Dc)));
+        float above = vz_above + (Dc.w - d_above);
+        if (LAYER) {
+            if (fi_cell != 1.f || fi1_face != 1.f) {
+                const float2 x = dup2(fi1_face), y = dup2(fi_cell);
+                XH01 = mul2(XH01, x); XH23 = mul2(XH23, x);
+                YL01 = mul2(YL01, y); YL23 = mul2(YL23, y);
+                YH01 = mul2(YH01, y); YH23 = mul2(YH23, y);
+                Z01 = mul2(Z01, y); Z23 = mul2(Z23, y);
+                above = above * fi_cell;
+            }
+            if (damp_y) {
+                const float2 x = dup2(fj_cell), y = dup2(fj_face), z = dup2(fj1_face);
+                XH01 = mul2(XH01, x); XH23 = mul2(XH23, x);
+                YL01 = mul2(YL01, y); YL23 = mul2(YL23, y);
+                YH01 = mul2(YH01, z); YH23 = mul2(YH23, z);
+                Z01 = mul2(Z01, x); Z23 = mul2(Z23, x);
+                above = above * fj_cell;
+            }
+            if (damp_z) {
+                XH01 = mul2(XH01, fkc01); XH23 = mul2(XH23, fkc23);
+                YL01 = mul2(YL01, fkc01); YL23 = mul2(YL23, fkc23);
+                YH01 = mul2(YH01, fkc01); YH23 = mul2(YH23, fkc23);
+                Z01 = mul2(Z01, fkf01); Z23 = mul2(Z23, fkf23);
+                above = above * fkf4;
+            }
+        }
+
+        // ---- lambda(p^{n+1}) = L + c_v div_interior(mu^{n+1})
+        const float2 xh01 = x_hi ? XH01 : zero2, xh23 = x_hi ? XH23 : zero2;
+        const float2 xl01 = x_lo ? XL01 : zero2, xl23 = x_lo ? XL23 : zero2;
+        const float2 yh01 = y_hi ? YH01 : zero2, yh23 = y_hi ? YH23 : zero2;
+        const float2 yl01 = y_lo ? YL01 : zero2, yl23 = y_lo ? YL23 : zero2;
+        const float2 zu01 = make_float2(Z01.y, Z23.x);
+        const float2 zu23 = make_float2(Z23.y, z_hi ? above : 0.f);     // face k = nz: boundary
+        const float2 zl01 = make_float2(z_lo ? Z01.x : 0.f, Z01.y);     // face k = 0: boundary
+        float2 d01 = sub2(xh01, xl01), d23 = sub2(xh23, xl23);
+        d01 = add2(d01, sub2(yh01, yl01));
+        d23 = add2(d23, sub2(yh23, yl23));
+        d01 = add2(d01, sub2(zu01, zl01));
+        d23 = add2(d23, sub2(zu23, Z23));
+        const float2 ncv = g.k[kAdjNegCv];
+        float2 P01 = sub2(lo2(L), mul2(ncv, d01)), P23 = sub2(hi2(L), mul2(ncv, d23));
+        if (any_mine) {
+            float LPn[kVec] = {P01.x, P01.y, P23.x, P23.y};
+            uint32_t m = all_points ? 0u : receiver_bits(points, s.n_src);
+            for (int r = all_points ? 0 : -1; all_points ? r < s.n_rec : m != 0; r++) {
+                if (!all_points) {
+                    r = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.rec_off[r] - base;
+                if (d >= 0 && d < kVec && step >= s.rec_start[r]) {
+                    const float gr = (float)a.grad_rec[r * a.grad_stride + (step - a.grad_step0)];
+#pragma unroll
+                    for (int e = 0; e < kVec; e++)
+                        if (e == d) LPn[e] = LPn[e] + gr;
+                }
+            }
+            m = all_points ? 0u : source_bits(points, s.n_src);
+            for (int q = all_points ? 0 : -1; all_points ? q < s.n_src : m != 0; q++) {
+                if (!all_points) {
+                    q = __ffs(m) - 1;
+                    m &= m - 1;
+                }
+                const int64_t d = s.src_off[q] - base;
+                if (d >= 0 && d < kVec && step < s.src_len[q]) {
+                    float v = LPn[0];
+#pragma unroll
+                    for (int e = 1; e < kVec; e++)
+                        if (e == d) v = LPn[e];
+                    a.grad_src[q * a.grad_stride + (step - a.grad_step0)] = (double)(s.cs * v);
+                }
+            }
+            P01 = make_float2(LPn[0], LPn[1]);
+            P23 = make_float2(LPn[2], LPn[3]);
+        }
+
+        // ---- the layer, wall and relaxation transposes
+        float2 h01 = P01, h23 = P23;             // lp_hat
+        if (LAYER) {
+            if (fi_cell != 1.f) { h01 = mul2(h01, dup2(fi_cell)); h23 = mul2(h23, dup2(fi_cell)); }
+            if (fj_cell != 1.f) { h01 = mul2(h01, dup2(fj_cell)); h23 = mul2(h23, dup2(fj_cell)); }
+            if (damp_z) { h01 = mul2(h01, fkc01); h23 = mul2(h23, fkc23); }
+        }
+        float2 t01 = h01, t23 = h23;             // lp_tilde
+        float2 n01 = h01, n23 = h23;             // the new lambda(p)
+        if (WALLS && (wall_column || i == 0 || i == s.nx - 1)) {
+            float lph[kVec] = {h01.x, h01.y, h23.x, h23.y};
+            float lpt[kVec] = {h01.x, h01.y, h23.x, h23.y};
+            float lpart[kVec] = {h01.x, h01.y, h23.x, h23.y};
+#pragma unroll
+            for (int e = 0; e < kVec; e++) {
+                int64_t idx;
+                const int f = shell_face(s, i, j, k0 + e, idx);
+                if (f < 0) continue;
+                const float *entry = s.shell[f] + 2 * idx;
+                const float u = __ldg(entry), q = __ldg(entry + 1);
+                lpt[e] = u * lph[e];
+                lpart[e] = lpt[e] - q * lph[e];
+                if (a.grad_shell) {
+                    const float *hh = a.hist.shell + (step - a.hist.shell_step0) * 2 * a.hist.shell_total +
+                                      a.hist.face_off[f] + idx;
+                    const double uu = (double)u;
+                    a.grad_shell[a.hist.face_off[f] + idx] +=
+                        -(double)lph[e] * uu * uu * ((double)hh[a.hist.shell_total] + (double)hh[0]);
+                }
+            }
+            t01 = make_float2(lpt[0], lpt[1]);
+            t23 = make_float2(lpt[2], lpt[3]);
+            n01 = make_float2(lpart[0], lpart[1]);
+            n23 = make_float2(lpart[2], lpart[3]);
+        }
+        float2 D01 = mul2(g.k[kAdjScp], t01), D23 = mul2(g.k[kAdjScp], t23);   // lambda_D^n
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            const float2 p01 = lo2(LS[r]), p23 = hi2(LS[r]);
+            // ld + gain ((1 - decay) lpsi - mean lpt); lpsi <- decay lpsi + mean lpt
+            const float2 in01 = sub2(mul2(g.k[kAdjOneMinusDecay + r], p01), mul2(g.k[kAdjMean + r], t01));
+            const float2 in23 = sub2(mul2(g.k[kAdjOneMinusDecay + r], p23), mul2(g.k[kAdjMean + r], t23));
+            D01 = sub2(D01, mul2(g.k[kAdjNegGain + r], in01));
+            D23 = sub2(D23, mul2(g.k[kAdjNegGain + r], in23));
+            const float2 s01 = sub2(mul2(g.k[kAdjDecay + r], p01), mul2(g.k[kAdjNegMean + r], t01));
+            const float2 s23 = sub2(mul2(g.k[kAdjDecay + r], p23), mul2(g.k[kAdjNegMean + r], t23));
+            LS[r] = make_float4(s01.x, s01.y, s23.x, s23.y);
+        }
+
+        // ---- stores
+        *reinterpret_cast<float4 *>(a.lp + base) = make_float4(n01.x, n01.y, n23.x, n23.y);
+#pragma unroll
+        for (int r = 0; r < NR; r++) *reinterpret_cast<float4 *>(a.lpsi + r * s.field + base) = LS[r];
+        *reinterpret_cast<float4 *>(a.out_d + base) = make_float4(D01.x, D01.y, D23.x, D23.y);
+        *reinterpret_cast<float4 *>(a.out_vx + base) = make_float4(XL01.x, XL01.y, XL23.x, XL23.y);
+        *reinterpret_cast<float4 *>(a.out_vy + base) = make_float4(YL01.x, YL01.y, YL23.x, YL23.y);
+        *reinterpret_cast<float4 *>(a.out_vz + base) = make_float4(Z01.x, Z01.y, Z23.x, Z23.y);
+        if (!x_hi)
+            *reinterpret_cast<float4 *>(a.out_vx + base + s.plane) = make_float4(XH01.x, XH01.y, XH23.x, XH23.y);
+        if (!y_hi)
+            *reinterpret_cast<float4 *>(a.out_vy + base + s.pz) = make_float4(YH01.x, YH01.y, YH23.x, YH23.y);
+        if (!z_hi) a.out_vz[base + kVec] = above;
+        Dc = Dxp;
+        XL01 = XH01;
+        XL23 = XH23;
+    }
+}
+
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, 3) lean_adjoint_sweep(const LeanAdjointParams g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= g.a.room.nz / kVec || j >= g.a.room.ny) return;
+    const int i_begin = blockIdx.z * g.a.planes;
+    lean_adjoint_column<LAYER, WALLS, NR>(g, i_begin, min(g.a.room.nx, i_begin + g.a.planes), j, c,
+                                          *g.a.step_base + g.a.local_step);
+}
+
 template <typename T, bool LAYER>
 __device__ __forceinline__ void adjoint_velocity_column(const AdjointParams<T> &a, int i_begin,
                                                         int i_end, int j, int c) {
@@ -5224,6 +5489,28 @@ struct AdjFused {
 };
 
 template <typename T, bool L, bool W, int NR>
+struct LeanAdjFused {
+    static void launch(const LeanAdjointParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        lean_adjoint_sweep<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
+// The packed coefficients of lean_adjoint_sweep, rounded to float as the room's own and
+// combined in float as adjoint_pressure_column combines them.
+void fill_adjoint_pairs(float2 *k, const RoomHost &h) {
+    auto put = [&](int slot, float v) { k[slot] = make_float2(v, v); };
+    put(kAdjNegCv, -(float)h.coef[0]);
+    put(kAdjScp, (float)h.coef[3] - (float)h.coef[1]);
+    for (int r = 0; r < h.n_relax; r++) {
+        put(kAdjNegGain + r, -(float)h.gain[r]);
+        put(kAdjOneMinusDecay + r, 1.0f - (float)h.decay[r]);
+        put(kAdjMean + r, (float)h.mean[r]);
+        put(kAdjNegMean + r, -(float)h.mean[r]);
+        put(kAdjDecay + r, (float)h.decay[r]);
+    }
+}
+
+template <typename T, bool L, bool W, int NR>
 struct AdjFusedAir {
     static void launch(const AdjointParams<T> &p, dim3 g, dim3 b, cudaStream_t st) {
         if (NR > 0) adjoint_fused_sweep<T, L, W, NR, NR != 0, 2><<<g, b, 0, st>>>(p);
@@ -5501,11 +5788,25 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     }
     int parity = 0;       // the copy holding the latest mu and lambda_D
     bool first = true;
+    // Without air gradients, single precision with nz a multiple of 4 takes the packed step.
+    const bool lean_adjoint = !air && sizeof(T) == 4 && h.nz % kVec == 0;
     auto fused_unit = [&](int32_t local, cudaStream_t s, int par) {
         AdjointParams<T> q = par ? a1 : a0;
         q.local_step = local;
-        if (air) dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, s);
-        else dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        if (air) {
+            dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, s);
+            return;
+        }
+        if constexpr (sizeof(T) == 4) {
+            if (lean_adjoint) {
+                LeanAdjointParams lq{};
+                lq.a = q;
+                fill_adjoint_pairs(lq.k, h);
+                dispatch_pressure<float, LeanAdjFused>(h.has_layer, h.has_walls, h.n_relax, lq, L.grid, L.block, s);
+                return;
+            }
+        }
+        dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
     };
     // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter),
     // one graph per starting copy. Steps [e - G, e) in reverse: graph locals are captured in

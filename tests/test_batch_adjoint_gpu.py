@@ -97,12 +97,14 @@ def test_batched_patch_gradient_matches_central_differences():
     assert np.max(np.abs(got - np.array(fds))) <= 1e-6 * np.max(np.abs(grads[2].walls)), (got, fds)
 
 
-def test_single_precision_lean_recorded_rooms_equal_the_batch():
-    """Without air, a single-precision room with nz a multiple of 4 records its forward run with
-    the lean one-sweep step (writing the boundary history as it goes) while a batch records with
-    two sweeps: recordings and wall and source gradients agree bit for bit, over an odd number of
-    steps (the state ends in the second copy and is moved back), and the final pressure equals a
-    plain run's."""
+@pytest.mark.parametrize("air", [None, AirAbsorption(temperature=21.0, relative_humidity=45.0)])
+def test_single_precision_lean_recorded_rooms_equal_the_batch(air):
+    """Without air gradients, a single-precision room with nz a multiple of 4 records its forward
+    run with the lean one-sweep step (writing the boundary history as it goes) and reverses it
+    with the packed adjoint step, while a batch records with two sweeps and reverses with the
+    generic adjoint sweeps: recordings and wall and source gradients agree bit for bit, with and
+    without relaxation states and a sponge, over an odd number of steps (the state ends in the
+    second copy and is moved back), and the final pressure equals a plain run's."""
     from ac_fdtd_b200 import CudaAcousticFDTD
 
     steps = 71
@@ -111,6 +113,8 @@ def test_single_precision_lean_recorded_rooms_equal_the_batch():
         dict(grid=Grid(dx=0.05, nx=9, ny=14, nz=16), walls=WallAdmittances(0.2, 0.1, 0.3, 0.05, 0.4, 0.15),
              absorbing_layer=AbsorbingLayer(thickness=3, faces=((1, 1),))),
     ]
+    if air is not None:
+        specs = [dict(spec, air_absorption=air) for spec in specs]
     batch = DifferentiableBatch(specs, dtype=np.float32, max_steps=steps)
     for r, spec in enumerate(specs):
         pts = points(spec, r)
@@ -123,9 +127,10 @@ def test_single_precision_lean_recorded_rooms_equal_the_batch():
     for r, spec in enumerate(specs):
         pts = points(spec, r)
         room = DifferentiableRoom(spec["grid"], dtype=np.float32, walls=spec["walls"],
-                                  absorbing_layer=spec.get("absorbing_layer"), max_steps=steps)
+                                  absorbing_layer=spec.get("absorbing_layer"), air_absorption=air,
+                                  max_steps=steps)
         plain = CudaAcousticFDTD(spec["grid"], dtype=np.float32, walls=spec["walls"],
-                                 absorbing_layer=spec.get("absorbing_layer"))
+                                 absorbing_layer=spec.get("absorbing_layer"), air_absorption=air)
         for s in (room.solver, plain):
             s.add_volume_source(pts[0], gaussian_pulse(steps, s.dt, 2000.0))
             for p in pts[1:]:
