@@ -4212,6 +4212,7 @@ int set_time_blocking(acf_batch *b, int32_t steps) {
     groups = (h.nx + planes - 1) / planes;
     const size_t ring_bytes = (size_t)groups * kPairRing * h.plane * sizeof(float);
     const size_t counters = (size_t)(per_group * groups);
+    b->time_block = 1;          // until the new buffers are in place
     cudaFree(b->pair_ring);
     cudaFree(b->pair_progress);
     b->pair_ring = nullptr;
