@@ -482,13 +482,16 @@ def run_ours(args) -> None:
     phases["h2d_GBps"] = h2d / (phases["h2d_ms"] * 1e-3) / 1e9 if phases["h2d_ms"] > 0 else None
     phases["d2h_GBps"] = d2h / (phases["d2h_ms"] * 1e-3) / 1e9 if phases["d2h_ms"] > 0 else None
 
-    batched = None if args.skip_extras else batched_vs_per_room(args)
-    adjoint = None if args.skip_extras else adjoint_cost(args)
-    inversion = None if args.skip_extras else batched_adjoint_cost(args)
-    precision = None if args.skip_extras else precision_check(args)
-    slabs = None if args.skip_extras else slab_overhead(args)
-    pressure_only = None if args.skip_extras else pressure_only_cost(args)
-    time_blocking = None if args.skip_extras else time_blocking_cost(args)
+    # The extra sections are single-GPU measurements: the N = 1 line carries them, and a
+    # multi-rank run does not hold its GPUs for them.
+    skip = args.skip_extras or world > 1
+    batched = None if skip else batched_vs_per_room(args)
+    adjoint = None if skip else adjoint_cost(args)
+    inversion = None if skip else batched_adjoint_cost(args)
+    precision = None if skip else precision_check(args)
+    slabs = None if skip else slab_overhead(args)
+    pressure_only = None if skip else pressure_only_cost(args)
+    time_blocking = None if skip else time_blocking_cost(args)
 
     clock_record = clocks.summary()
     if clock_record.get("sm_mhz"):
