@@ -62,3 +62,5 @@ def test_null_arguments_are_refused():
     assert lib.acf_set_wait_test(None, 0, -1) == 1
     assert lib.acf_batch_device_status(None, None) == 1
     assert lib.acf_device_status(None, None) == 1
+    assert lib.acf_set_time_blocking(None, 2) == 1
+    assert lib.acf_get_time_blocking(None) == -1
