@@ -2993,9 +2993,11 @@ struct LeanAdjointParams {
     float2 k[22];          // the kAdj* slots, each value in both lanes
 };
 
-template <bool LAYER, bool WALLS, int NR>
+// AIR: also accumulate the air-strength sums of adjoint_pressure_column into `acc` (3R + 1
+// two-lane partial sums), from the D/psi history of the reversed step.
+template <bool LAYER, bool WALLS, int NR, bool AIR = false>
 __device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, int i_begin, int i_end,
-                                                    int j, int c, int64_t step) {
+                                                    int j, int c, int64_t step, float2 *acc = nullptr) {
     const AdjointParams<float> &a = g.a;
     const Room<float> &s = a.room;
     const int k0 = c * kVec;
@@ -3056,8 +3058,22 @@ __device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, 
             prefetch_l2(a.lp + next);
 #pragma unroll
             for (int r = 0; r < NR; r++) prefetch_l2(a.lpsi + r * s.field + next);
+            if (AIR && NR > 0) {
+                const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
+                const float *h = a.hist.fields + slot * (1 + NR) * s.field + next;
+#pragma unroll
+                for (int r = 0; r <= NR; r++) prefetch_l2(h + r * s.field);
+            }
         }
         // ---- loads
+        float4 HD = make_float4(0.f, 0.f, 0.f, 0.f), HS[NR > 0 ? NR : 1];
+        if (AIR && NR > 0) {   // D^n and psi^n of the reversed step
+            const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
+            const float *h = a.hist.fields + slot * (1 + NR) * s.field + base;
+            HD = __ldg(reinterpret_cast<const float4 *>(h));
+#pragma unroll
+            for (int r = 0; r < NR; r++) HS[r] = __ldg(reinterpret_cast<const float4 *>(h + (1 + r) * s.field));
+        }
         float4 Dxp = make_float4(0.f, 0.f, 0.f, 0.f), Dy = Dxp, Dyp = Dxp;
         if (x_hi) Dxp = __ldg(reinterpret_cast<const float4 *>(a.ld + base + s.plane));
         if (y_lo) Dy = __ldg(reinterpret_cast<const float4 *>(a.ld + base - s.pz));
@@ -3207,10 +3223,20 @@ __device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, 
             const float2 in23 = sub2(mul2(g.k[kAdjOneMinusDecay + r], p23), mul2(g.k[kAdjMean + r], t23));
             D01 = sub2(D01, mul2(g.k[kAdjNegGain + r], in01));
             D23 = sub2(D23, mul2(g.k[kAdjNegGain + r], in23));
+            if (AIR) {   // d inner, lpt off, lpsi off with off = psi - gain d
+                const float2 d01 = lo2(HD), d23 = hi2(HD);
+                const float2 o01 = add2(lo2(HS[r]), mul2(g.k[kAdjNegGain + r], d01));
+                const float2 o23 = add2(hi2(HS[r]), mul2(g.k[kAdjNegGain + r], d23));
+                acc[r] = add2(add2(acc[r], mul2(d01, in01)), mul2(d23, in23));
+                acc[NR + r] = add2(add2(acc[NR + r], mul2(t01, o01)), mul2(t23, o23));
+                acc[2 * NR + r] = add2(add2(acc[2 * NR + r], mul2(p01, o01)), mul2(p23, o23));
+            }
             const float2 s01 = sub2(mul2(g.k[kAdjDecay + r], p01), mul2(g.k[kAdjNegMean + r], t01));
             const float2 s23 = sub2(mul2(g.k[kAdjDecay + r], p23), mul2(g.k[kAdjNegMean + r], t23));
             LS[r] = make_float4(s01.x, s01.y, s23.x, s23.y);
         }
+        if (AIR && NR > 0)
+            acc[3 * NR] = add2(add2(acc[3 * NR], mul2(lo2(HD), t01)), mul2(hi2(HD), t23));
 
         // ---- stores
         *reinterpret_cast<float4 *>(a.lp + base) = make_float4(n01.x, n01.y, n23.x, n23.y);
@@ -3228,6 +3254,41 @@ __device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, 
         Dc = Dxp;
         XL01 = XH01;
         XL23 = XH23;
+    }
+}
+
+// The same step with the air-strength sums (relaxation states present): per-thread two-lane
+// sums over the launch's cells, then FP64 block sums into air_partials, as adjoint_fused_sweep.
+template <bool LAYER, bool WALLS, int NR>
+__global__ void __launch_bounds__(256, 2) lean_adjoint_air_sweep(const LeanAdjointParams g) {
+    constexpr int NA = 3 * NR + 1;
+    const AdjointParams<float> &a = g.a;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    float2 acc[NA];
+#pragma unroll
+    for (int t = 0; t < NA; t++) acc[t] = dup2(0.f);
+    if (c < a.room.nz / kVec && j < a.room.ny) {
+        const int i_begin = blockIdx.z * a.planes;
+        lean_adjoint_column<LAYER, WALLS, NR, true>(g, i_begin, min(a.room.nx, i_begin + a.planes), j, c,
+                                                    *a.step_base + a.local_step, acc);
+    }
+    __shared__ double red[NA][8];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int n_warps = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+    for (int t = 0; t < NA; t++) {
+        double v = (double)acc[t].x + (double)acc[t].y;
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+        if (lane == 0) red[t][warp] = v;
+    }
+    __syncthreads();
+    if (tid < NA) {
+        double v = 0.0;
+        for (int w = 0; w < n_warps; w++) v += red[tid][w];
+        const int64_t block = ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        a.air_partials[block * NA + tid] += v;
     }
 }
 
@@ -5496,6 +5557,14 @@ struct LeanAdjFused {
     }
 };
 
+template <typename T, bool L, bool W, int NR>
+struct LeanAdjFusedAir {
+    static void launch(const LeanAdjointParams &p, dim3 g, dim3 b, cudaStream_t st) {
+        if constexpr (NR > 0) lean_adjoint_air_sweep<L, W, NR><<<g, b, 0, st>>>(p);
+        else lean_adjoint_sweep<L, W, NR><<<g, b, 0, st>>>(p);
+    }
+};
+
 // The packed coefficients of lean_adjoint_sweep, rounded to float as the room's own and
 // combined in float as adjoint_pressure_column combines them.
 void fill_adjoint_pairs(float2 *k, const RoomHost &h) {
@@ -5789,25 +5858,28 @@ int adjoint_impl(acf_batch *b, const double *grad_rec, double *grad_src, double 
     }
     int parity = 0;       // the copy holding the latest mu and lambda_D
     bool first = true;
-    // Without air gradients, single precision with nz a multiple of 4 takes the packed step.
-    const bool lean_adjoint = !air && sizeof(T) == 4 && h.nz % kVec == 0;
+    // Single precision with nz a multiple of 4 takes the packed step, with or without the air
+    // sums (4 z elements per thread, so its grid of blocks is within the air partials' count).
+    const bool lean_adjoint = sizeof(T) == 4 && h.nz % kVec == 0;
     auto fused_unit = [&](int32_t local, cudaStream_t s, int par) {
         AdjointParams<T> q = par ? a1 : a0;
         q.local_step = local;
-        if (air) {
-            dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, s);
-            return;
-        }
         if constexpr (sizeof(T) == 4) {
             if (lean_adjoint) {
                 LeanAdjointParams lq{};
                 lq.a = q;
                 fill_adjoint_pairs(lq.k, h);
-                dispatch_pressure<float, LeanAdjFused>(h.has_layer, h.has_walls, h.n_relax, lq, L.grid, L.block, s);
+                if (air)
+                    dispatch_pressure<float, LeanAdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, lq, L.grid,
+                                                              L.block, s);
+                else
+                    dispatch_pressure<float, LeanAdjFused>(h.has_layer, h.has_walls, h.n_relax, lq, L.grid,
+                                                           L.block, s);
                 return;
             }
         }
-        dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
+        if (air) dispatch_pressure<T, AdjFusedAir>(h.has_layer, h.has_walls, h.n_relax, q, LA.grid, LA.block, s);
+        else dispatch_pressure<T, AdjFused>(h.has_layer, h.has_walls, h.n_relax, q, L.grid, L.block, s);
     };
     // Graph chunks of at most kAdjointChunk steps (one per segment when segments are shorter),
     // one graph per starting copy. Steps [e - G, e) in reverse: graph locals are captured in

@@ -268,6 +268,40 @@ def test_air_gradients_agree_with_and_without_recompute():
     assert auto.checkpoint_every == STEPS          # a small room's history always fits
 
 
+def test_single_precision_packed_air_adjoint_tracks_double():
+    """Single precision with nz a multiple of 4 reverses its steps with the packed adjoint step,
+    air sums included; against the double-precision generic adjoint: walls and source to
+    2e-3 / 1e-3 as the unpacked single-precision adjoint, the ISO strengths and times to 2e-3 of
+    their largest gradient. With whole-run history and with checkpoint recompute the single-
+    precision gradients agree bit for bit."""
+    grid = Grid(dx=0.05, nx=14, ny=12, nz=12)
+    air = AirAbsorption(temperature=19.0, relative_humidity=55.0)
+    steps = 77
+
+    def gradients(dtype, every):
+        room = DifferentiableRoom(grid, dtype=dtype, walls=WallAdmittances(*XI), air_absorption=air,
+                                  max_steps=steps, wrt=("signal", "walls", "air"), checkpoint_every=every)
+        room.solver.add_volume_source(SOURCE, gaussian_pulse(steps, room.dt, 2500.0))
+        for point in RECEIVERS:
+            room.solver.add_pressure_receiver(point)
+        rec = room.forward(steps).astype(np.float64)
+        w = np.random.default_rng(12).standard_normal(rec.shape)
+        g = room.backward(w * rec)
+        room.solver.close()
+        return g
+
+    g64 = gradients(np.float64, steps)
+    g32 = gradients(np.float32, steps)
+    g32_recompute = gradients(np.float32, 9)
+    for name in ("walls", "signal", "strength", "relaxation_time"):
+        np.testing.assert_array_equal(getattr(g32, name), getattr(g32_recompute, name))
+    np.testing.assert_allclose(g32.walls, g64.walls, rtol=2e-3)
+    assert np.max(np.abs(g32.signal - g64.signal)) < 1e-3 * np.max(np.abs(g64.signal))
+    for name in ("strength", "relaxation_time"):
+        a, b = getattr(g32, name), getattr(g64, name)
+        assert np.max(np.abs(a - b)) <= 2e-3 * np.max(np.abs(b)), (name, a, b)
+
+
 @pytest.mark.parametrize("every", [STEPS, 9])
 def test_l2_prefetch_leaves_gradients_unchanged(every):
     """The plane prefetch (off by default at this size, forced on here) touches no arithmetic:
