@@ -249,7 +249,11 @@ int acf_energy_terms_planes(acf_solver *solver, double dx, int64_t x_begin, int6
  * -- the recorded run then keeps them and nothing is recomputed -- else ceil(sqrt(max_steps)).
  *
  * acf_adjoint_prepare  allocates the history for runs of up to max_steps steps.
- * acf_forward_record   is acf_run that also writes that history (and the checkpoints).
+ * acf_forward_record   is acf_run that also writes that history (and the checkpoints). In
+ *                      single precision with nz a multiple of 4 and no checkpoints it takes one
+ *                      lean sweep per step into the second copy of p and v -- allocated on the
+ *                      first such call when the scheme has none -- and leaves the state in the
+ *                      primary copy; results equal the two-sweep record bit for bit.
  * acf_adjoint_run      takes dL/drec (n_receivers rows of n_steps doubles, host) and returns
  *                      (each optional, host, FP64): dL/dsignal (n_sources rows of n_steps),
  *                      dL/da per boundary cell (acf_adjoint_shell_size entries, shell order of
