@@ -250,7 +250,7 @@ int acf_energy_terms_planes(acf_solver *solver, double dx, int64_t x_begin, int6
  *
  * acf_adjoint_prepare  allocates the history for runs of up to max_steps steps.
  * acf_forward_record   is acf_run that also writes that history (and the checkpoints). In
- *                      single precision with nz a multiple of 4 and no checkpoints it takes one
+ *                      single precision with nz a multiple of 4 and no air gradients it takes one
  *                      lean sweep per step into the second copy of p and v -- allocated on the
  *                      first such call when the scheme has none -- and leaves the state in the
  *                      primary copy; results equal the two-sweep record bit for bit.
