@@ -144,3 +144,40 @@ def test_single_precision_lean_recorded_rooms_equal_the_batch(air):
         np.testing.assert_array_equal(grads[r].signal, single.signal)
         room.solver.close()
         plain.close()
+
+
+@pytest.mark.parametrize("shape", [(2, 3, 4), (5, 1, 8), (1, 6, 12), (7, 6, 16)])
+def test_packed_adjoint_on_small_and_degenerate_rooms(shape):
+    """The packed single-precision adjoint step on rooms where one chunk is both the bottom and
+    the top of its row (nz = 4), with a single row or a single plane, a sponge on every face,
+    walls and relaxation states, sources and receivers on the room's corners: recordings and wall
+    and source gradients equal the batch's generic adjoint bit for bit."""
+    steps = 45
+    grid = Grid(dx=0.05, nx=shape[0], ny=shape[1], nz=shape[2])
+    spec = dict(grid=grid, walls=WallAdmittances(0.3, 0.1, 0.45, 0.2, 0.08, 0.27),
+                absorbing_layer=AbsorbingLayer(thickness=1),
+                air_absorption=AirAbsorption(temperature=22.0, relative_humidity=40.0))
+    other = dict(spec, grid=Grid(dx=0.05, nx=4, ny=5, nz=8))
+    L = grid.lengths
+    corner = tuple(0.999 * x for x in L)
+    pts = [(0.0, 0.0, 0.0), corner, (0.0, corner[1], 0.0)]
+    batch = DifferentiableBatch([spec, other], dtype=np.float32, max_steps=steps)
+    for r in range(2):
+        batch.batch.add_volume_source(r, pts[0], gaussian_pulse(steps, batch.batch.dt(r), 2000.0))
+        for p in pts[1:]:
+            batch.batch.add_pressure_receiver(r, p)
+    recs = batch.forward(steps)
+    w = np.random.default_rng(sum(shape)).standard_normal(recs[0].shape)
+    grads = batch.backward([w * recs[0].astype(np.float64), np.zeros_like(recs[1], dtype=np.float64)])
+    room = DifferentiableRoom(grid, dtype=np.float32, walls=spec["walls"],
+                              absorbing_layer=spec["absorbing_layer"],
+                              air_absorption=spec["air_absorption"], max_steps=steps)
+    room.solver.add_volume_source(pts[0], gaussian_pulse(steps, room.dt, 2000.0))
+    for p in pts[1:]:
+        room.solver.add_pressure_receiver(p)
+    rec = room.forward(steps)
+    np.testing.assert_array_equal(rec, recs[0])
+    single = room.backward(w * rec.astype(np.float64))
+    np.testing.assert_array_equal(grads[0].walls, single.walls)
+    np.testing.assert_array_equal(grads[0].signal, single.signal)
+    room.solver.close()
