@@ -95,6 +95,11 @@ struct Vec4<float> {
         const float4 t = __ldg(reinterpret_cast<const float4 *>(a));
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     }
+    // Streaming (evict-first) load: data read once, such as the adjoint's history.
+    __device__ __forceinline__ static void ldcs(const float *a, float v[4]) {
+        const float4 t = __ldcs(reinterpret_cast<const float4 *>(a));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
 };
 
 template <>
@@ -113,7 +118,22 @@ struct Vec4<double> {
         const double2 t1 = __ldg(reinterpret_cast<const double2 *>(a + 2));
         v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
     }
+    __device__ __forceinline__ static void ldcs(const double *a, double v[4]) {
+        const double2 t0 = __ldcs(reinterpret_cast<const double2 *>(a));
+        const double2 t1 = __ldcs(reinterpret_cast<const double2 *>(a + 2));
+        v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+    }
 };
+
+// Streaming (evict-first) stores of 4 elements, for data written once and read once much later
+// -- the adjoint's D/psi history -- so that it does not push the state out of L2.
+__device__ __forceinline__ void store_streaming(float *a, const float v[4]) {
+    __stcs(reinterpret_cast<float4 *>(a), make_float4(v[0], v[1], v[2], v[3]));
+}
+__device__ __forceinline__ void store_streaming(double *a, const double v[4]) {
+    __stcs(reinterpret_cast<double2 *>(a), make_double2(v[0], v[1]));
+    __stcs(reinterpret_cast<double2 *>(a + 2), make_double2(v[2], v[3]));
+}
 
 // Ask L2 for the line holding `a` ahead of its load: the request holds no register and no
 // shared memory, so a marching thread can have its next plane on the way from DRAM while it
@@ -570,9 +590,9 @@ __device__ __forceinline__ void pressure_column(const Room<T> &s, int i_begin, i
             const int64_t slot = rel % hist->fields_slots;
             if (rel >= 0) {
                 T *h = hist->fields + slot * (1 + NR) * s.field + base;
-                Vec4<T>::store(h, D);
+                store_streaming(h, D);
 #pragma unroll
-                for (int r = 0; r < NR; r++) Vec4<T>::store(h + (1 + r) * s.field, S[r]);
+                for (int r = 0; r < NR; r++) store_streaming(h + (1 + r) * s.field, S[r]);
             }
         }
 
@@ -989,6 +1009,7 @@ struct VecW;
 template <typename T>
 struct VecW<T, 4> {
     __device__ __forceinline__ static void ldg(const T *__restrict__ a, T v[4]) { Vec4<T>::ldg(a, v); }
+    __device__ __forceinline__ static void ldcs(const T *a, T v[4]) { Vec4<T>::ldcs(a, v); }
     __device__ __forceinline__ static void load(const T *a, T v[4]) { Vec4<T>::load(a, v); }
     __device__ __forceinline__ static void store(T *__restrict__ a, const T v[4]) { Vec4<T>::store(a, v); }
     __device__ __forceinline__ static void lds(const T *a, T v[4]) { lds4<T>(a, v); }
@@ -998,6 +1019,10 @@ template <>
 struct VecW<float, 2> {
     __device__ __forceinline__ static void ldg(const float *__restrict__ a, float v[2]) {
         const float2 t = __ldg(reinterpret_cast<const float2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void ldcs(const float *a, float v[2]) {
+        const float2 t = __ldcs(reinterpret_cast<const float2 *>(a));
         v[0] = t.x; v[1] = t.y;
     }
     __device__ __forceinline__ static void load(const float *a, float v[2]) {
@@ -1017,6 +1042,10 @@ template <>
 struct VecW<double, 2> {
     __device__ __forceinline__ static void ldg(const double *__restrict__ a, double v[2]) {
         const double2 t = __ldg(reinterpret_cast<const double2 *>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    __device__ __forceinline__ static void ldcs(const double *a, double v[2]) {
+        const double2 t = __ldcs(reinterpret_cast<const double2 *>(a));
         v[0] = t.x; v[1] = t.y;
     }
     __device__ __forceinline__ static void load(const double *a, double v[2]) {
@@ -2774,9 +2803,9 @@ __device__ __forceinline__ void adjoint_pressure_column(const AdjointParams<T> &
         if (air) {
             const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
             const T *h = a.hist.fields + slot * (1 + NR) * s.field + base;
-            VecW<T, VW>::ldg(h, HD);
+            VecW<T, VW>::ldcs(h, HD);           // read once: streaming
 #pragma unroll
-            for (int r = 0; r < NR; r++) VecW<T, VW>::ldg(h + (1 + r) * s.field, HS[r]);
+            for (int r = 0; r < NR; r++) VecW<T, VW>::ldcs(h + (1 + r) * s.field, HS[r]);
         }
         T fi = T(1), fj = T(1);
         if (LAYER) {
@@ -3070,9 +3099,9 @@ __device__ __forceinline__ void lean_adjoint_column(const LeanAdjointParams &g, 
         if (AIR && NR > 0) {   // D^n and psi^n of the reversed step
             const int64_t slot = (step - a.hist.fields_step0) % a.hist.fields_slots;
             const float *h = a.hist.fields + slot * (1 + NR) * s.field + base;
-            HD = __ldg(reinterpret_cast<const float4 *>(h));
+            HD = __ldcs(reinterpret_cast<const float4 *>(h));         // read once: streaming
 #pragma unroll
-            for (int r = 0; r < NR; r++) HS[r] = __ldg(reinterpret_cast<const float4 *>(h + (1 + r) * s.field));
+            for (int r = 0; r < NR; r++) HS[r] = __ldcs(reinterpret_cast<const float4 *>(h + (1 + r) * s.field));
         }
         float4 Dxp = make_float4(0.f, 0.f, 0.f, 0.f), Dy = Dxp, Dyp = Dxp;
         if (x_hi) Dxp = __ldg(reinterpret_cast<const float4 *>(a.ld + base + s.plane));
